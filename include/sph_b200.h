@@ -1,0 +1,186 @@
+/*
+ * sph_b200.h -- C ABI of the B200 (sm_100a) pseudospectral transform core.
+ *
+ * Drop-in for the device branch (`IF (gdev_active)`) of REDONDITO's sphp-gpu
+ * transforms and of its pseudospectral/boundary operators.  A Fortran
+ * ISO_C_BINDING shim keeps the reference's subroutine signatures and calls
+ * these functions with device addresses (the `use_device_addr` pattern of
+ * src/sphp-gpu/sphp_sca.F90:83-87).
+ *
+ * Conventions
+ *  - Every pointer named grid/in/out/a/b/... is a DEVICE pointer.
+ *  - Physical fields: double (nz planes) x (nphi) x (nlat), theta fastest,
+ *    i.e. Fortran REAL(8) f(nlat,nphi,nz) with one MPI rank (ksta=1, kend=nz).
+ *  - Spectral fields: interleaved complex double (re,im), lm fastest,
+ *    i.e. Fortran COMPLEX(8) f(nlm,nz) with lmsta=1, lmend=nlm; lm in SHTns
+ *    m-major order, lm(l,m) = m*(2*lmax+1-m)/2 + l (0-based).
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream).  Calls are
+ *    stream-ordered and return once the work is enqueued; the Fortran shim
+ *    synchronises to keep the reference's blocking semantics.
+ *  - One plan per host thread: a plan's scratch is not re-entrant, like the
+ *    reference's shared gcarr1-3 buffers (src/sphp-gpu/sphp_mod.F90:56-77).
+ *  - Every function returns SPH_OK (0) or an SPH_E* code; the reference
+ *    prints and STOPs instead (the shim maps a non-zero code to that).
+ */
+#ifndef SPH_B200_H
+#define SPH_B200_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  SPH_OK = 0,
+  SPH_EINVAL = 1,    /* bad size, pointer or argument */
+  SPH_ENOMEM = 2,    /* device or host allocation failed */
+  SPH_ECUDA = 3,     /* a CUDA call or launch failed */
+  SPH_ENOTREADY = 4, /* boundary tables not set up (sph_setup_bc) */
+  SPH_EIO = 5,       /* FC-Gram table file missing or short */
+  SPH_ETIMEDOUT = 6  /* a bounded device wait gave up */
+};
+
+enum { SPH_FP64 = 0, SPH_MIXED = 1 };
+
+typedef struct sph_plan sph_plan;
+
+/* ---------------------------------------------------------------- plans */
+
+/* Replaces fcgram_create_plan (src/sphp/fcgram_mod.f90:49-150) together with
+ * fftp3d_create_plan (src/sphp-gpu/sphp_sca.F90:478-625), grid_init and
+ * box_init (src/pseudo/pseudospec_mod.f90:41-69,126-236).
+ *   lmax         : triangular truncation (mmax = lmax, mres = 1)
+ *   nlat, nphi   : Gauss grid (nlat even, nphi > 2*lmax)
+ *   nz           : radial points including the Cz continuation points
+ *   Cz, oz       : FC-Gram continuation and matching points (0,0 = periodic)
+ *   rint, rext   : shell radii; z(k) = rint + k*dz, dz = (rext-rint)/(nz-Cz-1)
+ *   dir          : host pointer, Cz x oz column-major continuation operator
+ *                  dir = A.Q^T (see sph_fcgram_load_tables); NULL if Cz == 0
+ *   precision    : SPH_FP64 or SPH_MIXED (Legendre on tensor cores in
+ *                  compensated bf16 / scaled fp16, FFTs in fp32)
+ * Allocates the plan's device tables and scratch with cudaMalloc on the
+ * current device. */
+int sph_plan_create(sph_plan** plan, int lmax, int nlat, int nphi, int nz, int Cz, int oz,
+                    double rint, double rext, const double* dir, int precision);
+
+/* fcgram_destroy_plan (src/sphp/fcgram_mod.f90:153-182). */
+int sph_plan_destroy(sph_plan* plan);
+
+/* load_dirichlet_tables (src/sphp/fcgram_mod.f90:186-263): reads
+ * tdir/A{C}-{d}.dat and tdir/Q{d}.dat (raw column-major float64) and writes
+ * dir = A.Q^T (C x d, column-major) to the host array dir. */
+int sph_fcgram_load_tables(const char* tdir, int C, int d, double* dir);
+
+/* Sizes of a plan: nlm, and the element counts of one physical field
+ * (nlat*nphi*nz doubles) and one spectral field (nlm*nz complex). */
+int sph_plan_sizes(const sph_plan* plan, int* nlm, long long* grid_elems, long long* spec_elems);
+
+/* box_init outputs (pseudospec_mod.f90:174-227), host arrays (any may be NULL):
+ * theta(nlat), Gauss weights(nlat), phi(nphi), z(nz), kz(nz), ell(nlm), emm(nlm). */
+int sph_grid(const sph_plan* plan, double* theta, double* weights, double* phi, double* z,
+             double* kz, int* ell, int* emm);
+
+/* ---------------------------------------------------------------- transforms */
+
+/* fftp2d_real_to_complex_xy (src/sphp-gpu/sphp_sca.F90:771-853): per-plane
+ * spherical-harmonic analysis of all nz planes, in (nlat,nphi,nz) -> out
+ * (nlm,nz).  The input is preserved (the reference destroys it). */
+int sph_fftp2d_real_to_complex_xy(sph_plan* plan, const double* in, double* out, void* stream);
+
+/* fftp2d_complex_to_real_xy (src/sphp-gpu/sphp_sca.F90:984-1065): per-plane
+ * synthesis, in (nlm,nz) preserved -> out (nlat,nphi,nz). */
+int sph_fftp2d_complex_to_real_xy(sph_plan* plan, const double* in, double* out, void* stream);
+
+/* fftp1d_real_to_complex_z (src/sphp-gpu/sphp_sca.F90:856-945 device
+ * branch; CPU arithmetic src/sphp/sphp_sca.F90:332-397): FC-Gram
+ * continuation, forward DFT along z (sign -1), divide by nz.  In place. */
+int sph_fftp1d_real_to_complex_z(sph_plan* plan, double* inout, void* stream);
+
+/* fftp1d_complex_to_real_z (src/sphp-gpu/sphp_sca.F90:1068-1114; CPU
+ * src/sphp/sphp_sca.F90:495-530): inverse DFT along z (sign +1), no scaling.
+ * In place. */
+int sph_fftp1d_complex_to_real_z(sph_plan* plan, double* inout, void* stream);
+
+/* fftp3d_real_to_complex (src/sphp-gpu/sphp_sca.F90:735-768): 2D analysis +
+ * z forward.  in preserved. */
+int sph_fftp3d_real_to_complex(sph_plan* plan, const double* in, double* out, void* stream);
+
+/* fftp3d_complex_to_real (src/sphp-gpu/sphp_sca.F90:948-981): z inverse +
+ * 2D synthesis.  in is destroyed (the z transform is in place), as in the
+ * reference. */
+int sph_fftp3d_complex_to_real(sph_plan* plan, double* in, double* out, void* stream);
+
+/* fftp2d_vec_to_qst (src/sphp-gpu/sphp_vec.F90:128-218): (v_r,v_th,v_ph) ->
+ * (Q,S,T) with v = Q Y r + S r grad Y - T r x grad Y.  Inputs preserved. */
+int sph_fftp2d_vec_to_qst(sph_plan* plan, const double* vr, const double* vt, const double* vp,
+                          double* q, double* s, double* t, void* stream);
+
+/* fftp2d_qst_to_vec (src/sphp-gpu/sphp_vec.F90:221-309). Inputs preserved. */
+int sph_fftp2d_qst_to_vec(sph_plan* plan, const double* q, const double* s, const double* t,
+                          double* vr, double* vt, double* vp, void* stream);
+
+/* ---------------------------------------------------------------- operators
+ * src/pseudo/pseudospec_hd.f90.  Spectral arrays are (nlm,nz) complex. */
+
+/* derivr (pseudospec_hd.f90:18-135): b = d^p a / dr^p; esp 'r' (a,b in
+ * (lm,r): continuation + forward + (i kz)^p + inverse, one kernel) or 'k'
+ * (a,b in (lm,kz): b = (i kz)^p a, Nyquist kept). a is preserved. */
+int sph_derivr(sph_plan* plan, const double* a, double* b, int p, char esp, void* stream);
+/* laplang (pseudospec_hd.f90:138-172): b = -l(l+1) a */
+int sph_laplang(sph_plan* plan, const double* a, double* b, void* stream);
+/* multr (pseudospec_hd.f90:175-208): b = z^p a */
+int sph_multr(sph_plan* plan, const double* a, double* b, int p, void* stream);
+/* dlr (pseudospec_hd.f90:254-288): b = d2a/dr2 - l(l+1) a / r^2 (one kernel) */
+int sph_dlr(sph_plan* plan, const double* a, double* b, void* stream);
+/* saxpby_c (pseudospec_hd.f90:291-326): z = a x + b y (z may alias x or y) */
+int sph_saxpby_c(sph_plan* plan, double* z, const double* x, double a, const double* y, double b,
+                 void* stream);
+/* saxpby_r (pseudospec_hd.f90:329-366): the same on physical fields */
+int sph_saxpby_r(sph_plan* plan, double* z, const double* x, double a, const double* y, double b,
+                 void* stream);
+/* fc_filter (pseudospec_hd.f90:369-467): a *= exp(-16 ln10 (2kz/(nz Dkz))^100), in place */
+int sph_fc_filter(sph_plan* plan, double* a, char esp, void* stream);
+/* copy (pseudospec_hd.f90:470-497): b = a */
+int sph_copy(sph_plan* plan, const double* a, double* b, void* stream);
+/* prodvec (pseudospec_hd.f90:211-251): C = A x B on the physical planes
+ * k < nz - Cz; the continuation planes of C are set to zero. */
+int sph_prodvec(sph_plan* plan, const double* ar, const double* at, const double* ap,
+                const double* br, const double* bt, const double* bp, double* cr, double* ct,
+                double* cp, void* stream);
+
+/* ---------------------------------------------------------------- boundary
+ * src/boundary/boundary_mod.f90, src/boundary/vboundary.f90 */
+
+/* setup_bc / v_setup / invDl_setup (boundary_mod.f90:35-59,140-241;
+ * vboundary.f90:34-56): bcint, bcext = "noslip" (the only type).  Builds the
+ * FC-Gram derivative matrices, the row-scaled LU per l in FP64 on the host,
+ * and uploads M_l (N x (N-4) per l) and the d2/dr2 border rows. */
+int sph_setup_bc(sph_plan* plan, const char* bcint, const char* bcext);
+/* dirichlet (boundary_mod.f90:62-93): a(lm,1) = a(lm,N) = 0 */
+int sph_dirichlet(sph_plan* plan, double* a, void* stream);
+/* invDl (boundary_mod.f90:244-292): W = M_l phi(3:N-2), batched FP64 GEMM on
+ * the device; l = 0 and the continuation points are zero. */
+int sph_invDl(sph_plan* plan, const double* phi, double* w, void* stream);
+/* v_imposebc (vboundary.f90:59-87): dirichlet(tor), pol = invDl(phi), phi = D_l pol */
+int sph_v_imposebc(sph_plan* plan, double* tor, double* phi, double* pol, void* stream);
+/* v_imposebc_fast (vboundary.f90:90-130): phi recomputed at rows 1,2,N-1,N only */
+int sph_v_imposebc_fast(sph_plan* plan, double* tor, double* phi, double* pol, void* stream);
+
+/* ---------------------------------------------------------------- NL + RK3
+ * Composed from the reference's building blocks (the reference has no
+ * driver; vboundary.f90:61-63 says the BCs close every RK stage).
+ * State (Z, W, phi) in (lm,r), phi = D_l W.  u = curl curl(W r^) + curl(Z r^).
+ *   rhs_z   = r T_N + nu D_l Z
+ *   rhs_phi = d(r S_N)/dr - Q_N + nu D_l phi,    N = u x curl u
+ * energy (host double, may be NULL) = 0.5 * int |u|^2 dV over the physical
+ * shell (trapezoid in r, Gauss in theta), accumulated in FP64.  Needs
+ * sph_setup_bc. */
+int sph_nl_rhs(sph_plan* plan, const double* Z, const double* W, const double* phi, double nu,
+               double* rhs_z, double* rhs_phi, double* energy, void* stream);
+/* One RK3 step, X = X0 + (dt/o) RHS(X) for o = 3,2,1 with v_imposebc after
+ * each stage; Z, W, phi updated in place.  energy of the initial state. */
+int sph_rk3_step(sph_plan* plan, double* Z, double* W, double* phi, double nu, double dt,
+                 double* energy, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,186 @@
+// k_zfft.cu -- radial (z) transforms on the (lm, z) spectral layout.
+//
+// One CTA owns LB consecutive lm columns and all nz rows in shared memory
+// (row-major: element (k, c) at sm[k*LB + c]), so every global access is a
+// contiguous LB*16-byte run of one row.  The reference's steps, each a
+// separate pass over HBM there, are fused here into one read and one write:
+//   fftp1d_real_to_complex_z (src/sphp/sphp_sca.F90:332-397): continuation
+//     of the last C rows from rows 1..d and N-d+1..N (sphp_sca.F90:369-381,
+//     same summation order), DFT sign -1, divide by nz;
+//   fftp1d_complex_to_real_z (sphp_sca.F90:495-530): DFT sign +1;
+//   derivr_r (src/pseudo/pseudospec_hd.f90:101-135): forward, (i kz)^p,
+//     inverse, without the reference's temporary copy;
+//   fc_filter_r (pseudospec_hd.f90:443-467) and dlr (pseudospec_hd.f90:254-288)
+//     likewise.
+#include "fft_engine.cuh"
+
+namespace {
+
+constexpr int ZTHREADS = 256;
+constexpr int ZMAXCOL = 4096;  // LB*nz complex values per CTA (64 KB)
+
+struct ZArgs {
+  const double2* in;
+  double2* out;
+  int nlm, nz, N, C, d, LB, order;
+  const double* dir;      // C x d column-major
+  const double2* kfac;    // (i kz)^order, nz entries
+  const double* filt;     // nz
+  const double* zinv2;    // nz
+  const int* ell;         // nlm
+  FftDesc fd;
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(ZTHREADS) zfft_kernel(ZArgs a) {
+  extern __shared__ double2 sm[];
+  const int LB = a.LB, nz = a.nz, nlm = a.nlm;
+  const int lm0 = blockIdx.x * LB;
+  const int tid = threadIdx.x;
+  const bool cont = (MODE != Z_INV) && a.C > 0;
+  const int nload = cont ? a.N : nz;
+  double2* orig = sm + (size_t)LB * nz;  // D_l keeps the input column for the l(l+1)/r^2 term
+
+  const int* __restrict__ rev = a.fd.rev;
+  for (int idx = tid; idx < nload * LB; idx += ZTHREADS) {
+    int r = idx / LB, c = idx - r * LB;
+    int lm = lm0 + c;
+    double2 v = lm < nlm ? a.in[(size_t)r * nlm + lm] : make_double2(0.0, 0.0);
+    // the inverse transform takes its input in digit-reversed order
+    sm[(MODE == Z_INV ? __ldg(rev + r) : r) * LB + c] = v;
+  }
+  if (MODE == Z_DLR) {
+    for (int idx = tid; idx < nz * LB; idx += ZTHREADS) {
+      int r = idx / LB, c = idx - r * LB;
+      int lm = lm0 + c;
+      orig[idx] = lm < nlm ? a.in[(size_t)r * nlm + lm] : make_double2(0.0, 0.0);
+    }
+  }
+  __syncthreads();
+
+  if (cont) {
+    // inout(n-C+ii) = sum_jj dir(ii,jj) inout(n-C-d+jj) + dir(C-ii+1,jj) inout(d-jj+1)
+    const int C = a.C, d = a.d, N = a.N;
+    for (int idx = tid; idx < C * LB; idx += ZTHREADS) {
+      int ii = idx / LB, c = idx - ii * LB;  // ii is 0-based
+      double2 acc;
+      {
+        double wr = __ldg(a.dir + ii), wl = __ldg(a.dir + (C - 1 - ii));
+        double2 xr = sm[(N - d) * LB + c], xl = sm[(d - 1) * LB + c];
+        acc = make_double2(wr * xr.x + wl * xl.x, wr * xr.y + wl * xl.y);
+      }
+      for (int jj = 1; jj < d; ++jj) {
+        double wr = __ldg(a.dir + ii + C * jj), wl = __ldg(a.dir + (C - 1 - ii) + C * jj);
+        double2 xr = sm[(N - d + jj) * LB + c], xl = sm[(d - 1 - jj) * LB + c];
+        acc.x = (acc.x + wr * xr.x) + wl * xl.x;
+        acc.y = (acc.y + wr * xr.y) + wl * xl.y;
+      }
+      sm[(N + ii) * LB + c] = acc;
+    }
+    __syncthreads();
+  }
+
+  FftGeom g;
+  g.n = nz; g.batch = LB; g.bs = 1; g.es = LB; g.pad = 0; g.jfast = false;
+  if (MODE == Z_INV) {
+    fft_dit(sm, a.fd, g, +1);
+  } else {
+    fft_dif(sm, a.fd, g, -1);
+  }
+
+  if (MODE == Z_DERIV || MODE == Z_FILTER || MODE == Z_DLR) {
+    // spectral multiply in place (frequency k sits at row rev[k]), then back
+    const double rn = (double)nz;
+    for (int idx = tid; idx < nz * LB; idx += ZTHREADS) {
+      int k = idx / LB, c = idx - k * LB;
+      int o = __ldg(rev + k) * LB + c;
+      double2 v = sm[o];
+      v.x = v.x / rn;
+      v.y = v.y / rn;
+      if (MODE == Z_FILTER) v = cscale(v, a.filt[k]);
+      else v = cmul(a.kfac[k], v);
+      sm[o] = v;
+    }
+    __syncthreads();
+    fft_dit(sm, a.fd, g, +1);
+  }
+
+  for (int idx = tid; idx < nz * LB; idx += ZTHREADS) {
+    int r = idx / LB, c = idx - r * LB;
+    int lm = lm0 + c;
+    if (lm >= nlm) continue;
+    double2 v;
+    if (MODE == Z_FWD) {
+      v = sm[__ldg(rev + r) * LB + c];
+      v.x = v.x / (double)nz;
+      v.y = v.y / (double)nz;
+    } else {
+      v = sm[idx];
+    }
+    if (MODE == Z_DLR) {
+      // b = b + z^-2 * (-l(l+1) a)   (laplang, multr(-2), saxpby_c)
+      double lf = -(double)(a.ell[lm] * (a.ell[lm] + 1));
+      double2 o = orig[idx];
+      double zi = a.zinv2[r];
+      v.x = v.x + zi * (lf * o.x);
+      v.y = v.y + zi * (lf * o.y);
+    }
+    a.out[(size_t)r * nlm + lm] = v;
+  }
+}
+
+template <int MODE>
+int launch_mode(const ZArgs& a, int nblocks, size_t smem, cudaStream_t st) {
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev & 63]) {
+    if (cudaFuncSetAttribute(zfft_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             200 * 1024) != cudaSuccess)
+      return SPH_ECUDA;
+    attr_set[dev & 63] = true;
+  }
+  zfft_kernel<MODE><<<nblocks, ZTHREADS, smem, st>>>(a);
+  SPH_LAUNCH_OK();
+  return SPH_OK;
+}
+
+}  // namespace
+
+int launch_zfft(const sph_plan* p, int mode, const double2* in, double2* out, int order,
+                cudaStream_t st) {
+  ZArgs a;
+  a.in = in;
+  a.out = out;
+  a.nlm = p->nlm;
+  a.nz = p->nz;
+  a.N = p->N;
+  a.C = p->C;
+  a.d = p->d;
+  a.order = order;
+  a.dir = p->d_dir;
+  a.kfac = (order >= 1 && order <= 4) ? p->kfac + (size_t)(order - 1) * p->nz : nullptr;
+  a.filt = p->filt;
+  a.zinv2 = p->zinv2;
+  a.ell = p->d_ell;
+  a.fd = p->fz;
+  // columns per CTA: a power of two with LB*nz <= ZMAXCOL, at most 64
+  int LB = 64;
+  while (LB > 1 && LB * p->nz > ZMAXCOL) LB >>= 1;
+  if (LB * p->nz > ZMAXCOL) return SPH_EINVAL;
+  a.LB = LB;
+  int nblocks = (p->nlm + LB - 1) / LB;
+  size_t smem = (size_t)LB * p->nz * sizeof(double2) * (mode == Z_DLR ? 2 : 1);
+  switch (mode) {
+    case Z_FWD: return launch_mode<Z_FWD>(a, nblocks, smem, st);
+    case Z_INV: return launch_mode<Z_INV>(a, nblocks, smem, st);
+    case Z_DERIV:
+      if (!a.kfac) return SPH_EINVAL;
+      return launch_mode<Z_DERIV>(a, nblocks, smem, st);
+    case Z_FILTER: return launch_mode<Z_FILTER>(a, nblocks, smem, st);
+    case Z_DLR:
+      a.kfac = p->kfac + (size_t)1 * p->nz;  // (i kz)^2
+      return launch_mode<Z_DLR>(a, nblocks, smem, st);
+  }
+  return SPH_EINVAL;
+}

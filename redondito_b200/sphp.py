@@ -1,0 +1,328 @@
+"""Host-side mirror of REDONDITO's sphp / pseudo / boundary interfaces over
+the B200 C ABI (include/sph_b200.h, redondito_b200/_lib/libsph_b200.so).
+
+The names and argument meanings follow the reference's Fortran routines
+(src/sphp-gpu/sphp_sca.F90, src/sphp-gpu/sphp_vec.F90,
+src/pseudo/pseudospec_hd.f90, src/boundary/*.f90) so that code written
+against them reads the same:
+
+    plan = Plan(lmax=31, nz=58, Cz=25, oz=5, rint=0.35, rext=1.0)
+    fftp3d_real_to_complex(plan, grid, spec)      # grid (nz,nphi,nlat) f64
+    fftp3d_complex_to_real(plan, spec, grid)      # spec (nz,nlm) c128, destroyed
+    derivr(plan, a, b, 1, 'r')
+
+Fields are torch tensors on the plan's CUDA device: physical fields float64
+of shape (nz, nphi, nlat) (Fortran f(nlat,nphi,nz)), spectral fields
+complex128 of shape (nz, nlm) (Fortran f(nlm,nz)).  PyTorch only provides
+device memory and the current stream; every transform runs in the sm_100a
+library.  There is no CPU fallback: without the built library or a CUDA
+device the calls raise.
+
+Errors: the reference prints and STOPs (e.g. fcgram_mod.f90:96-102); here a
+non-zero status from the library raises SphError with the code's name.
+"""
+import ctypes
+import os
+
+import torch
+
+from . import build as _build
+
+SPH_FP64, SPH_MIXED = 0, 1
+_CODES = {1: "SPH_EINVAL", 2: "SPH_ENOMEM", 3: "SPH_ECUDA", 4: "SPH_ENOTREADY", 5: "SPH_EIO",
+          6: "SPH_ETIMEDOUT"}
+TABLES_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tables")
+
+# exported symbols, as declared in include/sph_b200.h
+SYMBOLS = (
+    "sph_plan_create", "sph_plan_destroy", "sph_fcgram_load_tables", "sph_plan_sizes", "sph_grid",
+    "sph_fftp2d_real_to_complex_xy", "sph_fftp2d_complex_to_real_xy",
+    "sph_fftp1d_real_to_complex_z", "sph_fftp1d_complex_to_real_z",
+    "sph_fftp3d_real_to_complex", "sph_fftp3d_complex_to_real",
+    "sph_fftp2d_vec_to_qst", "sph_fftp2d_qst_to_vec",
+    "sph_derivr", "sph_laplang", "sph_multr", "sph_dlr", "sph_saxpby_c", "sph_saxpby_r",
+    "sph_fc_filter", "sph_copy", "sph_prodvec",
+    "sph_setup_bc", "sph_dirichlet", "sph_invDl", "sph_v_imposebc", "sph_v_imposebc_fast",
+    "sph_nl_rhs", "sph_rk3_step",
+)
+
+
+class SphError(RuntimeError):
+    def __init__(self, fn, code):
+        super().__init__(f"{fn} failed: {_CODES.get(code, code)}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib(build_if_missing=True):
+    """Load the in-tree library (building it with nvcc if it is stale)."""
+    global _lib
+    if _lib is None:
+        if build_if_missing and not _build.up_to_date():
+            _build.build()
+        if not os.path.exists(_build.LIB):
+            raise RuntimeError(f"{_build.LIB} is not built; run python -m redondito_b200.build")
+        L = ctypes.CDLL(_build.LIB)
+        P, I, D, Vp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+        pD = ctypes.POINTER(ctypes.c_double)
+        pI = ctypes.POINTER(ctypes.c_int)
+        sig = {
+            "sph_plan_create": [ctypes.POINTER(P), I, I, I, I, I, I, D, D, pD, I],
+            "sph_plan_destroy": [P],
+            "sph_fcgram_load_tables": [ctypes.c_char_p, I, I, pD],
+            "sph_plan_sizes": [P, pI, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)],
+            "sph_grid": [P, pD, pD, pD, pD, pD, pI, pI],
+            "sph_fftp2d_real_to_complex_xy": [P, Vp, Vp, Vp],
+            "sph_fftp2d_complex_to_real_xy": [P, Vp, Vp, Vp],
+            "sph_fftp1d_real_to_complex_z": [P, Vp, Vp],
+            "sph_fftp1d_complex_to_real_z": [P, Vp, Vp],
+            "sph_fftp3d_real_to_complex": [P, Vp, Vp, Vp],
+            "sph_fftp3d_complex_to_real": [P, Vp, Vp, Vp],
+            "sph_fftp2d_vec_to_qst": [P] + [Vp] * 6 + [Vp],
+            "sph_fftp2d_qst_to_vec": [P] + [Vp] * 6 + [Vp],
+            "sph_derivr": [P, Vp, Vp, I, ctypes.c_char, Vp],
+            "sph_laplang": [P, Vp, Vp, Vp],
+            "sph_multr": [P, Vp, Vp, I, Vp],
+            "sph_dlr": [P, Vp, Vp, Vp],
+            "sph_saxpby_c": [P, Vp, Vp, D, Vp, D, Vp],
+            "sph_saxpby_r": [P, Vp, Vp, D, Vp, D, Vp],
+            "sph_fc_filter": [P, Vp, ctypes.c_char, Vp],
+            "sph_copy": [P, Vp, Vp, Vp],
+            "sph_prodvec": [P] + [Vp] * 9 + [Vp],
+            "sph_setup_bc": [P, ctypes.c_char_p, ctypes.c_char_p],
+            "sph_dirichlet": [P, Vp, Vp],
+            "sph_invDl": [P, Vp, Vp, Vp],
+            "sph_v_imposebc": [P, Vp, Vp, Vp, Vp],
+            "sph_v_imposebc_fast": [P, Vp, Vp, Vp, Vp],
+            "sph_nl_rhs": [P, Vp, Vp, Vp, D, Vp, Vp, pD, Vp],
+            "sph_rk3_step": [P, Vp, Vp, Vp, D, D, pD, Vp],
+        }
+        for name, args in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _check(fn, rc):
+    if rc != 0:
+        raise SphError(fn, rc)
+
+
+def _call(name, *args):
+    _check(name, getattr(lib(), name)(*args))
+
+
+def nlat_for(lmax):
+    """grid_init rule (src/pseudo/pseudospec_mod.f90:67)."""
+    return 4 * ((3 * (lmax + 1) + 7) // 8)
+
+
+def load_dirichlet_tables(C=25, d=5, tdir=TABLES_DIR):
+    """load_dirichlet_tables (src/sphp/fcgram_mod.f90:186-263): dir = A.Q^T."""
+    out = (ctypes.c_double * (C * d))()
+    _call("sph_fcgram_load_tables", tdir.encode(), C, d, out)
+    return list(out)
+
+
+class Plan:
+    """fcgram_create_plan + grid_init/box_init: the angular grid, the FC-Gram
+    continuation in z, the device tables and the plan's scratch."""
+
+    def __init__(self, lmax, nz, nlat=None, nphi=None, Cz=0, oz=0, rint=0.35, rext=1.0,
+                 tdir=TABLES_DIR, precision=SPH_FP64, device=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("redondito_b200 needs a CUDA device (B200, sm_100a)")
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        self.lmax, self.nz, self.Cz, self.oz = lmax, nz, Cz, oz
+        self.nlat = nlat if nlat is not None else nlat_for(lmax)
+        self.nphi = nphi if nphi is not None else 2 * self.nlat
+        self.rint, self.rext = rint, rext
+        self.precision = precision
+        dirp = None
+        if Cz > 0:
+            d = load_dirichlet_tables(Cz, oz, tdir)
+            self._dir = (ctypes.c_double * len(d))(*d)
+            dirp = self._dir
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            _call("sph_plan_create", ctypes.byref(h), lmax, self.nlat, self.nphi, nz, Cz, oz,
+                  float(rint), float(rext), dirp, int(precision))
+        self.h = h
+        self.nlm = (lmax + 1) * (lmax + 2) // 2
+        self.N = nz - Cz
+        self._grid_arrays()
+        self._bc = False
+
+    def _grid_arrays(self):
+        def dbl(n):
+            return (ctypes.c_double * n)()
+        th, w, ph, z, kz = dbl(self.nlat), dbl(self.nlat), dbl(self.nphi), dbl(self.nz), dbl(self.nz)
+        ell, emm = (ctypes.c_int * self.nlm)(), (ctypes.c_int * self.nlm)()
+        _call("sph_grid", self.h, th, w, ph, z, kz, ell, emm)
+        self.theta = torch.tensor(list(th), dtype=torch.float64)
+        self.weights = torch.tensor(list(w), dtype=torch.float64)
+        self.phi = torch.tensor(list(ph), dtype=torch.float64)
+        self.z = torch.tensor(list(z), dtype=torch.float64)
+        self.kz = torch.tensor(list(kz), dtype=torch.float64)
+        self.ell = torch.tensor(list(ell), dtype=torch.int32)
+        self.emm = torch.tensor(list(emm), dtype=torch.int32)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().sph_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # allocation helpers
+    def new_grid(self):
+        return torch.zeros((self.nz, self.nphi, self.nlat), dtype=torch.float64, device=self.device)
+
+    def new_spec(self):
+        return torch.zeros((self.nz, self.nlm), dtype=torch.complex128, device=self.device)
+
+    def lm(self, l, m):
+        return m * (2 * self.lmax + 1 - m) // 2 + l
+
+
+def _ptr(t, shape, dtype):
+    if not isinstance(t, torch.Tensor) or t.device.type != "cuda":
+        raise TypeError("fields must be CUDA tensors")
+    if t.dtype != dtype or tuple(t.shape) != tuple(shape) or not t.is_contiguous():
+        raise ValueError(f"expected contiguous {dtype} tensor of shape {tuple(shape)}, "
+                         f"got {t.dtype} {tuple(t.shape)}")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _g(plan, t):
+    return _ptr(t, (plan.nz, plan.nphi, plan.nlat), torch.float64)
+
+
+def _s(plan, t):
+    return _ptr(t, (plan.nz, plan.nlm), torch.complex128)
+
+
+def _stream(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+# ---------------------------------------------------------------- transforms
+def fftp2d_real_to_complex_xy(plan, in_, out, stream=None):
+    _call("sph_fftp2d_real_to_complex_xy", plan.h, _g(plan, in_), _s(plan, out), _stream(stream))
+
+
+def fftp2d_complex_to_real_xy(plan, in_, out, stream=None):
+    _call("sph_fftp2d_complex_to_real_xy", plan.h, _s(plan, in_), _g(plan, out), _stream(stream))
+
+
+def fftp1d_real_to_complex_z(plan, inout, stream=None):
+    _call("sph_fftp1d_real_to_complex_z", plan.h, _s(plan, inout), _stream(stream))
+
+
+def fftp1d_complex_to_real_z(plan, inout, stream=None):
+    _call("sph_fftp1d_complex_to_real_z", plan.h, _s(plan, inout), _stream(stream))
+
+
+def fftp3d_real_to_complex(plan, in_, out, stream=None):
+    _call("sph_fftp3d_real_to_complex", plan.h, _g(plan, in_), _s(plan, out), _stream(stream))
+
+
+def fftp3d_complex_to_real(plan, in_, out, stream=None):
+    """The input is destroyed (the z transform is in place), as in the reference."""
+    _call("sph_fftp3d_complex_to_real", plan.h, _s(plan, in_), _g(plan, out), _stream(stream))
+
+
+def fftp2d_vec_to_qst(plan, vr, vt, vp, q, s, t, stream=None):
+    _call("sph_fftp2d_vec_to_qst", plan.h, _g(plan, vr), _g(plan, vt), _g(plan, vp),
+          _s(plan, q), _s(plan, s), _s(plan, t), _stream(stream))
+
+
+def fftp2d_qst_to_vec(plan, q, s, t, vr, vt, vp, stream=None):
+    _call("sph_fftp2d_qst_to_vec", plan.h, _s(plan, q), _s(plan, s), _s(plan, t),
+          _g(plan, vr), _g(plan, vt), _g(plan, vp), _stream(stream))
+
+
+# ---------------------------------------------------------------- operators
+def derivr(plan, a, b, p, esp, stream=None):
+    _call("sph_derivr", plan.h, _s(plan, a), _s(plan, b), int(p), esp.encode()[:1], _stream(stream))
+
+
+def laplang(plan, a, b, stream=None):
+    _call("sph_laplang", plan.h, _s(plan, a), _s(plan, b), _stream(stream))
+
+
+def multr(plan, a, b, p, stream=None):
+    _call("sph_multr", plan.h, _s(plan, a), _s(plan, b), int(p), _stream(stream))
+
+
+def dlr(plan, a, b, stream=None):
+    _call("sph_dlr", plan.h, _s(plan, a), _s(plan, b), _stream(stream))
+
+
+def saxpby_c(plan, z, x, a, y, b, stream=None):
+    _call("sph_saxpby_c", plan.h, _s(plan, z), _s(plan, x), float(a), _s(plan, y), float(b),
+          _stream(stream))
+
+
+def saxpby_r(plan, z, x, a, y, b, stream=None):
+    _call("sph_saxpby_r", plan.h, _g(plan, z), _g(plan, x), float(a), _g(plan, y), float(b),
+          _stream(stream))
+
+
+def fc_filter(plan, a, esp, stream=None):
+    _call("sph_fc_filter", plan.h, _s(plan, a), esp.encode()[:1], _stream(stream))
+
+
+def copy(plan, a, b, stream=None):
+    _call("sph_copy", plan.h, _s(plan, a), _s(plan, b), _stream(stream))
+
+
+def prodvec(plan, ar, at, ap, br, bt, bp, cr, ct, cp, stream=None):
+    _call("sph_prodvec", plan.h, *[_g(plan, x) for x in (ar, at, ap, br, bt, bp, cr, ct, cp)],
+          _stream(stream))
+
+
+# ---------------------------------------------------------------- boundary
+def setup_bc(plan, bckind=("noslip", "noslip")):
+    _call("sph_setup_bc", plan.h, bckind[0].encode(), bckind[1].encode())
+    plan._bc = True
+
+
+def dirichlet(plan, a, stream=None):
+    _call("sph_dirichlet", plan.h, _s(plan, a), _stream(stream))
+
+
+def invDl(plan, a, b, stream=None):
+    _call("sph_invDl", plan.h, _s(plan, a), _s(plan, b), _stream(stream))
+
+
+def v_imposebc(plan, tor, phi, pol, stream=None):
+    _call("sph_v_imposebc", plan.h, _s(plan, tor), _s(plan, phi), _s(plan, pol), _stream(stream))
+
+
+def v_imposebc_fast(plan, tor, phi, pol, stream=None):
+    _call("sph_v_imposebc_fast", plan.h, _s(plan, tor), _s(plan, phi), _s(plan, pol), _stream(stream))
+
+
+# ---------------------------------------------------------------- NL + RK3
+def nl_rhs(plan, Z, W, phi, nu, rhs_z, rhs_phi, stream=None):
+    e = ctypes.c_double(0.0)
+    _call("sph_nl_rhs", plan.h, _s(plan, Z), _s(plan, W), _s(plan, phi), float(nu),
+          _s(plan, rhs_z), _s(plan, rhs_phi), ctypes.byref(e), _stream(stream))
+    return e.value
+
+
+def rk3_step(plan, Z, W, phi, nu, dt, stream=None, energy=True):
+    e = ctypes.c_double(0.0)
+    _call("sph_rk3_step", plan.h, _s(plan, Z), _s(plan, W), _s(plan, phi), float(nu), float(dt),
+          ctypes.byref(e) if energy else None, _stream(stream))
+    return e.value

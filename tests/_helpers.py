@@ -1,0 +1,25 @@
+"""Shared helpers for the parity tests: seeded inputs and error measures."""
+import numpy as np
+
+
+def rel_l2(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    den = np.linalg.norm(b.ravel())
+    return np.linalg.norm((a - b).ravel()) / (den if den > 0 else 1.0)
+
+
+def radial_profile(z, rint, rext, rng, kmax=8):
+    """sum_k c_k cos(k pi (r - rint)/(rext - rint)), c_k ~ N(0,1)/(k+1)^2."""
+    c = rng.normal(size=kmax + 1) / (np.arange(kmax + 1) + 1.0) ** 2
+    return sum(c[k] * np.cos(k * np.pi * (z - rint) / (rext - rint)) for k in range(kmax + 1))
+
+
+def random_spec(P, rng, power=2.0, radial=True):
+    """a_lm(r) = N(0,1)(l+1)^-power (real for m = 0) times a smooth radial profile."""
+    a = (rng.normal(size=P.nlm) + 1j * rng.normal(size=P.nlm)) * (P.ell + 1.0) ** -power
+    a[P.emm == 0] = a[P.emm == 0].real
+    if radial:
+        prof = radial_profile(P.z, P.rint, P.rext, rng)
+        return prof[:, None] * a[None, :]
+    return np.repeat(a[None, :], P.nz, axis=0) * (1.0 + np.arange(P.nz))[:, None]
