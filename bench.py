@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""3D transform pairs/s at lmax=511, nr=256 on B200 (one line of JSON).
+
+Workload (one "step" = one transform pair of the field set): a scalar field
+and a vector field (3 components) at lmax = 511, Gauss grid 768 x 1536,
+nz = 256 radial points with FC-Gram C = 25, d = 5 continuation, r in
+[0.35, 1].  The state lives in (lm, kz) space; a pair is
+    scalar: fftp3d_complex_to_real + fftp3d_real_to_complex
+    vector: 3 x fftp1d_complex_to_real_z + fftp2d_qst_to_vec
+            + fftp2d_vec_to_qst + 3 x fftp1d_real_to_complex_z
+Synthetic seeded inputs stand in for a simulation state: coefficients
+N(0,1) (l+1)^-2.5 (real for m = 0) with 1% of the (r, l, m) entries set to
+amplitude 1e3 and random phase, taken to (lm, kz) by the forward z
+transform.  Every buffer is larger than L2 (126 MB), so no flush is needed.
+
+  value   : pairs/s with the state resident in HBM (device events)
+  e2e     : the same through the C ABI with host buffers: each step copies
+            the 4 spectral fields host->device, runs the pair and copies
+            them back (pinned memory, copies inside the timed region)
+  roofline: the kernel class with the largest share of the timed region,
+            achieved = algorithmic bytes (or flops) / its measured time
+  cpu_baseline: the CPU oracle (a C++ restatement of the reference's
+            arithmetic; the Fortran reference cannot be built here) on a
+            bounded sample, extrapolated to the full pair
+
+Multi-GPU: one process per GPU (torchrun); each rank runs its own replica
+of the workload (a single problem does not shard: the reference's only
+exchange is the slab transpose, which this design keeps on one device),
+so scaling is weak and value is the sum over ranks of max-time throughput.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W = dict(lmax=511, nlat=768, nphi=1536, nz=256, Cz=25, oz=5, rint=0.35, rext=1.0)
+# a smaller case of the same kernels for ncu captures (each grid 150 MB, still > L2)
+CASES = {"c3": W, "small": dict(lmax=255, nlat=384, nphi=768, nz=64, Cz=25, oz=5, rint=0.35, rext=1.0)}
+METRIC = "3D transform pairs/s at lmax=511 nr=256"
+SEED = 20261203 + 3
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--case", default="c3", choices=sorted(CASES),
+                    help="c3: the benchmark workload; small: profiling case for ncu")
+    a = ap.parse_args()
+    W.update(CASES[a.case]) if a.case != "c3" else None
+    return a
+
+
+# ---------------------------------------------------------------- CPU side
+def cpu_pairs_per_s(threads=None):
+    """The oracle's pair time on a bounded sample: the angular transforms of
+    all four fields on 2 and on 4 planes (a + b*nz fit, extrapolated to 256
+    planes) plus the z transforms of one full field (x4)."""
+    from oracle import oracle as O
+    if threads:
+        O.set_threads(threads)
+    nthreads = O.lib().orc_get_threads()
+    rng = np.random.default_rng(SEED)
+    times = {}
+    for nzs in (2, 4):
+        P = O.Plan(W["lmax"], nzs, nlat=W["nlat"], nphi=W["nphi"])
+        a = (rng.normal(size=(nzs, P.nlm)) + 1j * rng.normal(size=(nzs, P.nlm))) * (P.ell + 1.0) ** -2.5
+        a[:, P.emm == 0] = a[:, P.emm == 0].real
+        s0 = a.copy()
+        s0[:, 0] = 0
+        t0 = time.perf_counter()
+        g = P.sh_synthesis(a)
+        P.sh_analysis(g)
+        v = P.qst_synthesis(a, s0, s0)
+        P.qst_analysis(*v)
+        times[nzs] = time.perf_counter() - t0
+    t_sht = times[2] + (W["nz"] - 2) * (times[4] - times[2]) / 2.0
+    Pz = O.Plan(W["lmax"], W["nz"], nlat=W["nlat"], nphi=W["nphi"], C=W["Cz"], d=W["oz"],
+                rint=W["rint"], rext=W["rext"])
+    f = rng.normal(size=(W["nz"], Pz.nlm)) + 1j * rng.normal(size=(W["nz"], Pz.nlm))
+    t0 = time.perf_counter()
+    Pz.z_inverse(Pz.z_forward(f))
+    t_z = time.perf_counter() - t0
+    t_pair = t_sht + 4 * t_z
+    sample = ("oracle on all 4 fields: angular transforms on 2 and 4 planes "
+              f"({times[2]:.2f} s, {times[4]:.2f} s) extrapolated to 256 planes, "
+              f"plus one full z forward+inverse x4 ({t_z:.2f} s)")
+    return 1.0 / t_pair, nthreads, sample
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    v, cores, sample = cpu_pairs_per_s()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "pairs/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "scalar + vector field, lmax=511, 768x1536, nz=256, FC-Gram C=25 d=5",
+                   **W, "fields": 4},
+        "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference (Fortran + SHTns + FFTW + MPI) cannot be built here; "
+                "this is its C++ restatement (the oracle) on the host cores",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- GPU side
+def make_state(S, P, torch, gen):
+    """4 spectral fields in (lm, kz): scalar a, vector q, s, t."""
+    dev = P.device
+    ell = P.ell.to(dev).double()
+    emm = P.emm.to(dev)
+    amp = (ell + 1.0) ** -2.5
+    fields = []
+    for f in range(4):
+        re = torch.randn((P.nz, P.nlm), generator=gen, device=dev, dtype=torch.float64)
+        im = torch.randn((P.nz, P.nlm), generator=gen, device=dev, dtype=torch.float64)
+        x = torch.complex(re * amp, im * amp)
+        spike = torch.rand((P.nz, P.nlm), generator=gen, device=dev) < 0.01
+        ph = torch.rand((P.nz, P.nlm), generator=gen, device=dev, dtype=torch.float64) * 2 * np.pi
+        x = torch.where(spike, 1e3 * torch.exp(1j * ph), x)
+        x[:, emm == 0] = x[:, emm == 0].real.to(torch.complex128)
+        if f >= 2:  # S and T have no l = 0 part
+            x[:, 0] = 0
+        x = x.contiguous()
+        S.fftp1d_real_to_complex_z(P, x)
+        fields.append(x)
+    return fields
+
+
+def pair(S, P, st, grids):
+    a, q, s, t = st
+    g0, g1, g2, g3 = grids
+    S.fftp3d_complex_to_real(P, a, g0)
+    for x in (q, s, t):
+        S.fftp1d_complex_to_real_z(P, x)
+    S.fftp2d_qst_to_vec(P, q, s, t, g1, g2, g3)
+    S.fftp3d_real_to_complex(P, g0, a)
+    S.fftp2d_vec_to_qst(P, g1, g2, g3, q, s, t)
+    for x in (q, s, t):
+        S.fftp1d_real_to_complex_z(P, x)
+
+
+def fp64_peak():
+    from redondito_b200 import build as B
+    try:
+        out = subprocess.run([B.build_peak()], capture_output=True, text=True, timeout=120)
+        return json.loads(out.stdout.strip().splitlines()[-1])["fp64_tensor_tflops"]
+    except Exception:
+        return None
+
+
+def algorithmic_work(P, nfield_passes):
+    """Bytes (HBM kernels) or flops (Legendre) per step for each kernel class."""
+    nlm, nz, nlat, nphi, lmax = P.nlm, P.nz, P.nlat, P.nphi, P.lmax
+    grid_b = nlat * nphi * nz * 8
+    fold_b = (lmax + 1) * nlat * nz * 16
+    spec_b = nlm * nz * 16
+    leg = 4.0 * nz * (nlat // 2) * nlm  # flops, one scalar direction (even/odd folded)
+    return {
+        "phi_fwd": ("hbm", 4 * (grid_b + fold_b)),
+        "phi_inv": ("hbm", 4 * (grid_b + fold_b)),
+        "zfft": ("hbm", 8 * 2 * spec_b),
+        "leg_analysis": ("tensor", 2 * leg),
+        "leg_synthesis": ("tensor", 2 * leg),
+        "vec_analysis": ("tensor", 4 * leg),
+        "vec_synthesis": ("tensor", 4 * leg),
+        "ops": ("hbm", 0),
+    }
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import torch
+    import torch.distributed as dist
+    from redondito_b200 import sphp as S
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+
+    prec = S.SPH_FP64 if args.precision == "fp64" else S.SPH_MIXED
+    P = S.Plan(W["lmax"], W["nz"], nlat=W["nlat"], nphi=W["nphi"], Cz=W["Cz"], oz=W["oz"],
+               rint=W["rint"], rext=W["rext"], precision=prec)
+    gen = torch.Generator(device=P.device)
+    gen.manual_seed(SEED + rank)
+    st = make_state(S, P, torch, gen)
+    ref = [x.clone() for x in st]
+    grids = [P.new_grid() for _ in range(4)]
+    stream = torch.cuda.current_stream()
+
+    for _ in range(args.warmup):
+        pair(S, P, st, grids)
+    torch.cuda.synchronize()
+
+    peak_fp64 = fp64_peak() if rank == 0 else None
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+
+    gpu_index = local
+    cvd = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if cvd:
+        try:
+            gpu_index = int(cvd.split(",")[local])
+        except ValueError:
+            pass
+    clk = ClockSampler(gpu_index)
+    clk.start()
+    time.sleep(0.3)
+
+    S.timer_reset(P)
+    S.timer_enable(P, True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        pair(S, P, st, grids)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    S.timer_enable(P, False)
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    stage = S.timer_read(P)
+    if world > 1:
+        t = torch.tensor([ms], device=P.device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * args.steps / (ms * 1e-3)
+
+    # parity at full size: a pair is the identity on a forward-transformed state
+    rt = [float((torch.linalg.vector_norm(x - r) / torch.linalg.vector_norm(r)).item()) for x, r in zip(st, ref)]
+
+    # e2e through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        host = [x.cpu().pin_memory() for x in st]
+        nbytes = sum(h.numel() * h.element_size() for h in host)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0.record(stream)
+        for _ in range(args.steps):
+            for h, d in zip(host, st):
+                d.copy_(h, non_blocking=True)
+            pair(S, P, st, grids)
+            for h, d in zip(host, st):
+                h.copy_(d, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ems], device=P.device)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": world * args.steps / (ems * 1e-3), "unit": "pairs/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
+
+    # roofline of the dominant kernel class
+    work = algorithmic_work(P, 4)
+    dom = max(stage, key=lambda c: stage[c][0])
+    bound, per_step = work[dom]
+    tms, nl = stage[dom]
+    if bound == "hbm":
+        achieved = per_step * args.steps / (tms * 1e-3) / 1e9
+        peak = peaks.get("hbm_gbs", 6650.0)
+        unit = "GB/s"
+    else:
+        achieved = per_step * args.steps / (tms * 1e-3) / 1e12
+        peak = peak_fp64 if (peak_fp64 and args.precision == "fp64") else peaks.get("bf16_tflops", 1590.0)
+        unit = "TFLOP/s"
+    roofline = {"kernel": dom, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
+                "frac": achieved / peak if peak else None, "traffic": None,
+                "launches": nl, "ms_per_launch": tms / max(nl, 1),
+                "peak_source": ("fp64 DMMA probe run live (redondito_b200/peak/fp64_peak.cu)"
+                                if bound == "tensor" and args.precision == "fp64"
+                                else "MEASURED_PEAKS.json")}
+    shares = {c: round(stage[c][0] / max(ms, 1e-9), 4) for c in stage if stage[c][1]}
+    launches = sum(v[1] for v in stage.values())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, cores, sample = cpu_pairs_per_s()
+        cpu = {"value": v, "unit": "pairs/s", "cores": cores, "kind": "port", "sample": sample}
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "bf16x3/f32",
+        "data": "synthetic",
+        "config": {"workload": "scalar + vector field, lmax=511, 768x1536, nz=256, FC-Gram C=25 d=5",
+                   **W, "fields": 4, "precision": args.precision,
+                   "l2_flush": "inputs larger than L2 (every buffer > 126 MB)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "roofline": roofline,
+        "stage_share": shares,
+        "roundtrip_rel_l2": {"scalar": rt[0], "Q": rt[1], "S": rt[2], "T": rt[3]},
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -180,6 +180,21 @@ int sph_nl_rhs(sph_plan* plan, const double* Z, const double* W, const double* p
 int sph_rk3_step(sph_plan* plan, double* Z, double* W, double* phi, double nu, double dt,
                  double* energy, void* stream);
 
+/* ---------------------------------------------------------------- timers
+ * The reference accumulates wall time per stage in gtimer handles
+ * (src/sphp/sphp_mod.F90:36-41: comtime, ffttime, conttime, tottime;
+ * src/utils/gtimer_mod.f90).  Here each kernel launch of a plan can be
+ * bracketed by CUDA events on its own stream, accumulated per kernel class:
+ *   0 phi FFT forward   1 phi FFT inverse   2 Legendre analysis
+ *   3 Legendre synthesis 4 vector analysis  5 vector synthesis
+ *   6 z transforms      7 pointwise/boundary operators
+ * sph_timer_read synchronises the recorded events and returns, per class,
+ * the summed milliseconds and the number of launches since the last reset. */
+#define SPH_NTIMERS 8
+int sph_timer_enable(sph_plan* plan, int on);
+int sph_timer_reset(sph_plan* plan);
+int sph_timer_read(sph_plan* plan, double* ms, int* launches);
+
 #ifdef __cplusplus
 }
 #endif

@@ -37,6 +37,19 @@ def up_to_date():
     return all(os.path.getmtime(f) <= t for f in sources() + headers())
 
 
+PEAK_SRC = os.path.join(HERE, "peak", "fp64_peak.cu")
+PEAK_BIN = os.path.join(LIBDIR, "fp64_peak")
+
+
+def build_peak(force=False):
+    """The FP64 DMMA throughput probe used as the FP64 roofline denominator."""
+    if not force and os.path.exists(PEAK_BIN) and os.path.getmtime(PEAK_BIN) >= os.path.getmtime(PEAK_SRC):
+        return PEAK_BIN
+    os.makedirs(LIBDIR, exist_ok=True)
+    subprocess.run([NVCC, *ARCH, "-O3", "-ccbin", "/usr/bin/g++", "-o", PEAK_BIN, PEAK_SRC], check=True)
+    return PEAK_BIN
+
+
 def build(force=False, verbose=False, extra=()):
     if not force and up_to_date():
         return LIB
@@ -71,3 +84,4 @@ if __name__ == "__main__":
     v = "-v" in sys.argv
     extra = ["-Xptxas", "-v"] if "--ptxas" in sys.argv else []
     print(build(force=True, verbose=v or bool(extra), extra=extra))
+    print(build_peak(force=True))

@@ -376,6 +376,7 @@ int launch_leg_analysis(const sph_plan* p, int gfield, double2* spec, cudaStream
   a.out = spec;
   a.tiles = p->tilesA;
   dim3 grid(p->ntilesA, (2 * p->nz + AT_N - 1) / AT_N);
+  TimedLaunch tl(p, T_LEG_ANA, st);
   leg_analysis_kernel<<<grid, 128, 0, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;
@@ -387,6 +388,7 @@ int launch_leg_synthesis(const sph_plan* p, const double2* spec, int gfield, cud
   a.spec = spec;
   a.tiles = p->tilesS;
   dim3 grid(p->ntilesS, (2 * p->nz + ST_N - 1) / ST_N);
+  TimedLaunch tl(p, T_LEG_SYN, st);
   leg_synthesis_kernel<<<grid, 256, 0, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;
@@ -402,6 +404,7 @@ int launch_vec_analysis(const sph_plan* p, double2* s, double2* t, cudaStream_t 
                                           (int)smem) == cudaSuccess;
   if (!once) return SPH_ECUDA;
   dim3 grid(p->ntilesA32, (2 * p->nz + VA_N - 1) / VA_N);
+  TimedLaunch tl(p, T_VEC_ANA, st);
   vec_analysis_kernel<<<grid, 128, smem, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;
@@ -413,6 +416,7 @@ int launch_vec_synthesis(const sph_plan* p, const double2* s, const double2* t, 
   a.spec2 = t;
   a.tiles = p->tilesS32;
   dim3 grid(p->ntilesS32, (2 * p->nz + VS_N - 1) / VS_N);
+  TimedLaunch tl(p, T_VEC_SYN, st);
   vec_synthesis_kernel<<<grid, 256, 0, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;

@@ -197,6 +197,7 @@ int launch_kmul(const sph_plan* p, const double2* a, double2* b, int order, cuda
     if (a != b) SPH_CUDA_OK(cudaMemcpyAsync(b, a, n * sizeof(double2), cudaMemcpyDeviceToDevice, st));
     return SPH_OK;
   }
+  TimedLaunch tl(p, T_OPS, st);
   kmul_kernel<<<ew_blocks(n), EW_THREADS, 0, st>>>(a, b, p->kfac + (size_t)(order - 1) * p->nz, p->nlm, n);
   SPH_LAUNCH_OK();
   return SPH_OK;
@@ -204,6 +205,7 @@ int launch_kmul(const sph_plan* p, const double2* a, double2* b, int order, cuda
 
 int launch_filter_k(const sph_plan* p, double2* a, cudaStream_t st) {
   size_t n = spec_elems(p);
+  TimedLaunch tl(p, T_OPS, st);
   rowscale_kernel<<<ew_blocks(n), EW_THREADS, 0, st>>>(a, p->filt, p->nlm, n);
   SPH_LAUNCH_OK();
   return SPH_OK;
@@ -211,6 +213,7 @@ int launch_filter_k(const sph_plan* p, double2* a, cudaStream_t st) {
 
 int launch_laplang(const sph_plan* p, const double2* a, double2* b, cudaStream_t st) {
   size_t n = spec_elems(p);
+  TimedLaunch tl(p, T_OPS, st);
   laplang_kernel<<<ew_blocks(n), EW_THREADS, 0, st>>>(a, b, p->d_ell, p->nlm, n);
   SPH_LAUNCH_OK();
   return SPH_OK;
@@ -218,13 +221,15 @@ int launch_laplang(const sph_plan* p, const double2* a, double2* b, cudaStream_t
 
 int launch_multr(const sph_plan* p, const double2* a, double2* b, int power, cudaStream_t st) {
   size_t n = spec_elems(p);
+  TimedLaunch tl(p, T_OPS, st);
   multr_kernel<<<ew_blocks(n), EW_THREADS, 0, st>>>(a, b, p->d_z, power, p->nlm, n);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
 
-int launch_saxpby(double* z, const double* x, double a, const double* y, double b, size_t n,
-                  cudaStream_t st) {
+int launch_saxpby(const sph_plan* p, double* z, const double* x, double a, const double* y, double b,
+                  size_t n, cudaStream_t st) {
+  TimedLaunch tl(p, T_OPS, st);
   saxpby_kernel<<<ew_blocks(n), EW_THREADS, 0, st>>>(z, x, a, y, b, n);
   SPH_LAUNCH_OK();
   return SPH_OK;
@@ -234,6 +239,7 @@ int launch_prodvec(const sph_plan* p, const double* const* A, const double* cons
                    double* const* Cout, cudaStream_t st) {
   size_t plane = (size_t)p->nlat * p->nphi;
   size_t ntot = plane * p->nz, nphys = plane * p->N;
+  TimedLaunch tl(p, T_OPS, st);
   prodvec_kernel<<<ew_blocks(ntot), EW_THREADS, 0, st>>>(A[0], A[1], A[2], B[0], B[1], B[2], Cout[0],
                                                         Cout[1], Cout[2], nphys, ntot);
   SPH_LAUNCH_OK();
@@ -241,6 +247,7 @@ int launch_prodvec(const sph_plan* p, const double* const* A, const double* cons
 }
 
 int launch_dirichlet(const sph_plan* p, double2* a, cudaStream_t st) {
+  TimedLaunch tl(p, T_OPS, st);
   dirichlet_kernel<<<ew_blocks(p->nlm), EW_THREADS, 0, st>>>(a, p->nlm, p->N);
   SPH_LAUNCH_OK();
   return SPH_OK;
@@ -255,12 +262,14 @@ int launch_invDl(const sph_plan* p, const double2* phi, double2* w, cudaStream_t
                                           200 * 1024) == cudaSuccess;
   if (!once) return SPH_ECUDA;
   dim3 grid(p->lmax, (p->lmax + 1 + IDL_M - 1) / IDL_M);
+  TimedLaunch tl(p, T_OPS, st);
   invdl_kernel<<<grid, 256, smem, st>>>(phi, w, p->binv, p->d_mbase, p->nlm, p->N);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
 
 int launch_bc_fast_rows(const sph_plan* p, double2* phi, const double2* w, cudaStream_t st) {
+  TimedLaunch tl(p, T_OPS, st);
   bc_fast_kernel<<<ew_blocks(p->nlm), EW_THREADS, 0, st>>>(phi, w, p->d2bor, p->d_ell, p->d_z, p->nlm,
                                                             p->nz, p->N);
   SPH_LAUNCH_OK();
@@ -270,6 +279,7 @@ int launch_bc_fast_rows(const sph_plan* p, double2* phi, const double2* w, cudaS
 int launch_qst_scale(const sph_plan* p, const double2* in, double2* out, int rpow, int lfac, double sc,
                      cudaStream_t st) {
   size_t n = spec_elems(p);
+  TimedLaunch tl(p, T_OPS, st);
   qst_scale_kernel<<<ew_blocks(n), EW_THREADS, 0, st>>>(in, out, p->d_z, p->d_ell, rpow, lfac, sc, p->nlm, n);
   SPH_LAUNCH_OK();
   return SPH_OK;
@@ -279,6 +289,7 @@ int launch_energy(const sph_plan* p, const double* ur, const double* ut, const d
                   cudaStream_t st) {
   size_t n = (size_t)p->nlat * p->nphi * p->N;
   double scale = 0.5 * p->dz * 2.0 * 3.14159265358979323846 / p->nphi;
+  TimedLaunch tl(p, T_OPS, st);
   energy_kernel<<<ew_blocks(n), EW_THREADS, 0, st>>>(ur, ut, up, p->wfull, p->d_z, p->nlat, p->nphi, p->N,
                                                      scale, acc);
   SPH_LAUNCH_OK();

@@ -162,6 +162,7 @@ int launch_phi_fwd(const sph_plan* p, const double* const* grids, int nfields, c
   if (!once) return SPH_ECUDA;
   dim3 grid(p->nlat2 / a.NP, p->nz, nfields);
   size_t smem = (size_t)a.NP * seq_stride(p->nphi) * sizeof(double2);
+  TimedLaunch tl(p, T_PHI_FWD, st);
   phi_fwd_kernel<<<grid, PTHREADS, smem, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;
@@ -182,6 +183,7 @@ int launch_phi_inv(const sph_plan* p, double* const* grids, int nfields, cudaStr
   if (!once) return SPH_ECUDA;
   dim3 grid(p->nlat2 / a.NP, p->nz, nfields);
   size_t smem = (size_t)a.NP * seq_stride(p->nphi) * sizeof(double2);
+  TimedLaunch tl(p, T_PHI_INV, st);
   phi_inv_kernel<<<grid, PTHREADS, smem, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;

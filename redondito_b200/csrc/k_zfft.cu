@@ -171,6 +171,7 @@ int launch_zfft(const sph_plan* p, int mode, const double2* in, double2* out, in
   a.LB = LB;
   int nblocks = (p->nlm + LB - 1) / LB;
   size_t smem = (size_t)LB * p->nz * sizeof(double2) * (mode == Z_DLR ? 2 : 1);
+  TimedLaunch tl(p, T_ZFFT, st);
   switch (mode) {
     case Z_FWD: return launch_mode<Z_FWD>(a, nblocks, smem, st);
     case Z_INV: return launch_mode<Z_INV>(a, nblocks, smem, st);

@@ -141,6 +141,7 @@ static int upload(T** dst, const T* src, size_t n) {
 }
 
 static void plan_free(sph_plan* p) {
+  for (auto e : p->ev_pool) cudaEventDestroy(e);
   void* ptrs[] = {p->P, p->dP, p->mPs, p->wfold, p->wfull, p->d_dir, p->d_z, p->kfac, p->filt,
                   p->zinv2, p->d_ell, p->d_mbase, p->twz, p->twphi, p->twzf, p->twphif, p->revz,
                   p->revphi, p->tilesA,
@@ -375,6 +376,59 @@ extern "C" int sph_grid(const sph_plan* p, double* theta, double* weights, doubl
   return SPH_OK;
 }
 
+// ---------------------------------------------------------------- timers
+int timer_start(const sph_plan* cp, int cls, cudaStream_t st) {
+  sph_plan* p = const_cast<sph_plan*>(cp);
+  if (!p->timing) return -1;
+  int slot = p->ev_used++;
+  while ((int)p->ev_pool.size() < 2 * p->ev_used) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) {
+      p->ev_used--;
+      return -1;
+    }
+    p->ev_pool.push_back(e);
+  }
+  if ((int)p->ev_class.size() < p->ev_used) p->ev_class.resize(p->ev_used);
+  p->ev_class[slot] = cls;
+  cudaEventRecord(p->ev_pool[2 * slot], st);
+  return slot;
+}
+
+void timer_stop(const sph_plan* cp, int slot, cudaStream_t st) {
+  if (slot < 0) return;
+  sph_plan* p = const_cast<sph_plan*>(cp);
+  cudaEventRecord(p->ev_pool[2 * slot + 1], st);
+}
+
+extern "C" int sph_timer_enable(sph_plan* p, int on) {
+  if (!p) return SPH_EINVAL;
+  p->timing = on ? 1 : 0;
+  return SPH_OK;
+}
+
+extern "C" int sph_timer_reset(sph_plan* p) {
+  if (!p) return SPH_EINVAL;
+  p->ev_used = 0;
+  return SPH_OK;
+}
+
+extern "C" int sph_timer_read(sph_plan* p, double* ms, int* launches) {
+  if (!p || !ms || !launches) return SPH_EINVAL;
+  for (int c = 0; c < SPH_NTIMERS; ++c) {
+    ms[c] = 0.0;
+    launches[c] = 0;
+  }
+  for (int i = 0; i < p->ev_used; ++i) {
+    if (cudaEventSynchronize(p->ev_pool[2 * i + 1]) != cudaSuccess) return SPH_ECUDA;
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, p->ev_pool[2 * i], p->ev_pool[2 * i + 1]) != cudaSuccess) return SPH_ECUDA;
+    ms[p->ev_class[i]] += t;
+    launches[p->ev_class[i]] += 1;
+  }
+  return SPH_OK;
+}
+
 // ---------------------------------------------------------------- transforms
 #define ST(s) ((cudaStream_t)(s))
 #define RC(x)                 \
@@ -467,13 +521,13 @@ extern "C" int sph_dlr(sph_plan* p, const double* a, double* b, void* s) {
 extern "C" int sph_saxpby_c(sph_plan* p, double* z, const double* x, double a, const double* y, double b,
                             void* s) {
   if (!p || !z || !x || !y) return SPH_EINVAL;
-  return launch_saxpby(z, x, a, y, b, 2 * spec_elems(p), ST(s));
+  return launch_saxpby(p, z, x, a, y, b, 2 * spec_elems(p), ST(s));
 }
 
 extern "C" int sph_saxpby_r(sph_plan* p, double* z, const double* x, double a, const double* y, double b,
                             void* s) {
   if (!p || !z || !x || !y) return SPH_EINVAL;
-  return launch_saxpby(z, x, a, y, b, grid_elems(p), ST(s));
+  return launch_saxpby(p, z, x, a, y, b, grid_elems(p), ST(s));
 }
 
 extern "C" int sph_fc_filter(sph_plan* p, double* a, char esp, void* s) {
@@ -716,13 +770,13 @@ static int nl_rhs_impl(sph_plan* p, const double2* Z, const double2* W, const do
   // rhs_z = r T_N + nu D_l Z
   RC(launch_multr(p, s2, s4, 1, st));
   RC(launch_zfft(p, Z_DLR, Z, s3, 2, st));
-  RC(launch_saxpby((double*)rz, (const double*)s4, 1.0, (const double*)s3, nu, 2 * spec_elems(p), st));
+  RC(launch_saxpby(p, (double*)rz, (const double*)s4, 1.0, (const double*)s3, nu, 2 * spec_elems(p), st));
   // rhs_phi = (r S_N)' - Q_N + nu D_l phi
   RC(launch_multr(p, s1, s4, 1, st));
   RC(launch_zfft(p, Z_DERIV, s4, s3, 1, st));
-  RC(launch_saxpby((double*)rf, (const double*)s3, 1.0, (const double*)s0, -1.0, 2 * spec_elems(p), st));
+  RC(launch_saxpby(p, (double*)rf, (const double*)s3, 1.0, (const double*)s0, -1.0, 2 * spec_elems(p), st));
   RC(launch_zfft(p, Z_DLR, F, s4, 2, st));
-  RC(launch_saxpby((double*)rf, (const double*)rf, 1.0, (const double*)s4, nu, 2 * spec_elems(p), st));
+  RC(launch_saxpby(p, (double*)rf, (const double*)rf, 1.0, (const double*)s4, nu, 2 * spec_elems(p), st));
   return SPH_OK;
 }
 
@@ -750,8 +804,8 @@ extern "C" int sph_rk3_step(sph_plan* p, double* Z, double* W, double* phi, doub
   for (int o = 3; o >= 1; --o) {
     RC(nl_rhs_impl(p, CD2(Z), CD2(W), CD2(phi), nu, rz, rf, st));
     if (o == 3) SPH_CUDA_OK(cudaMemcpyAsync(e0, p->energy, sizeof(double), cudaMemcpyDeviceToDevice, st));
-    RC(launch_saxpby(Z, (const double*)Z0, 1.0, (const double*)rz, dt / o, 2 * spec_elems(p), st));
-    RC(launch_saxpby(phi, (const double*)F0, 1.0, (const double*)rf, dt / o, 2 * spec_elems(p), st));
+    RC(launch_saxpby(p, Z, (const double*)Z0, 1.0, (const double*)rz, dt / o, 2 * spec_elems(p), st));
+    RC(launch_saxpby(p, phi, (const double*)F0, 1.0, (const double*)rf, dt / o, 2 * spec_elems(p), st));
     RC(sph_v_imposebc(p, Z, phi, W, st));
   }
   if (energy) {

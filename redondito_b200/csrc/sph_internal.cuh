@@ -83,9 +83,26 @@ struct sph_plan {
   double* binv = nullptr;   // [lmax][N-4][N]  M_l column-major per l
   double* d2bor = nullptr;  // [N][4]
   double* energy = nullptr; // device accumulator (1 double)
-  // streams/events owned by the plan
-  cudaEvent_t ev = nullptr;
+  // stage timers (sph_timer_*): event pairs recorded around each launch
+  int timing = 0;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<int> ev_class;  // class of the i-th recorded pair
+  int ev_used = 0;
 };
+
+// Records a start event for kernel class `cls` on `st` when timing is on;
+// returns the slot to close with timer_stop (or -1).
+int timer_start(const sph_plan* p, int cls, cudaStream_t st);
+void timer_stop(const sph_plan* p, int slot, cudaStream_t st);
+
+struct TimedLaunch {
+  const sph_plan* p;
+  int slot;
+  cudaStream_t st;
+  TimedLaunch(const sph_plan* p_, int cls, cudaStream_t st_) : p(p_), slot(timer_start(p_, cls, st_)), st(st_) {}
+  ~TimedLaunch() { timer_stop(p, slot, st); }
+};
+enum { T_PHI_FWD = 0, T_PHI_INV, T_LEG_ANA, T_LEG_SYN, T_VEC_ANA, T_VEC_SYN, T_ZFFT, T_OPS };
 
 static inline size_t spec_elems(const sph_plan* p) { return (size_t)p->nz * p->nlm; }
 static inline size_t grid_elems(const sph_plan* p) { return (size_t)p->nz * p->nphi * p->nlat; }
@@ -123,8 +140,8 @@ int launch_kmul(const sph_plan* p, const double2* a, double2* b, int order, cuda
 int launch_filter_k(const sph_plan* p, double2* a, cudaStream_t st);
 int launch_laplang(const sph_plan* p, const double2* a, double2* b, cudaStream_t st);
 int launch_multr(const sph_plan* p, const double2* a, double2* b, int power, cudaStream_t st);
-int launch_saxpby(double* z, const double* x, double a, const double* y, double b, size_t n,
-                  cudaStream_t st);
+int launch_saxpby(const sph_plan* p, double* z, const double* x, double a, const double* y, double b,
+                  size_t n, cudaStream_t st);
 int launch_prodvec(const sph_plan* p, const double* const* A, const double* const* B,
                    double* const* Cout, cudaStream_t st);
 int launch_dirichlet(const sph_plan* p, double2* a, cudaStream_t st);

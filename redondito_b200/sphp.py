@@ -44,7 +44,10 @@ SYMBOLS = (
     "sph_fc_filter", "sph_copy", "sph_prodvec",
     "sph_setup_bc", "sph_dirichlet", "sph_invDl", "sph_v_imposebc", "sph_v_imposebc_fast",
     "sph_nl_rhs", "sph_rk3_step",
+    "sph_timer_enable", "sph_timer_reset", "sph_timer_read",
 )
+TIMER_CLASSES = ("phi_fwd", "phi_inv", "leg_analysis", "leg_synthesis", "vec_analysis",
+                 "vec_synthesis", "zfft", "ops")
 
 
 class SphError(RuntimeError):
@@ -98,6 +101,9 @@ def lib(build_if_missing=True):
             "sph_v_imposebc_fast": [P, Vp, Vp, Vp, Vp],
             "sph_nl_rhs": [P, Vp, Vp, Vp, D, Vp, Vp, pD, Vp],
             "sph_rk3_step": [P, Vp, Vp, Vp, D, D, pD, Vp],
+            "sph_timer_enable": [P, I],
+            "sph_timer_reset": [P],
+            "sph_timer_read": [P, pD, pI],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -326,3 +332,20 @@ def rk3_step(plan, Z, W, phi, nu, dt, stream=None, energy=True):
     _call("sph_rk3_step", plan.h, _s(plan, Z), _s(plan, W), _s(plan, phi), float(nu), float(dt),
           ctypes.byref(e) if energy else None, _stream(stream))
     return e.value
+
+
+# ---------------------------------------------------------------- timers
+def timer_enable(plan, on=True):
+    _call("sph_timer_enable", plan.h, int(bool(on)))
+
+
+def timer_reset(plan):
+    _call("sph_timer_reset", plan.h)
+
+
+def timer_read(plan):
+    """{class: (milliseconds, launches)} accumulated since the last reset."""
+    ms = (ctypes.c_double * len(TIMER_CLASSES))()
+    n = (ctypes.c_int * len(TIMER_CLASSES))()
+    _call("sph_timer_read", plan.h, ms, n)
+    return {c: (ms[i], n[i]) for i, c in enumerate(TIMER_CLASSES)}

@@ -14,6 +14,8 @@ pytestmark = pytest.mark.gpu
 
 TOL = 1e-12
 TOL_CONT = 1e-11
+# second radial derivatives multiply the continuation's round-off by kz^2
+TOL_D2 = 1e-10
 
 
 def _pair(lmax, nz, C=0, d=0, nlat=None, nphi=None, rint=0.35, rext=1.0):
@@ -133,17 +135,17 @@ def pseudo():
 
 def test_derivr_ops(pseudo):
     S, P, G, a = pseudo
-    for order in (1, 2):
+    for order, tol in ((1, TOL_CONT), (2, TOL_D2)):
         b = G.new_spec()
         S.derivr(G, dev(a), b, order, "r")
-        assert rel_l2(host(b), P.derivr(a, order)) < TOL_CONT
+        assert rel_l2(host(b), P.derivr(a, order)) < tol
     ak = P.z_forward(a)
     b = G.new_spec()
     S.derivr(G, dev(ak), b, 1, "k")
     assert rel_l2(host(b), P.derivr(ak, 1, "k")) < TOL
     b = G.new_spec()
     S.dlr(G, dev(a), b)
-    assert rel_l2(host(b), P.dlr(a)) < TOL_CONT
+    assert rel_l2(host(b), P.dlr(a)) < TOL_D2
 
 
 def test_pointwise_ops(pseudo):
@@ -197,12 +199,12 @@ def test_boundary(pseudo):
     S.v_imposebc(G, T, F, W)
     assert rel_l2(host(T), t_ref) == 0.0
     assert rel_l2(host(W), w_ref) < TOL_CONT
-    assert rel_l2(host(F), f_ref) < TOL_CONT
+    assert rel_l2(host(F), f_ref) < TOL_D2
     t_ref, f_ref, w_ref = P.imposebc(tor, phi, fast=True)
     T, F, W = dev(tor), dev(phi), G.new_spec()
     S.v_imposebc_fast(G, T, F, W)
     assert rel_l2(host(W), w_ref) < TOL_CONT
-    assert rel_l2(host(F), f_ref) < TOL_CONT
+    assert rel_l2(host(F), f_ref) < TOL_D2
 
 
 def test_nl_rhs_and_rk3():
@@ -218,12 +220,12 @@ def test_nl_rhs_and_rk3():
     rz, rf = G.new_spec(), G.new_spec()
     e = S.nl_rhs(G, dev(Z), dev(W), dev(phi), 1e-3, rz, rf)
     assert abs(e - e_ref) / e_ref < 1e-12
-    assert rel_l2(host(rz), rz_ref) < TOL_CONT
-    assert rel_l2(host(rf), rf_ref) < TOL_CONT
+    assert rel_l2(host(rz), rz_ref) < TOL_D2
+    assert rel_l2(host(rf), rf_ref) < TOL_D2
     Zr, Wr, Fr, e_ref = P.rk3_step(Z, W, phi, 1e-3, 1e-4)
     Zg, Wg, Fg = dev(Z), dev(W), dev(phi)
     e = S.rk3_step(G, Zg, Wg, Fg, 1e-3, 1e-4)
     assert abs(e - e_ref) / e_ref < 1e-12
-    assert rel_l2(host(Zg), Zr) < TOL_CONT
-    assert rel_l2(host(Wg), Wr) < TOL_CONT
-    assert rel_l2(host(Fg), Fr) < TOL_CONT
+    assert rel_l2(host(Zg), Zr) < TOL_D2
+    assert rel_l2(host(Wg), Wr) < TOL_D2
+    assert rel_l2(host(Fg), Fr) < TOL_D2
