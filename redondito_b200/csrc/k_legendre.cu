@@ -3,45 +3,45 @@
 // The reference does these inside SHTns, one plane at a time (spat_to_SH /
 // SH_to_spat / spat_to_SHqst / SHqst_to_spat at src/sphp/sphp_sca.F90:312,485
 // and src/sphp/sphp_vec.F90:89-91,157-159).  Here every plane and field is a
-// column of one GEMM per m, so the Legendre table tile is loaded once per
-// (m, l-block) for all nz planes:
-//   analysis   a[l][n] = sum_i  Pbar_lm(x_i) G_par(l)[i][n]      (K = nlat/2)
-//   synthesis  S_q[i][n] = sum_{l: (l-m)%2 = q} Pbar_lm(x_i) a[l][n]  (K = lmax+1-m)
-// with n = (plane, re/im) and the even/odd folding of mirror rings halving K.
-// FP64 tiles run on the DMMA pipe through mma.sync.m8n8k4.f64.
+// column of one GEMM per m, so each Legendre table tile is read once per
+// (m, row block) for all nz planes:
+//   analysis   a[l][n]   = sum_i Pbar_lm(x_i) G_(l-m)%2[i][n]          K = nlat/2
+//   synthesis  S_q[i][n] = sum_{l: (l-m)%2 = q} Pbar_lm(x_i) a[l][n]    K = lmax+1-m
+// with n = (plane, re/im); folding mirror rings into even/odd parts halves K.
+// The vector transforms fold their complex factors into the operand loads:
+//   S_l  = 1/(l(l+1)) sum_i [ dP_l Vt_(1-p) + mPs_l (-i Vp_p) ]
+//   T_l  = 1/(l(l+1)) sum_i [ mPs_l (-i Vt_p) - dP_l Vp_(1-p) ]
+//   Vt_q = sum_(p=1-q) dP_l S_l + sum_(p=q) mPs_l (i T_l)
+//   Vp_q = sum_(p=1-q) dP_l (-T_l) + sum_(p=q) mPs_l (i S_l)
+// (p = (l-m)%2, fold 0 = F(i)+F(mirror), fold 1 = F(i)-F(mirror); Pbar has
+// the parity of p, dPbar the opposite), so each output is one accumulator
+// over a K twice as long.
+//
+// Every kernel streams its tiles through a 3-stage cp.async pipeline into
+// padded shared memory (conflict-free fragment loads) and runs FP64
+// mma.sync.m8n8k4 on the DMMA pipe; output tiles are staged through shared
+// memory so global writes are contiguous rows.
 #include "sph_internal.cuh"
 
 namespace {
 
-// D (8x8) += A (8x4, row) * B (4x8, col), FP64.  Fragments: a = A[g][t],
-// b = B[t][g], c = {C[g][2t], C[g][2t+1]}, g = lane/4, t = lane%4.
+// ---------------------------------------------------------------- primitives
 __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                : "+d"(c[0]), "+d"(c[1])
                : "d"(a), "d"(b));
 }
 
-// Warp tile (8*MT) x (8*NT) += A (8*MT x K) * B (K x 8*NT) from shared memory.
-// A_KMAJOR: A stored as As[k*lda + row], else As[row*lda + k].
-// B_NMAJOR: B stored as Bs[col*ldb + k], else Bs[k*ldb + col].
-template <int MT, int NT, bool A_KMAJOR, bool B_NMAJOR>
-__device__ __forceinline__ void warp_mma(double (&acc)[MT][NT][2], const double* As, int lda,
-                                         const double* Bs, int ldb, int K) {
-  const int lane = threadIdx.x & 31;
-  const int g = lane >> 2, t = lane & 3;
-  for (int k0 = 0; k0 < K; k0 += 4) {
-    double a[MT], b[NT];
-#pragma unroll
-    for (int mt = 0; mt < MT; ++mt)
-      a[mt] = A_KMAJOR ? As[(k0 + t) * lda + mt * 8 + g] : As[(mt * 8 + g) * lda + k0 + t];
-#pragma unroll
-    for (int nt = 0; nt < NT; ++nt)
-      b[nt] = B_NMAJOR ? Bs[(nt * 8 + g) * ldb + k0 + t] : Bs[(k0 + t) * ldb + nt * 8 + g];
-#pragma unroll
-    for (int mt = 0; mt < MT; ++mt)
-#pragma unroll
-      for (int nt = 0; nt < NT; ++nt) dmma(acc[mt][nt], a[mt], b[nt]);
-  }
+// 16-byte global->shared copy; pred == false fills zeros (no global read).
+__device__ __forceinline__ void cp16(void* smem, const void* gmem, bool pred) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int sz = pred ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
 template <int MT, int NT>
@@ -52,303 +52,436 @@ __device__ __forceinline__ void zero_acc(double (&acc)[MT][NT][2]) {
     for (int nt = 0; nt < NT; ++nt) acc[mt][nt][0] = acc[mt][nt][1] = 0.0;
 }
 
+// B-operand forms applied at fragment-load time to an interleaved complex
+// column pair (column 2k = re, 2k+1 = im of the same value v):
+//   PLAIN: v    NEG: -v    MULI: i v    MULMI: -i v
+enum BForm { PLAIN = 0, NEG = 1, MULI = 2, MULMI = 3 };
+
+// Fragment b for column n of a complex operand stored as doubles where the
+// (re, im) pair of column n>>1 sits at base[0], base[1].
+template <int FORM>
+__device__ __forceinline__ double bform(const double* pair, int c) {
+  if (FORM == PLAIN) return pair[c];
+  if (FORM == NEG) return -pair[c];
+  if (FORM == MULI) return c ? pair[0] : -pair[1];  // (i v).re = -v.im, (i v).im = v.re
+  return c ? -pair[0] : pair[1];                    // (-i v).re = v.im, (-i v).im = -v.re
+}
+
 struct LegArgs {
-  const double* P;     // [nlm][nlat2]
-  const double* dP;    // [nlm][nlat2]
-  const double* mPs;   // [nlm][nlat2]
-  const double2* G;    // folded coefficients, field 0 (read)
-  double2* Gw;         // folded coefficients (written by synthesis)
+  const double* P;     // [nlm][ldn]
+  const double* dP;    // [nlm][ldn]
+  const double* mPs;   // [nlm][ldn]
+  const double2* G;    // folded coefficients [field][m][2][nz][ldn]
+  double2* Gw;
   size_t Gfield;
-  int gfield;          // which G field
-  const double2* spec; // (nz, nlm) input (synthesis)
+  int gfield;
+  const double2* spec;  // (nz, nlm)
   const double2* spec2;
-  double2* out;        // (nz, nlm) output (analysis)
+  double2* out;
   double2* out2;
   const LegTile* tiles;
   const int* mbase;
-  int lmax, nlat2, nz, nlm;
+  int lmax, ldn, nz, nlm;
 };
 
-// ---------------------------------------------------------------- scalar analysis
-// CTA: 64 consecutive l (32 even-offset rows, 32 odd) x 64 columns (32 planes).
-constexpr int AT_L = 64, AT_N = 64, AT_K = 16, AT_LDA = AT_K + 4, AT_LDB = AT_K + 4;
+constexpr int STAGES = 3;
+
+// ================================================================ scalar analysis
+// CTA: 64 consecutive l (rows split by parity, 32 each) x 32 planes (64
+// columns); K tile 16 nodes.  4 warps = (parity, column half), 32x32 each.
+namespace an {
+constexpr int L = 64, KZ = 32, K = 16, LDA = K + 4, LDB = K + 4;  // LDB in complex units
+constexpr int A_SZ = 2 * 32 * LDA;          // doubles
+constexpr int B_SZ = 2 * KZ * LDB * 2;      // doubles
+constexpr int STAGE = A_SZ + B_SZ;
+constexpr int SMEM = STAGES * STAGE * 8;
+}  // namespace an
 
 __global__ void __launch_bounds__(128) leg_analysis_kernel(LegArgs a) {
-  __shared__ __align__(16) double smem[2 * 32 * AT_LDA + 2 * AT_N * AT_LDB > 32 * 64 * 2
-                                           ? 2 * 32 * AT_LDA + 2 * AT_N * AT_LDB
-                                           : 32 * 64 * 2];
-  double* As = smem;                    // [par][32][AT_LDA]
-  double* Bs = smem + 2 * 32 * AT_LDA;  // [par][AT_N][AT_LDB]  (N-major)
+  using namespace an;
+  extern __shared__ __align__(16) double sm[];
   const LegTile tile = a.tiles[blockIdx.x];
   const int m = tile.m, l0 = tile.r0;
-  const int n0 = blockIdx.y * AT_N;  // column = 2*plane + re/im
-  const int kz0 = n0 / 2;
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int kz0 = blockIdx.y * KZ;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
   const int par = warp >> 1, nh = warp & 1;
-  const double2* G = a.G + (size_t)a.gfield * a.Gfield;
+  const double2* G = a.G + (size_t)a.gfield * a.Gfield + (size_t)m * 2 * a.nz * a.ldn;
   const size_t base_lm = (size_t)a.mbase[m] - m;
+  const int nk = (a.ldn + K - 1) / K;
+
+  auto load = [&](int st, int k0) {
+    double* As = sm + st * STAGE;
+    double* Bs = As + A_SZ;
+    for (int c = tid; c < L * (K / 2); c += 128) {  // A: 64 rows x 8 chunks
+      int row = c >> 3, cc = c & 7;
+      int l = l0 + row, i = k0 + 2 * cc;
+      bool ok = l <= a.lmax && i < a.ldn;
+      const double* src = ok ? a.P + (base_lm + l) * a.ldn + i : a.P;
+      cp16(As + ((row & 1) * 32 + (row >> 1)) * LDA + 2 * cc, src, ok);
+    }
+    for (int c = tid; c < 2 * KZ * K; c += 128) {  // B: [par][plane][node] complex
+      int i_ = c % K, r = c / K, kzl = r % KZ, pr = r / KZ;
+      int kz = kz0 + kzl, i = k0 + i_;
+      bool ok = kz < a.nz && i < a.ldn;
+      const double2* src = ok ? G + ((size_t)pr * a.nz + kz) * a.ldn + i : a.G;
+      cp16(Bs + ((pr * KZ + kzl) * LDB + i_) * 2, src, ok);
+    }
+  };
 
   double acc[4][4][2];
   zero_acc(acc);
-
-  for (int k0 = 0; k0 < a.nlat2; k0 += AT_K) {
-    // A: rows l0 .. l0+63, nodes k0 .. k0+15 (row-major per parity)
-    for (int idx = tid; idx < AT_L * AT_K; idx += 128) {
-      int row = idx / AT_K, kk = idx - row * AT_K;
-      int l = l0 + row, i = k0 + kk;
-      double v = (l <= a.lmax && i < a.nlat2) ? __ldg(a.P + (base_lm + l) * a.nlat2 + i) : 0.0;
-      As[((row & 1) * 32 + (row >> 1)) * AT_LDA + kk] = v;
-    }
-    // B: G[m][par][plane][node] -> Bs[par][2*plane + c][node]
-    for (int idx = tid; idx < 2 * (AT_N / 2) * AT_K; idx += 128) {
-      int kk = idx % AT_K, rest = idx / AT_K;
-      int pl = rest % (AT_N / 2), pr = rest / (AT_N / 2);
-      int kz = kz0 + pl, i = k0 + kk;
-      double2 v = make_double2(0.0, 0.0);
-      if (kz < a.nz && i < a.nlat2) v = G[(((size_t)m * 2 + pr) * a.nz + kz) * a.nlat2 + i];
-      Bs[(pr * AT_N + 2 * pl) * AT_LDB + kk] = v.x;
-      Bs[(pr * AT_N + 2 * pl + 1) * AT_LDB + kk] = v.y;
-    }
-    __syncthreads();
-    warp_mma<4, 4, false, true>(acc, As + par * 32 * AT_LDA, AT_LDA,
-                                Bs + (par * AT_N + nh * 32) * AT_LDB, AT_LDB, AT_K);
-    __syncthreads();
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < nk) load(s, s * K);
+    cp_commit();
   }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_wait<STAGES - 2>();
+    __syncthreads();
+    const double* As = sm + (kt % STAGES) * STAGE + par * 32 * LDA;
+    const double* Bs = sm + (kt % STAGES) * STAGE + A_SZ + (par * KZ + nh * 16) * LDB * 2;
+#pragma unroll
+    for (int k0 = 0; k0 < K; k0 += 4) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt) av[mt] = As[(mt * 8 + g) * LDA + k0 + t];
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) bv[nt] = Bs[((nt * 4 + (g >> 1)) * LDB + k0 + t) * 2 + (g & 1)];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) dmma(acc[mt][nt], av[mt], bv[nt]);
+    }
+    int nx = kt + STAGES - 1;
+    if (nx < nk) load(nx % STAGES, nx * K);
+    cp_commit();
+  }
+  cp_wait<0>();
+  __syncthreads();
 
-  // stage C through shared memory: Cs[plane][l] (double2), then contiguous rows
-  double2* Cs = reinterpret_cast<double2*>(smem);  // [32 planes][64 l]
-  const int lane = tid & 31, g = lane >> 2, t = lane & 3;
+  // Cs[plane][l] then contiguous rows of the (nz, nlm) output
+  double2* Cs = reinterpret_cast<double2*>(sm);
 #pragma unroll
   for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
     for (int nt = 0; nt < 4; ++nt) {
-      int row = mt * 8 + g;             // row within parity
-      int col = nh * 32 + nt * 8 + 2 * t;  // even column -> (re, im) of one plane
-      int lloc = 2 * row + par;
-      Cs[(col >> 1) * AT_L + lloc] = make_double2(acc[mt][nt][0], acc[mt][nt][1]);
+      int row = mt * 8 + g;
+      int pl = nh * 16 + nt * 4 + t;
+      Cs[pl * L + 2 * row + par] = make_double2(acc[mt][nt][0], acc[mt][nt][1]);
     }
   __syncthreads();
-  const int nvalid = min(AT_L, a.lmax + 1 - l0);
-  for (int idx = tid; idx < (AT_N / 2) * AT_L; idx += 128) {
-    int pl = idx / AT_L, ll = idx - pl * AT_L;
+  const int nvalid = min(L, a.lmax + 1 - l0);
+  for (int idx = tid; idx < KZ * L; idx += 128) {
+    int pl = idx / L, ll = idx - pl * L;
     int kz = kz0 + pl;
     if (kz >= a.nz || ll >= nvalid) continue;
     double2 v = Cs[idx];
-    if (m == 0) v.y = 0.0;  // m = 0 coefficients are real
+    if (m == 0) v.y = 0.0;  // m = 0 coefficients of a real field are real
     a.out[(size_t)kz * a.nlm + base_lm + l0 + ll] = v;
   }
 }
 
-// ---------------------------------------------------------------- scalar synthesis
-// CTA: 64 nodes x 64 columns, both parities; K loop over l in steps of 16
-// (8 per parity).  8 warps: (parity, node half, column half), 32x32 each.
-constexpr int ST_I = 64, ST_N = 64, ST_K = 16, ST_LDA = ST_I + 4, ST_LDB = ST_N + 4;
+// ================================================================ scalar synthesis
+// CTA: 64 nodes x 32 planes; K tile 16 consecutive l (8 per parity).
+// 8 warps = (parity, node half, column half), 32x32 each.
+namespace sy {
+constexpr int I = 64, KZ = 32, K = 16, LDA = I + 4, LDB = 2 * KZ + 4;
+constexpr int A_SZ = K * LDA, B_SZ = K * LDB;
+constexpr int STAGE = A_SZ + B_SZ;
+constexpr int SMEM = STAGES * STAGE * 8;
+}  // namespace sy
 
 __global__ void __launch_bounds__(256) leg_synthesis_kernel(LegArgs a) {
-  __shared__ __align__(16) double As[2 * (ST_K / 2) * ST_LDA];  // [par][q][node]  K-major
-  __shared__ __align__(16) double Bs[2 * (ST_K / 2) * ST_LDB];  // [par][q][col]   K x N
+  using namespace sy;
+  extern __shared__ __align__(16) double sm[];
   const LegTile tile = a.tiles[blockIdx.x];
   const int m = tile.m, i0 = tile.r0;
-  const int n0 = blockIdx.y * ST_N, kz0 = n0 / 2;
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int kz0 = blockIdx.y * KZ;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
   const int par = warp >> 2, mh = (warp >> 1) & 1, nh = warp & 1;
   const size_t base_lm = (size_t)a.mbase[m] - m;
+  const int nk = (a.lmax + 1 - m + K - 1) / K;
+
+  auto load = [&](int st, int lk) {
+    double* As = sm + st * STAGE;  // [par][q][node]  (K-major)
+    double* Bs = As + A_SZ;        // [par][q][col]   (K x N)
+    for (int c = tid; c < K * (I / 2); c += 256) {
+      int cc = c % (I / 2), q = c / (I / 2);
+      int l = lk + q, i = i0 + 2 * cc;
+      bool ok = l <= a.lmax && i < a.ldn;
+      const double* src = ok ? a.P + (base_lm + l) * a.ldn + i : a.P;
+      cp16(As + ((q & 1) * (K / 2) + (q >> 1)) * LDA + 2 * cc, src, ok);
+    }
+    for (int c = tid; c < K * KZ; c += 256) {
+      int q = c % K, pl = c / K;
+      int l = lk + q, kz = kz0 + pl;
+      bool ok = l <= a.lmax && kz < a.nz;
+      const double2* src = ok ? a.spec + (size_t)kz * a.nlm + base_lm + l : a.spec;
+      cp16(Bs + ((q & 1) * (K / 2) + (q >> 1)) * LDB + 2 * pl, src, ok);
+    }
+  };
 
   double acc[4][4][2];
   zero_acc(acc);
-
-  for (int lk = m; lk <= a.lmax; lk += ST_K) {
-    for (int idx = tid; idx < ST_K * ST_I; idx += 256) {
-      int q = idx / ST_I, ii = idx - q * ST_I;
-      int l = lk + q, i = i0 + ii;
-      double v = (l <= a.lmax && i < a.nlat2) ? __ldg(a.P + (base_lm + l) * a.nlat2 + i) : 0.0;
-      As[((q & 1) * (ST_K / 2) + (q >> 1)) * ST_LDA + ii] = v;
-    }
-    for (int idx = tid; idx < (ST_N / 2) * ST_K; idx += 256) {
-      int q = idx % ST_K, pl = idx / ST_K;
-      int l = lk + q, kz = kz0 + pl;
-      double2 v = make_double2(0.0, 0.0);
-      if (l <= a.lmax && kz < a.nz) v = a.spec[(size_t)kz * a.nlm + base_lm + l];
-      if (m == 0) v.y = 0.0;  // only Re a_l0 enters a real field
-      double* row = Bs + ((q & 1) * (ST_K / 2) + (q >> 1)) * ST_LDB;
-      row[2 * pl] = v.x;
-      row[2 * pl + 1] = v.y;
-    }
-    __syncthreads();
-    warp_mma<4, 4, true, false>(acc, As + par * (ST_K / 2) * ST_LDA + mh * 32, ST_LDA,
-                                Bs + par * (ST_K / 2) * ST_LDB + nh * 32, ST_LDB, ST_K / 2);
-    __syncthreads();
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < nk) load(s, m + s * K);
+    cp_commit();
   }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_wait<STAGES - 2>();
+    __syncthreads();
+    const double* As = sm + (kt % STAGES) * STAGE + par * (K / 2) * LDA + mh * 32;
+    const double* Bs = sm + (kt % STAGES) * STAGE + A_SZ + par * (K / 2) * LDB + nh * 32;
+#pragma unroll
+    for (int k0 = 0; k0 < K / 2; k0 += 4) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt) av[mt] = As[(k0 + t) * LDA + mt * 8 + g];
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) bv[nt] = Bs[(k0 + t) * LDB + nt * 8 + g];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) dmma(acc[mt][nt], av[mt], bv[nt]);
+    }
+    int nx = kt + STAGES - 1;
+    if (nx < nk) load(nx % STAGES, m + nx * K);
+    cp_commit();
+  }
+  cp_wait<0>();
 
-  double2* G = a.Gw + (size_t)a.gfield * a.Gfield;
-  const int lane = tid & 31, g = lane >> 2, t = lane & 3;
+  double2* G = a.Gw + (size_t)a.gfield * a.Gfield + ((size_t)m * 2 + par) * a.nz * a.ldn;
 #pragma unroll
   for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
     for (int nt = 0; nt < 4; ++nt) {
       int i = i0 + mh * 32 + mt * 8 + g;
-      int kz = kz0 + (nh * 32 + nt * 8 + 2 * t) / 2;
-      if (i < a.nlat2 && kz < a.nz)
-        G[(((size_t)m * 2 + par) * a.nz + kz) * a.nlat2 + i] = make_double2(acc[mt][nt][0], acc[mt][nt][1]);
+      int kz = kz0 + nh * 16 + nt * 4 + t;
+      if (i < a.ldn && kz < a.nz) G[(size_t)kz * a.ldn + i] = make_double2(acc[mt][nt][0], acc[mt][nt][1]);
     }
 }
 
-// ---------------------------------------------------------------- vector analysis
-// S_l = 1/(l(l+1)) sum_i [dP_l Vt_(1-p) - i mPs_l Vp_p]
-// T_l = 1/(l(l+1)) sum_i [-i mPs_l Vt_p - dP_l Vp_(1-p)]
-// (p = (l-m)%2; fold 0 = F(i)+F(mirror), fold 1 = F(i)-F(mirror);
-//  Pbar has the parity of p, dPbar the opposite.)
-// CTA: 32 consecutive l (16 per parity) x 64 columns; 4 warps (parity, half).
-constexpr int VA_L = 32, VA_N = 64, VA_K = 16, VA_LDA = VA_K + 4, VA_LDB = VA_K + 4;
+// ================================================================ vector analysis
+// CTA: 64 consecutive l x 32 planes; K tile 8 nodes.  8 warps =
+// (parity, output S/T, column half), 32x32 each.  Each output is one
+// accumulator over the dP block (nodes x Vt/Vp fold 1-p) and the mPs block
+// (nodes x Vt/Vp fold p).
+namespace va {
+constexpr int L = 64, KZ = 32, K = 8, LDA = K + 4, LDB = K + 4;  // LDB complex units
+constexpr int A_SZ = 2 * 2 * 32 * LDA;   // [table][par][row][k]
+constexpr int B_SZ = 2 * 2 * KZ * LDB * 2;  // [field][fold][plane][k] complex
+constexpr int STAGE = A_SZ + B_SZ;
+constexpr int SMEM = STAGES * STAGE * 8;
+}  // namespace va
 
-__global__ void __launch_bounds__(128) vec_analysis_kernel(LegArgs a) {
-  extern __shared__ __align__(16) double vsm[];
-  double* Ad = vsm;                          // dP   [par][16][VA_LDA]
-  double* Am = Ad + 2 * 16 * VA_LDA;         // mPs  [par][16][VA_LDA]
-  double* Bt = Am + 2 * 16 * VA_LDA;         // Vt   [fold][VA_N][VA_LDB]
-  double* Bp = Bt + 2 * VA_N * VA_LDB;       // Vp   [fold][VA_N][VA_LDB]
+template <int FORM>
+__device__ __forceinline__ void mma_block_nmaj(double (&acc)[4][4][2], const double* As, int lda,
+                                               const double* Bs, int ldbc, int g, int t) {
+#pragma unroll
+  for (int k0 = 0; k0 < 8; k0 += 4) {
+    double av[4], bv[4];
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt) av[mt] = As[(mt * 8 + g) * lda + k0 + t];
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) bv[nt] = bform<FORM>(Bs + ((nt * 4 + (g >> 1)) * ldbc + k0 + t) * 2, g & 1);
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) dmma(acc[mt][nt], av[mt], bv[nt]);
+  }
+}
+
+__global__ void __launch_bounds__(256) vec_analysis_kernel(LegArgs a) {
+  using namespace va;
+  extern __shared__ __align__(16) double sm[];
   const LegTile tile = a.tiles[blockIdx.x];
   const int m = tile.m, l0 = tile.r0;
-  const int n0 = blockIdx.y * VA_N, kz0 = n0 / 2;
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int par = warp >> 1, nh = warp & 1;
+  const int kz0 = blockIdx.y * KZ;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+  const int par = warp >> 2, outT = (warp >> 1) & 1, nh = warp & 1;
   const size_t base_lm = (size_t)a.mbase[m] - m;
-  const double2* Gt = a.G + (size_t)1 * a.Gfield;  // field 1: v_theta
-  const double2* Gp = a.G + (size_t)2 * a.Gfield;  // field 2: v_phi
+  const size_t moff = (size_t)m * 2 * a.nz * a.ldn;
+  const double2* Gt = a.G + 1 * a.Gfield + moff;  // v_theta
+  const double2* Gp = a.G + 2 * a.Gfield + moff;  // v_phi
+  const int nk = (a.ldn + K - 1) / K;
 
-  double x1[2][4][2], x2[2][4][2], x3[2][4][2], x4[2][4][2];
-  zero_acc(x1); zero_acc(x2); zero_acc(x3); zero_acc(x4);
+  auto load = [&](int st, int k0) {
+    double* As = sm + st * STAGE;
+    double* Bs = As + A_SZ;
+    for (int c = tid; c < 2 * L * (K / 2); c += 256) {  // 2 tables x 64 rows x 4 chunks
+      int cc = c & 3, r = c >> 2, row = r % L, tb = r / L;
+      int l = l0 + row, i = k0 + 2 * cc;
+      bool ok = l <= a.lmax && i < a.ldn;
+      const double* tab = tb ? a.mPs : a.dP;
+      const double* src = ok ? tab + (base_lm + l) * a.ldn + i : a.dP;
+      cp16(As + ((tb * 2 + (row & 1)) * 32 + (row >> 1)) * LDA + 2 * cc, src, ok);
+    }
+    for (int c = tid; c < 2 * 2 * KZ * K; c += 256) {  // 2 fields x 2 folds x 32 planes x 8 nodes
+      int i_ = c % K, r = c / K, kzl = r % KZ, r2 = r / KZ, fo = r2 & 1, fl = r2 >> 1;
+      int kz = kz0 + kzl, i = k0 + i_;
+      bool ok = kz < a.nz && i < a.ldn;
+      const double2* Gf = fl ? Gp : Gt;
+      const double2* src = ok ? Gf + ((size_t)fo * a.nz + kz) * a.ldn + i : a.G;
+      cp16(Bs + (((fl * 2 + fo) * KZ + kzl) * LDB + i_) * 2, src, ok);
+    }
+  };
 
-  for (int k0 = 0; k0 < a.nlat2; k0 += VA_K) {
-    for (int idx = tid; idx < VA_L * VA_K; idx += 128) {
-      int row = idx / VA_K, kk = idx - row * VA_K;
-      int l = l0 + row, i = k0 + kk;
-      bool ok = (l <= a.lmax && i < a.nlat2);
-      size_t off = (base_lm + l) * a.nlat2 + i;
-      int so = ((row & 1) * 16 + (row >> 1)) * VA_LDA + kk;
-      Ad[so] = ok ? __ldg(a.dP + off) : 0.0;
-      Am[so] = ok ? __ldg(a.mPs + off) : 0.0;
-    }
-    for (int idx = tid; idx < 2 * (VA_N / 2) * VA_K; idx += 128) {
-      int kk = idx % VA_K, rest = idx / VA_K;
-      int pl = rest % (VA_N / 2), fo = rest / (VA_N / 2);
-      int kz = kz0 + pl, i = k0 + kk;
-      double2 vt = make_double2(0.0, 0.0), vp = vt;
-      if (kz < a.nz && i < a.nlat2) {
-        size_t off = (((size_t)m * 2 + fo) * a.nz + kz) * a.nlat2 + i;
-        vt = Gt[off];
-        vp = Gp[off];
-      }
-      Bt[(fo * VA_N + 2 * pl) * VA_LDB + kk] = vt.x;
-      Bt[(fo * VA_N + 2 * pl + 1) * VA_LDB + kk] = vt.y;
-      Bp[(fo * VA_N + 2 * pl) * VA_LDB + kk] = vp.x;
-      Bp[(fo * VA_N + 2 * pl + 1) * VA_LDB + kk] = vp.y;
-    }
-    __syncthreads();
-    const double* ad = Ad + par * 16 * VA_LDA;
-    const double* am = Am + par * 16 * VA_LDA;
-    const int cofs = nh * 32;
-    warp_mma<2, 4, false, true>(x1, ad, VA_LDA, Bt + ((1 - par) * VA_N + cofs) * VA_LDB, VA_LDB, VA_K);
-    warp_mma<2, 4, false, true>(x2, am, VA_LDA, Bp + (par * VA_N + cofs) * VA_LDB, VA_LDB, VA_K);
-    warp_mma<2, 4, false, true>(x3, ad, VA_LDA, Bp + ((1 - par) * VA_N + cofs) * VA_LDB, VA_LDB, VA_K);
-    warp_mma<2, 4, false, true>(x4, am, VA_LDA, Bt + (par * VA_N + cofs) * VA_LDB, VA_LDB, VA_K);
-    __syncthreads();
+  double acc[4][4][2];
+  zero_acc(acc);
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < nk) load(s, s * K);
+    cp_commit();
   }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_wait<STAGES - 2>();
+    __syncthreads();
+    const double* As = sm + (kt % STAGES) * STAGE;
+    const double* Bs = As + A_SZ;
+    const double* Ad = As + ((0 * 2 + par) * 32) * LDA;  // dP rows of this parity
+    const double* Am = As + ((1 * 2 + par) * 32) * LDA;  // mPs rows
+    auto B = [&](int fl, int fo) { return Bs + ((fl * 2 + fo) * KZ + nh * 16) * LDB * 2; };
+    if (!outT) {
+      // S: dP x Vt_(1-p)  +  mPs x (-i Vp_p)
+      mma_block_nmaj<PLAIN>(acc, Ad, LDA, B(0, 1 - par), LDB, g, t);
+      mma_block_nmaj<MULMI>(acc, Am, LDA, B(1, par), LDB, g, t);
+    } else {
+      // T: mPs x (-i Vt_p)  -  dP x Vp_(1-p)
+      mma_block_nmaj<MULMI>(acc, Am, LDA, B(0, par), LDB, g, t);
+      mma_block_nmaj<NEG>(acc, Ad, LDA, B(1, 1 - par), LDB, g, t);
+    }
+    int nx = kt + STAGES - 1;
+    if (nx < nk) load(nx % STAGES, nx * K);
+    cp_commit();
+  }
+  cp_wait<0>();
+  __syncthreads();
 
-  const int lane = tid & 31, g = lane >> 2, t = lane & 3;
+  double2* Cs = reinterpret_cast<double2*>(sm);  // [out][plane][l]
 #pragma unroll
-  for (int mt = 0; mt < 2; ++mt)
+  for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
     for (int nt = 0; nt < 4; ++nt) {
       int row = mt * 8 + g;
-      int l = l0 + 2 * row + par;
-      int kz = kz0 + (nh * 32 + nt * 8 + 2 * t) / 2;
-      if (l > a.lmax || kz >= a.nz) continue;
-      double f = l ? 1.0 / ((double)l * (double)(l + 1)) : 0.0;
-      // S = X1 - i X2 ; T = -X3 - i X4
-      double2 S = make_double2(x1[mt][nt][0] + x2[mt][nt][1], x1[mt][nt][1] - x2[mt][nt][0]);
-      double2 T = make_double2(-x3[mt][nt][0] + x4[mt][nt][1], -x3[mt][nt][1] - x4[mt][nt][0]);
-      S = cscale(S, f);
-      T = cscale(T, f);
-      if (m == 0) { S.y = 0.0; T.y = 0.0; }
-      size_t o = (size_t)kz * a.nlm + base_lm + l;
-      a.out[o] = S;
-      a.out2[o] = T;
+      int pl = nh * 16 + nt * 4 + t;
+      Cs[(outT * KZ + pl) * L + 2 * row + par] = make_double2(acc[mt][nt][0], acc[mt][nt][1]);
     }
+  __syncthreads();
+  const int nvalid = min(L, a.lmax + 1 - l0);
+  for (int idx = tid; idx < 2 * KZ * L; idx += 256) {
+    int ll = idx % L, r = idx / L, pl = r % KZ, o = r / KZ;
+    int kz = kz0 + pl;
+    if (kz >= a.nz || ll >= nvalid) continue;
+    int l = l0 + ll;
+    double f = l ? 1.0 / ((double)l * (double)(l + 1)) : 0.0;
+    double2 v = Cs[idx];
+    v.x *= f;
+    v.y *= f;
+    if (m == 0) v.y = 0.0;
+    (o ? a.out2 : a.out)[(size_t)kz * a.nlm + base_lm + l] = v;
+  }
 }
 
-// ---------------------------------------------------------------- vector synthesis
-// Vt_q = sum_{p=1-q} dP_l S_l + i sum_{p=q} mPs_l T_l
-// Vp_q = -sum_{p=1-q} dP_l T_l + i sum_{p=q} mPs_l S_l
-// CTA: 32 nodes x 64 columns; 8 warps: (fold q, theta/phi, column half).
-constexpr int VS_I = 32, VS_N = 64, VS_K = 16, VS_LDA = VS_I + 4, VS_LDB = VS_N + 4;
+// ================================================================ vector synthesis
+// CTA: 32 nodes x 32 planes; K tile 16 consecutive l.  8 warps =
+// (fold q, output Vt/Vp, column half), 32x32 each.
+namespace vs {
+constexpr int I = 32, KZ = 32, K = 16, LDA = I + 4, LDB = 2 * KZ + 4;
+constexpr int A_SZ = 2 * K * LDA;  // [table][par][q][node]
+constexpr int B_SZ = 2 * K * LDB;  // [field S/T][par][q][col]
+constexpr int STAGE = A_SZ + B_SZ;
+constexpr int SMEM = STAGES * STAGE * 8;
+}  // namespace vs
+
+template <int FORM>
+__device__ __forceinline__ void mma_block_kmaj(double (&acc)[4][4][2], const double* As, int lda,
+                                               const double* Bs, int ldb, int g, int t) {
+#pragma unroll
+  for (int k0 = 0; k0 < 8; k0 += 4) {
+    double av[4], bv[4];
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt) av[mt] = As[(k0 + t) * lda + mt * 8 + g];
+    // column n = nt*8 + g of an interleaved (re, im) row
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) bv[nt] = bform<FORM>(Bs + (k0 + t) * ldb + nt * 8 + (g & ~1), g & 1);
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) dmma(acc[mt][nt], av[mt], bv[nt]);
+  }
+}
 
 __global__ void __launch_bounds__(256) vec_synthesis_kernel(LegArgs a) {
-  __shared__ __align__(16) double Ad[2 * 8 * VS_LDA];   // dP  [par][q8][node]
-  __shared__ __align__(16) double Am[2 * 8 * VS_LDA];   // mPs
-  __shared__ __align__(16) double Bsv[2 * 8 * VS_LDB];  // S   [par][q8][col]
-  __shared__ __align__(16) double Btv[2 * 8 * VS_LDB];  // T
+  using namespace vs;
+  extern __shared__ __align__(16) double sm[];
   const LegTile tile = a.tiles[blockIdx.x];
   const int m = tile.m, i0 = tile.r0;
-  const int n0 = blockIdx.y * VS_N, kz0 = n0 / 2;
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int q = warp >> 2, comp = (warp >> 1) & 1, nh = warp & 1;
+  const int kz0 = blockIdx.y * KZ;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+  const int q = warp >> 2, outP = (warp >> 1) & 1, nh = warp & 1;
   const size_t base_lm = (size_t)a.mbase[m] - m;
+  const int nk = (a.lmax + 1 - m + K - 1) / K;
 
-  double xa[4][4][2], xb[4][4][2];
-  zero_acc(xa);
-  zero_acc(xb);
-
-  for (int lk = m; lk <= a.lmax; lk += VS_K) {
-    for (int idx = tid; idx < VS_K * VS_I; idx += 256) {
-      int qq = idx / VS_I, ii = idx - qq * VS_I;
-      int l = lk + qq, i = i0 + ii;
-      bool ok = (l <= a.lmax && i < a.nlat2);
-      size_t off = (base_lm + l) * a.nlat2 + i;
-      int so = ((qq & 1) * 8 + (qq >> 1)) * VS_LDA + ii;
-      Ad[so] = ok ? __ldg(a.dP + off) : 0.0;
-      Am[so] = ok ? __ldg(a.mPs + off) : 0.0;
+  auto load = [&](int st, int lk) {
+    double* As = sm + st * STAGE;
+    double* Bs = As + A_SZ;
+    for (int c = tid; c < 2 * K * (I / 2); c += 256) {
+      int cc = c % (I / 2), r = c / (I / 2), qq = r % K, tb = r / K;
+      int l = lk + qq, i = i0 + 2 * cc;
+      bool ok = l <= a.lmax && i < a.ldn;
+      const double* tab = tb ? a.mPs : a.dP;
+      const double* src = ok ? tab + (base_lm + l) * a.ldn + i : a.dP;
+      cp16(As + (tb * K + (qq & 1) * (K / 2) + (qq >> 1)) * LDA + 2 * cc, src, ok);
     }
-    for (int idx = tid; idx < (VS_N / 2) * VS_K; idx += 256) {
-      int qq = idx % VS_K, pl = idx / VS_K;
+    for (int c = tid; c < 2 * K * KZ; c += 256) {
+      int qq = c % K, r = c / K, pl = r % KZ, fl = r / KZ;
       int l = lk + qq, kz = kz0 + pl;
-      double2 s = make_double2(0.0, 0.0), tt = s;
-      if (l <= a.lmax && kz < a.nz && l > 0) {
-        size_t o = (size_t)kz * a.nlm + base_lm + l;
-        s = a.spec[o];
-        tt = a.spec2[o];
-      }
-      if (m == 0) { s.y = 0.0; tt.y = 0.0; }
-      int ro = ((qq & 1) * 8 + (qq >> 1)) * VS_LDB;
-      Bsv[ro + 2 * pl] = s.x;
-      Bsv[ro + 2 * pl + 1] = s.y;
-      Btv[ro + 2 * pl] = tt.x;
-      Btv[ro + 2 * pl + 1] = tt.y;
+      bool ok = l <= a.lmax && kz < a.nz && l > 0;
+      const double2* sp = fl ? a.spec2 : a.spec;
+      const double2* src = ok ? sp + (size_t)kz * a.nlm + base_lm + l : a.spec;
+      cp16(Bs + (fl * K + (qq & 1) * (K / 2) + (qq >> 1)) * LDB + 2 * pl, src, ok);
     }
-    __syncthreads();
-    // rows of parity 1-q through dP, rows of parity q through mPs
-    const double* ad = Ad + (1 - q) * 8 * VS_LDA;
-    const double* am = Am + q * 8 * VS_LDA;
-    const double* bA = (comp == 0 ? Bsv : Btv) + (1 - q) * 8 * VS_LDB + nh * 32;
-    const double* bB = (comp == 0 ? Btv : Bsv) + q * 8 * VS_LDB + nh * 32;
-    warp_mma<4, 4, true, false>(xa, ad, VS_LDA, bA, VS_LDB, 8);
-    warp_mma<4, 4, true, false>(xb, am, VS_LDA, bB, VS_LDB, 8);
-    __syncthreads();
-  }
+  };
 
-  double2* G = a.Gw + (size_t)(1 + comp) * a.Gfield;
-  const int lane = tid & 31, g = lane >> 2, t = lane & 3;
-  const double sa = comp == 0 ? 1.0 : -1.0;
+  double acc[4][4][2];
+  zero_acc(acc);
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < nk) load(s, m + s * K);
+    cp_commit();
+  }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_wait<STAGES - 2>();
+    __syncthreads();
+    const double* As = sm + (kt % STAGES) * STAGE;
+    const double* Bs = As + A_SZ;
+    // rows of parity 1-q through dP, rows of parity q through mPs
+    const double* Ad = As + (0 * K + (1 - q) * (K / 2)) * LDA;
+    const double* Am = As + (1 * K + q * (K / 2)) * LDA;
+    const double* BS_d = Bs + (0 * K + (1 - q) * (K / 2)) * LDB + nh * 32;
+    const double* BT_d = Bs + (1 * K + (1 - q) * (K / 2)) * LDB + nh * 32;
+    const double* BS_m = Bs + (0 * K + q * (K / 2)) * LDB + nh * 32;
+    const double* BT_m = Bs + (1 * K + q * (K / 2)) * LDB + nh * 32;
+    if (!outP) {
+      // Vt_q = dP S + mPs (i T)
+      mma_block_kmaj<PLAIN>(acc, Ad, LDA, BS_d, LDB, g, t);
+      mma_block_kmaj<MULI>(acc, Am, LDA, BT_m, LDB, g, t);
+    } else {
+      // Vp_q = dP (-T) + mPs (i S)
+      mma_block_kmaj<NEG>(acc, Ad, LDA, BT_d, LDB, g, t);
+      mma_block_kmaj<MULI>(acc, Am, LDA, BS_m, LDB, g, t);
+    }
+    int nx = kt + STAGES - 1;
+    if (nx < nk) load(nx % STAGES, m + nx * K);
+    cp_commit();
+  }
+  cp_wait<0>();
+
+  double2* G = a.Gw + (size_t)(1 + outP) * a.Gfield + ((size_t)m * 2 + q) * a.nz * a.ldn;
 #pragma unroll
   for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
     for (int nt = 0; nt < 4; ++nt) {
       int i = i0 + mt * 8 + g;
-      int kz = kz0 + (nh * 32 + nt * 8 + 2 * t) / 2;
-      if (i >= a.nlat2 || kz >= a.nz) continue;
-      // V = sa * Xa + i * Xb
-      double2 v = make_double2(sa * xa[mt][nt][0] - xb[mt][nt][1], sa * xa[mt][nt][1] + xb[mt][nt][0]);
-      G[(((size_t)m * 2 + q) * a.nz + kz) * a.nlat2 + i] = v;
+      int kz = kz0 + nh * 16 + nt * 4 + t;
+      if (kz < a.nz && i < a.ldn) G[(size_t)kz * a.ldn + i] = make_double2(acc[mt][nt][0], acc[mt][nt][1]);
     }
 }
 
@@ -362,10 +495,16 @@ LegArgs base_args(const sph_plan* p) {
   a.Gfield = p->Gfield;
   a.mbase = p->d_mbase;
   a.lmax = p->lmax;
-  a.nlat2 = p->nlat2;
+  a.ldn = p->ldn;
   a.nz = p->nz;
   a.nlm = p->nlm;
   return a;
+}
+
+template <typename K>
+bool set_smem(K kernel, int bytes) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess &&
+         cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100) == cudaSuccess;
 }
 
 }  // namespace
@@ -375,9 +514,11 @@ int launch_leg_analysis(const sph_plan* p, int gfield, double2* spec, cudaStream
   a.gfield = gfield;
   a.out = spec;
   a.tiles = p->tilesA;
-  dim3 grid(p->ntilesA, (2 * p->nz + AT_N - 1) / AT_N);
+  static bool once = set_smem(leg_analysis_kernel, an::SMEM);
+  if (!once) return SPH_ECUDA;
+  dim3 grid(p->ntilesA, (p->nz + an::KZ - 1) / an::KZ);
   TimedLaunch tl(p, T_LEG_ANA, st);
-  leg_analysis_kernel<<<grid, 128, 0, st>>>(a);
+  leg_analysis_kernel<<<grid, 128, an::SMEM, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
@@ -387,9 +528,11 @@ int launch_leg_synthesis(const sph_plan* p, const double2* spec, int gfield, cud
   a.gfield = gfield;
   a.spec = spec;
   a.tiles = p->tilesS;
-  dim3 grid(p->ntilesS, (2 * p->nz + ST_N - 1) / ST_N);
+  static bool once = set_smem(leg_synthesis_kernel, sy::SMEM);
+  if (!once) return SPH_ECUDA;
+  dim3 grid(p->ntilesS, (p->nz + sy::KZ - 1) / sy::KZ);
   TimedLaunch tl(p, T_LEG_SYN, st);
-  leg_synthesis_kernel<<<grid, 256, 0, st>>>(a);
+  leg_synthesis_kernel<<<grid, 256, sy::SMEM, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
@@ -398,14 +541,12 @@ int launch_vec_analysis(const sph_plan* p, double2* s, double2* t, cudaStream_t 
   LegArgs a = base_args(p);
   a.out = s;
   a.out2 = t;
-  a.tiles = p->tilesA32;
-  size_t smem = (size_t)(4 * 16 * VA_LDA + 4 * VA_N * VA_LDB) * sizeof(double);
-  static bool once = cudaFuncSetAttribute(vec_analysis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem) == cudaSuccess;
+  a.tiles = p->tilesA;
+  static bool once = set_smem(vec_analysis_kernel, va::SMEM);
   if (!once) return SPH_ECUDA;
-  dim3 grid(p->ntilesA32, (2 * p->nz + VA_N - 1) / VA_N);
+  dim3 grid(p->ntilesA, (p->nz + va::KZ - 1) / va::KZ);
   TimedLaunch tl(p, T_VEC_ANA, st);
-  vec_analysis_kernel<<<grid, 128, smem, st>>>(a);
+  vec_analysis_kernel<<<grid, 256, va::SMEM, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
@@ -415,9 +556,11 @@ int launch_vec_synthesis(const sph_plan* p, const double2* s, const double2* t, 
   a.spec = s;
   a.spec2 = t;
   a.tiles = p->tilesS32;
-  dim3 grid(p->ntilesS32, (2 * p->nz + VS_N - 1) / VS_N);
+  static bool once = set_smem(vec_synthesis_kernel, vs::SMEM);
+  if (!once) return SPH_ECUDA;
+  dim3 grid(p->ntilesS32, (p->nz + vs::KZ - 1) / vs::KZ);
   TimedLaunch tl(p, T_VEC_SYN, st);
-  vec_synthesis_kernel<<<grid, 256, 0, st>>>(a);
+  vec_synthesis_kernel<<<grid, 256, vs::SMEM, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }

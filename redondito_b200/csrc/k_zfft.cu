@@ -12,7 +12,7 @@
 //     inverse, without the reference's temporary copy;
 //   fc_filter_r (pseudospec_hd.f90:443-467) and dlr (pseudospec_hd.f90:254-288)
 //     likewise.
-#include "fft_engine.cuh"
+#include "fft_ct.cuh"
 
 namespace {
 
@@ -31,7 +31,27 @@ struct ZArgs {
   FftDesc fd;
 };
 
-template <int MODE>
+template <int CTN>
+struct ZGeo {
+  typedef ct::Geo<CTN, 0, false> type;
+  static __device__ __forceinline__ type make(int LB, int) { return type{LB, 1, LB}; }
+};
+template <>
+struct ZGeo<0> {
+  typedef FftGeom type;
+  static __device__ __forceinline__ type make(int LB, int n) {
+    FftGeom g;
+    g.n = n;
+    g.batch = LB;
+    g.bs = 1;
+    g.es = LB;
+    g.pad = 0;
+    g.jfast = false;
+    return g;
+  }
+};
+
+template <int MODE, int CTN>
 __global__ void __launch_bounds__(ZTHREADS) zfft_kernel(ZArgs a) {
   extern __shared__ double2 sm[];
   const int LB = a.LB, nz = a.nz, nlm = a.nlm;
@@ -80,12 +100,13 @@ __global__ void __launch_bounds__(ZTHREADS) zfft_kernel(ZArgs a) {
     __syncthreads();
   }
 
-  FftGeom g;
-  g.n = nz; g.batch = LB; g.bs = 1; g.es = LB; g.pad = 0; g.jfast = false;
+  const auto g = ZGeo<CTN>::make(LB, nz);
   if (MODE == Z_INV) {
-    fft_dit(sm, a.fd, g, +1);
+    if constexpr (CTN > 0) ct::dit<double2, CTN, CTN>(sm, g, a.fd.twp, +1);
+    else fft_dit(sm, a.fd, g, +1);
   } else {
-    fft_dif(sm, a.fd, g, -1);
+    if constexpr (CTN > 0) ct::dif<double2, CTN, CTN>(sm, g, a.fd.twp, -1);
+    else fft_dif(sm, a.fd, g, -1);
   }
 
   if (MODE == Z_DERIV || MODE == Z_FILTER || MODE == Z_DLR) {
@@ -102,7 +123,8 @@ __global__ void __launch_bounds__(ZTHREADS) zfft_kernel(ZArgs a) {
       sm[o] = v;
     }
     __syncthreads();
-    fft_dit(sm, a.fd, g, +1);
+    if constexpr (CTN > 0) ct::dit<double2, CTN, CTN>(sm, g, a.fd.twp, +1);
+    else fft_dit(sm, a.fd, g, +1);
   }
 
   for (int idx = tid; idx < nz * LB; idx += ZTHREADS) {
@@ -129,20 +151,29 @@ __global__ void __launch_bounds__(ZTHREADS) zfft_kernel(ZArgs a) {
   }
 }
 
-template <int MODE>
-int launch_mode(const ZArgs& a, int nblocks, size_t smem, cudaStream_t st) {
-  static bool attr_set[64] = {false};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!attr_set[dev & 63]) {
-    if (cudaFuncSetAttribute(zfft_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             200 * 1024) != cudaSuccess)
-      return SPH_ECUDA;
-    attr_set[dev & 63] = true;
-  }
-  zfft_kernel<MODE><<<nblocks, ZTHREADS, smem, st>>>(a);
+template <int MODE, int CTN>
+int launch_ct(const ZArgs& a, int nblocks, size_t smem, cudaStream_t st) {
+  static bool once = cudaFuncSetAttribute(zfft_kernel<MODE, CTN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          200 * 1024) == cudaSuccess &&
+                     cudaFuncSetAttribute(zfft_kernel<MODE, CTN>,
+                                          cudaFuncAttributePreferredSharedMemoryCarveout, 100) == cudaSuccess;
+  if (!once) return SPH_ECUDA;
+  zfft_kernel<MODE, CTN><<<nblocks, ZTHREADS, smem, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;
+}
+
+#define Z_SIZES(X) X(16) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(512)
+
+template <int MODE>
+int launch_mode(const ZArgs& a, int nblocks, size_t smem, cudaStream_t st) {
+  switch (a.nz) {
+#define CASE(n) \
+  case n: return launch_ct<MODE, n>(a, nblocks, smem, st);
+    Z_SIZES(CASE)
+#undef CASE
+    default: return launch_ct<MODE, 0>(a, nblocks, smem, st);
+  }
 }
 
 }  // namespace

@@ -122,6 +122,27 @@ static std::vector<int> digit_reversal(const FftDesc& fd) {
   return rev;
 }
 
+// per-pass twiddles [pass][j][r-1] = W_L^{j r}, DIF pass order (fft_ct.cuh)
+static void pass_twiddles(int n, std::vector<double2>& tw, std::vector<float2>& twf) {
+  tw.clear();
+  twf.clear();
+  for (int L = n; L > 1;) {
+    int R = L % 8 == 0 ? 8 : L % 4 == 0 ? 4 : L % 2 == 0 ? 2 : L % 3 == 0 ? 3 : L;
+    int S = L / R;
+    for (int j = 0; j < S; ++j)
+      for (int r = 1; r < R; ++r) {
+        ld a = -2.0L * kPi * (ld)((long)j * r) / L;
+        tw.push_back(make_double2((double)cosl(a), (double)sinl(a)));
+        twf.push_back(make_float2((float)cosl(a), (float)sinl(a)));
+      }
+    L = S;
+  }
+  if (tw.empty()) {
+    tw.push_back(make_double2(1.0, 0.0));
+    twf.push_back(make_float2(1.f, 0.f));
+  }
+}
+
 static void twiddles(int n, std::vector<double2>& tw, std::vector<float2>& twf) {
   tw.resize(n);
   twf.resize(n);
@@ -144,7 +165,7 @@ static void plan_free(sph_plan* p) {
   for (auto e : p->ev_pool) cudaEventDestroy(e);
   void* ptrs[] = {p->P, p->dP, p->mPs, p->wfold, p->wfull, p->d_dir, p->d_z, p->kfac, p->filt,
                   p->zinv2, p->d_ell, p->d_mbase, p->twz, p->twphi, p->twzf, p->twphif, p->revz,
-                  p->revphi, p->tilesA,
+                  p->revphi, p->twpz, p->twpphi, p->twpzf, p->twpphif, p->tilesA,
                   p->tilesA32, p->tilesS, p->tilesS32, p->G, p->binv, p->d2bor, p->energy};
   for (void* q : ptrs)
     if (q) cudaFree(q);
@@ -179,6 +200,7 @@ extern "C" int sph_plan_create(sph_plan** out, int lmax, int nlat, int nphi, int
   p->lmax = lmax;
   p->nlat = nlat;
   p->nlat2 = nlat / 2;
+  p->ldn = (p->nlat2 + 3) & ~3;
   p->nphi = nphi;
   p->nz = nz;
   p->C = Cz;
@@ -223,8 +245,9 @@ extern "C" int sph_plan_create(sph_plan** out, int lmax, int nlat, int nphi, int
   if (Cz > 0) p->dir.assign(dir, dir + (size_t)Cz * oz);
 
   // Legendre tables on the northern nodes, [lm][node], built in parallel over m
-  const int n2 = p->nlat2;
-  std::vector<double> hP((size_t)p->nlm * n2), hdP((size_t)p->nlm * n2), hmPs((size_t)p->nlm * n2);
+  const int n2 = p->nlat2, ldn = p->ldn;
+  std::vector<double> hP((size_t)p->nlm * ldn, 0.0), hdP((size_t)p->nlm * ldn, 0.0),
+      hmPs((size_t)p->nlm * ldn, 0.0);
   {
     int nth = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
     std::vector<std::thread> th;
@@ -237,7 +260,7 @@ extern "C" int sph_plan_create(sph_plan** out, int lmax, int nlat, int nphi, int
             ld s = sqrtl((1.0L - x) * (1.0L + x));
             legendre_column(lmax, m, x, s, cP.data(), cdP.data(), cmP.data());
             for (int l = m; l <= lmax; ++l) {
-              size_t o = (size_t)(p->mbase[m] + l - m) * n2 + i;
+              size_t o = (size_t)(p->mbase[m] + l - m) * ldn + i;
               hP[o] = cP[l - m];
               hdP[o] = cdP[l - m];
               hmPs[o] = cmP[l - m];
@@ -246,7 +269,7 @@ extern "C" int sph_plan_create(sph_plan** out, int lmax, int nlat, int nphi, int
       });
     for (auto& x : th) x.join();
   }
-  std::vector<double> wf(n2);
+  std::vector<double> wf(ldn, 0.0);
   for (int i = 0; i < n2; ++i) wf[i] = p->w[i] * (2.0 * 3.14159265358979323846 / nphi);
   std::vector<double2> kf((size_t)4 * nz);
   for (int o = 1; o <= 4; ++o)
@@ -269,10 +292,16 @@ extern "C" int sph_plan_create(sph_plan** out, int lmax, int nlat, int nphi, int
   twiddles(nz, twz, twzf);
   twiddles(nphi, twp, twpf);
   std::vector<int> revz = digit_reversal(p->fz), revphi = digit_reversal(p->fphi);
+  std::vector<double2> tpz, tpp;
+  std::vector<float2> tpzf, tppf;
+  pass_twiddles(nz, tpz, tpzf);
+  pass_twiddles(nphi, tpp, tppf);
   auto tA = row_tiles(lmax, 64, true, n2);
   auto tA32 = row_tiles(lmax, 32, true, n2);
   auto tS = row_tiles(lmax, 64, false, n2);
   auto tS32 = row_tiles(lmax, 32, false, n2);
+  // heaviest synthesis tiles (small m: K = lmax+1-m) first
+
 
   int rc = SPH_OK;
 #define UP(dst, vec)                                              \
@@ -294,6 +323,10 @@ extern "C" int sph_plan_create(sph_plan** out, int lmax, int nlat, int nphi, int
   UP(p->twphif, twpf);
   UP(p->revz, revz);
   UP(p->revphi, revphi);
+  UP(p->twpz, tpz);
+  UP(p->twpphi, tpp);
+  UP(p->twpzf, tpzf);
+  UP(p->twpphif, tppf);
   UP(p->tilesA, tA);
   UP(p->tilesA32, tA32);
   UP(p->tilesS, tS);
@@ -307,12 +340,19 @@ extern "C" int sph_plan_create(sph_plan** out, int lmax, int nlat, int nphi, int
   p->fz.tw = p->twz;
   p->fz.twf = p->twzf;
   p->fz.rev = p->revz;
+  p->fz.twp = p->twpz;
+  p->fz.twpf = p->twpzf;
   p->fphi.tw = p->twphi;
   p->fphi.twf = p->twphif;
   p->fphi.rev = p->revphi;
-  p->Gfield = (size_t)(lmax + 1) * 2 * nz * n2;
+  p->fphi.twp = p->twpphi;
+  p->fphi.twpf = p->twpphif;
+  p->Gfield = (size_t)(lmax + 1) * 2 * nz * ldn;
   if (rc == SPH_OK && cudaMalloc((void**)&p->G, SPH_MAX_FIELDS * p->Gfield * sizeof(double2)) != cudaSuccess)
     rc = SPH_ENOMEM;
+  // node columns past nlat/2 are never written and must read as zero
+  if (rc == SPH_OK && cudaMemset(p->G, 0, SPH_MAX_FIELDS * p->Gfield * sizeof(double2)) != cudaSuccess)
+    rc = SPH_ECUDA;
   if (rc == SPH_OK && cudaMalloc((void**)&p->energy, sizeof(double)) != cudaSuccess) rc = SPH_ENOMEM;
   if (rc != SPH_OK) {
     plan_free(p);

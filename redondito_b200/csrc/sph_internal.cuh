@@ -26,6 +26,8 @@ struct FftDesc {
   const double2* tw;
   const float2* twf;  // same table in fp32 (mixed-precision path)
   const int* rev;
+  const double2* twp;   // per-pass table [pass][j][r-1] = W_L^{j r} (compile-time lengths)
+  const float2* twpf;
 };
 
 // Legendre GEMM work tile: one (m, row block) pair.
@@ -36,14 +38,15 @@ struct LegTile {
 struct sph_plan {
   // sizes
   int lmax, nlat, nlat2, nphi, nz, C, d, nlm, N, precision;
+  int ldn;  // node stride of the tables and folded buffers: nlat/2 rounded up to 4
   double rint, rext, dz, Dkz;
   // host copies of the grid (box_init)
   std::vector<double> theta, ct, w, phi, z, kz, dir;
   std::vector<int> ell, emm, mbase;
   // device tables
-  double* P = nullptr;    // [nlm][nlat2]  Pbar_lm(x_i), northern nodes
-  double* dP = nullptr;   // [nlm][nlat2]  d Pbar_lm / d theta
-  double* mPs = nullptr;  // [nlm][nlat2]  m Pbar_lm / sin theta
+  double* P = nullptr;    // [nlm][ldn]  Pbar_lm(x_i), northern nodes (0 past nlat/2)
+  double* dP = nullptr;   // [nlm][ldn]  d Pbar_lm / d theta
+  double* mPs = nullptr;  // [nlm][ldn]  m Pbar_lm / sin theta
   double* wfold = nullptr;  // [nlat2] w_i * 2 pi / nphi
   double* wfull = nullptr;  // [nlat] Gauss weights
   double* d_dir = nullptr;  // [C*d] column-major
@@ -59,6 +62,10 @@ struct sph_plan {
   float2* twphif = nullptr;
   int* revz = nullptr;      // [nz]
   int* revphi = nullptr;    // [nphi]
+  double2* twpz = nullptr;  // per-pass twiddles (see fft_ct.cuh)
+  double2* twpphi = nullptr;
+  float2* twpzf = nullptr;
+  float2* twpphif = nullptr;
   FftDesc fz, fphi;
   // Legendre work lists (device)
   LegTile* tilesA = nullptr;   // analysis: (m, l0) blocks of 64 l
@@ -69,7 +76,7 @@ struct sph_plan {
   int ntilesS = 0;
   LegTile* tilesS32 = nullptr; // vector synthesis: blocks of 32 nodes
   int ntilesS32 = 0;
-  // scratch: folded Fourier coefficients, per field [lmax+1][2][nz][nlat2] complex
+  // scratch: folded Fourier coefficients, per field [lmax+1][2][nz][ldn] complex
   double2* G = nullptr;
   size_t Gfield = 0;  // elements per field
   // spectral scratch (nz*nlm complex each)

@@ -229,3 +229,32 @@ def test_nl_rhs_and_rk3():
     assert rel_l2(host(Zg), Zr) < TOL_D2
     assert rel_l2(host(Wg), Wr) < TOL_D2
     assert rel_l2(host(Fg), Fr) < TOL_D2
+
+
+@pytest.mark.parametrize("lmax,nlat,nphi", [(255, 384, 768), (511, 768, 1536)])
+def test_sht_full_angular_size(lmax, nlat, nphi):
+    """The benchmark's angular sizes (compile-time 768/1536-point phi FFTs),
+    scalar and vector, on two planes."""
+    from redondito_b200 import sphp as S
+    P, G = _pair(lmax, 2, nlat=nlat, nphi=nphi)
+    rng = np.random.default_rng(lmax + 7)
+    a = random_spec(P, rng, power=1.0, radial=False)
+    g_ref = P.sh_synthesis(a)
+    g = G.new_grid()
+    S.fftp2d_complex_to_real_xy(G, dev(a), g)
+    assert rel_l2(host(g), g_ref) < TOL
+    s = G.new_spec()
+    S.fftp2d_real_to_complex_xy(G, dev(g_ref), s)
+    assert rel_l2(host(s), P.sh_analysis(g_ref)) < TOL
+    q, sv, tv = a, random_spec(P, rng, power=1.0, radial=False), random_spec(P, rng, power=1.0, radial=False)
+    sv[:, 0] = 0
+    tv[:, 0] = 0
+    v_ref = P.qst_synthesis(q, sv, tv)
+    out = [G.new_grid() for _ in range(3)]
+    S.fftp2d_qst_to_vec(G, dev(q), dev(sv), dev(tv), *out)
+    for o, r in zip(out, v_ref):
+        assert rel_l2(host(o), r) < TOL
+    qs = [G.new_spec() for _ in range(3)]
+    S.fftp2d_vec_to_qst(G, *[dev(x) for x in v_ref], *qs)
+    for o, r in zip(qs, P.qst_analysis(*v_ref)):
+        assert rel_l2(host(o), r) < TOL
