@@ -379,7 +379,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "bf16x3/f32",
         "data": "synthetic",
-        "config": {"workload": "scalar + vector field, lmax=511, 768x1536, nz=256, FC-Gram C=25 d=5",
+        "config": {"workload": (f"scalar + vector field, lmax={W['lmax']}, {W['nlat']}x{W['nphi']}, "
+                                f"nz={W['nz']}, FC-Gram C={W['Cz']} d={W['oz']}"),
                    **W, "fields": 4, "precision": args.precision,
                    "l2_flush": "inputs larger than L2 (every buffer > 126 MB)",
                    "parallelism": f"replicas x{world}"},

@@ -164,6 +164,19 @@ __device__ __forceinline__ void pass(T2* buf, const Geo<N, PAD, JFAST>& g, const
   __syncthreads();
 }
 
+// position of frequency k after dif<N> (the rev[] table, computed from the
+// compile-time radix sequence): k = q0 + R0 (q1 + R1 (...)), pos = sum q_p s_p
+template <int N, int L = N>
+__device__ __forceinline__ int rev_pos(int k) {
+  constexpr int R = radix_of(L), S = L / R;
+  if constexpr (S == 1) {
+    return k;  // last digit, span 1
+  } else {
+    const int q = k % R;
+    return q * S + rev_pos<N, S>(k / R);
+  }
+}
+
 template <typename T2, int N, int L, int PAD, bool JFAST>
 __device__ __forceinline__ void dif(T2* buf, const Geo<N, PAD, JFAST>& g, const T2* __restrict__ twp, int sign) {
   pass<T2, N, L, false>(buf, g, twp, sign);

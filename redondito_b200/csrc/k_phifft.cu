@@ -40,27 +40,126 @@ struct PhiArgs {
   FftDesc fd;
 };
 
-// The geometry type of a length: compile-time for CTN > 0, runtime otherwise.
-template <int CTN>
-struct PhiGeo {
-  typedef ct::Geo<CTN, 1, true> type;
-  static __device__ __forceinline__ type make(int NP, int ss, int) { return type{NP, ss, 1}; }
-};
-template <>
-struct PhiGeo<0> {
-  typedef FftGeom type;
-  static __device__ __forceinline__ type make(int NP, int ss, int n) {
-    FftGeom g;
-    g.n = n;
-    g.batch = NP;
-    g.bs = ss;
-    g.es = 1;
-    g.pad = 1;
-    g.jfast = true;
-    return g;
+// ---------------------------------------------------------------- lengths 2^a 3^b
+// N (phi length) and NP (ring pairs per CTA) fixed at compile time: every
+// thread keeps one ring (load/store) or one ring pair (spectrum) and walks
+// the other index with a constant stride, so no runtime divisions remain.
+template <int N, int NP>
+__global__ void __launch_bounds__(PTHREADS, 2) phi_fwd_ct(PhiArgs a) {
+  extern __shared__ double2 sm[];
+  constexpr int Q = 2 * NP;             // rings per CTA
+  constexpr int JSTEP = PTHREADS / Q;   // phi stride of one thread
+  const int nlat = a.nlat;
+  const int p0 = blockIdx.x * NP, k = blockIdx.y, f = blockIdx.z;
+  const int tid = threadIdx.x;
+  const double* plane = a.gin[f] + (size_t)k * N * nlat;
+  const ct::Geo<N, 1, true> g{NP, seq_stride(N), 1};
+  double* smd = reinterpret_cast<double*>(sm);
+  {
+    // ring slot q: 0..NP-1 northern rings p0+q (real part), NP..2NP-1 their
+    // mirrors in ascending address order (imaginary part of pair 2NP-1-q)
+    const int q = tid % Q, j0 = tid / Q;
+    const int b = q < NP ? q : 2 * NP - 1 - q;
+    const int ring = q < NP ? p0 + q : nlat - 1 - (p0 + b);
+    const int half = q < NP ? 0 : 1;
+    constexpr int NJ = (N + JSTEP - 1) / JSTEP;
+    constexpr int U = 8;
+#pragma unroll
+    for (int u0 = 0; u0 < NJ; u0 += U) {
+      double v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        int j = j0 + (u0 + u) * JSTEP;
+        v[u] = (u0 + u < NJ && j < N) ? __ldg(plane + (size_t)j * nlat + ring) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        int j = j0 + (u0 + u) * JSTEP;
+        if (u0 + u < NJ && j < N) smd[2 * g.addr(b, j) + half] = v[u];
+      }
+    }
   }
-};
+  __syncthreads();
+  ct::dif<double2, N, N>(sm, g, a.fd.twp, -1);
 
+  // both parities of one (m, pair) from one read of Z(m), Z(-m)
+  double2* G = a.G + (size_t)f * a.Gfield + (size_t)k * a.ldn + p0;
+  const size_t mstride = (size_t)2 * a.nz * a.ldn, pstride = (size_t)a.nz * a.ldn;
+  const int b = tid % NP;
+  const double W = __ldg(a.wfold + p0 + b);
+  for (int m = tid / NP; m <= a.lmax; m += PTHREADS / NP) {
+    double2 Z = sm[g.addr(b, ct::rev_pos<N>(m))];
+    double2 Zc = sm[g.addr(b, ct::rev_pos<N>(m == 0 ? 0 : N - m))];
+    // F(i) = (Z + conj Z(-m))/2, F(mirror) = -i (Z - conj Z(-m))/2
+    double2 Fi = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y - Zc.y));
+    double2 Fm = make_double2(0.5 * (Z.y + Zc.y), -0.5 * (Z.x - Zc.x));
+    G[m * mstride + b] = cscale(cadd(Fi, Fm), W);
+    G[m * mstride + pstride + b] = cscale(csub(Fi, Fm), W);
+  }
+}
+
+template <int N, int NP>
+__global__ void __launch_bounds__(PTHREADS, 2) phi_inv_ct(PhiArgs a) {
+  extern __shared__ double2 sm[];
+  constexpr int Q = 2 * NP;
+  constexpr int JSTEP = PTHREADS / Q;
+  const int nlat = a.nlat;
+  const int p0 = blockIdx.x * NP, k = blockIdx.y, f = blockIdx.z;
+  const int tid = threadIdx.x;
+  const ct::Geo<N, 1, true> g{NP, seq_stride(N), 1};
+  const int M = a.lmax + 1;
+
+  // zero everything, then scatter the 2 lmax + 1 nonzero frequencies
+  {
+    double2* s4 = sm;
+    const int tot = NP * seq_stride(N);
+    for (int i = tid; i < tot; i += PTHREADS) s4[i] = make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  {
+    const double2* G = a.Gc + (size_t)f * a.Gfield + (size_t)k * a.ldn + p0;
+    const size_t mstride = (size_t)2 * a.nz * a.ldn, pstride = (size_t)a.nz * a.ldn;
+    const int b = tid % NP;
+    constexpr int U = 4;
+    for (int m0 = tid / NP; m0 < M; m0 += U * (PTHREADS / NP)) {
+      double2 se[U], so[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        int m = m0 + u * (PTHREADS / NP);
+        se[u] = so[u] = make_double2(0.0, 0.0);
+        if (m < M) {
+          se[u] = __ldg(G + m * mstride + b);
+          so[u] = __ldg(G + m * mstride + pstride + b);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        int m = m0 + u * (PTHREADS / NP);
+        if (m >= M) continue;
+        double2 Fi = cadd(se[u], so[u]), Fm = csub(se[u], so[u]);
+        if (m == 0) {
+          sm[g.addr(b, 0)] = make_double2(Fi.x, Fm.x);
+        } else {
+          // z = x + i y with x, y the real fields of ring i and its mirror
+          sm[g.addr(b, ct::rev_pos<N>(m))] = make_double2(Fi.x - Fm.y, Fi.y + Fm.x);
+          sm[g.addr(b, ct::rev_pos<N>(N - m))] = make_double2(Fi.x + Fm.y, -Fi.y + Fm.x);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  ct::dit<double2, N, N>(sm, g, a.fd.twp, +1);
+
+  double* plane = a.gout[f] + (size_t)k * N * nlat;
+  const double* smd = reinterpret_cast<const double*>(sm);
+  const int q = tid % Q, j0 = tid / Q;
+  const int b = q < NP ? q : 2 * NP - 1 - q;
+  const int ring = q < NP ? p0 + q : nlat - 1 - (p0 + b);
+  const int half = q < NP ? 0 : 1;
+  for (int j = j0; j < N; j += JSTEP) plane[(size_t)j * nlat + ring] = smd[2 * g.addr(b, j) + half];
+}
+
+// ---------------------------------------------------------------- other lengths
 template <int CTN>
 __global__ void __launch_bounds__(PTHREADS, 2) phi_fwd_kernel(PhiArgs a) {
   extern __shared__ double2 sm[];
@@ -71,56 +170,31 @@ __global__ void __launch_bounds__(PTHREADS, 2) phi_fwd_kernel(PhiArgs a) {
   const int tid = threadIdx.x;
   const double* plane = a.gin[f] + (size_t)k * nphi * nlat;
   const int np = min(NP, nlat2 - p0);
-  const auto g = PhiGeo<CTN>::make(NP, seq_stride(nphi), nphi);
+  FftGeom g;
+  g.n = nphi; g.batch = NP; g.bs = seq_stride(nphi); g.es = 1; g.pad = 1; g.jfast = true;
   double* smd = reinterpret_cast<double*>(sm);
-
-  // rings p0..p0+np-1 (real part) and their mirrors (imaginary part);
-  // consecutive threads read consecutive theta addresses
   const int total = nphi * 2 * NP;
-  for (int base = tid; base < total; base += PTHREADS * UNR) {
-    double v[UNR];
-#pragma unroll
-    for (int u = 0; u < UNR; ++u) {
-      int idx = base + u * PTHREADS;
-      v[u] = 0.0;
-      if (idx < total) {
-        int j = idx / (2 * NP), q = idx - j * 2 * NP;
-        int b = q < NP ? q : NP - 1 - (q - NP);  // mirrors in ascending address order
-        int ring = q < NP ? p0 + q : nlat - 1 - (p0 + b);
-        if (b < np) v[u] = __ldg(plane + (size_t)j * nlat + ring);
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < UNR; ++u) {
-      int idx = base + u * PTHREADS;
-      if (idx < total) {
-        int j = idx / (2 * NP), q = idx - j * 2 * NP;
-        int b = q < NP ? q : NP - 1 - (q - NP);
-        smd[2 * g.addr(b, j) + (q < NP ? 0 : 1)] = v[u];
-      }
-    }
+  for (int idx = tid; idx < total; idx += PTHREADS) {
+    int j = idx / (2 * NP), q = idx - j * 2 * NP;
+    int b = q < NP ? q : NP - 1 - (q - NP);
+    int ring = q < NP ? p0 + q : nlat - 1 - (p0 + b);
+    smd[2 * g.addr(b, j) + (q < NP ? 0 : 1)] = b < np ? __ldg(plane + (size_t)j * nlat + ring) : 0.0;
   }
   __syncthreads();
-  if constexpr (CTN > 0) ct::dif<double2, CTN, CTN>(sm, g, a.fd.twp, -1);
-  else fft_dif(sm, a.fd, g, -1);
+  fft_dif(sm, a.fd, g, -1);
   const int* __restrict__ rev = a.fd.rev;
-
   double2* G = a.G + (size_t)f * a.Gfield;
   const int M = a.lmax + 1;
-  for (int idx = tid; idx < M * 2 * NP; idx += PTHREADS) {
-    int b = idx % NP;
-    int rest = idx / NP;
-    int par = rest & 1, m = rest >> 1;
+  for (int idx = tid; idx < M * NP; idx += PTHREADS) {
+    int b = idx % NP, m = idx / NP;
     if (b >= np) continue;
     double2 Z = sm[g.addr(b, __ldg(rev + m))];
     double2 Zc = sm[g.addr(b, __ldg(rev + (m == 0 ? 0 : nphi - m)))];
-    Zc.y = -Zc.y;
-    // F(i) = (Z + conj Z(-m))/2, F(mirror) = -i (Z - conj Z(-m))/2
-    double2 Fi = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
-    double2 Fm = make_double2(0.5 * (Z.y - Zc.y), -0.5 * (Z.x - Zc.x));
+    double2 Fi = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y - Zc.y));
+    double2 Fm = make_double2(0.5 * (Z.y + Zc.y), -0.5 * (Z.x - Zc.x));
     double W = __ldg(a.wfold + p0 + b);
-    double2 gv = par ? csub(Fi, Fm) : cadd(Fi, Fm);
-    G[(((size_t)m * 2 + par) * a.nz + k) * a.ldn + p0 + b] = cscale(gv, W);
+    G[(((size_t)m * 2 + 0) * a.nz + k) * a.ldn + p0 + b] = cscale(cadd(Fi, Fm), W);
+    G[(((size_t)m * 2 + 1) * a.nz + k) * a.ldn + p0 + b] = cscale(csub(Fi, Fm), W);
   }
 }
 
@@ -135,45 +209,26 @@ __global__ void __launch_bounds__(PTHREADS, 2) phi_inv_kernel(PhiArgs a) {
   const int np = min(NP, nlat2 - p0);
   const int M = a.lmax + 1;
   const double2* G = a.Gc + (size_t)f * a.Gfield;
-  const auto g = PhiGeo<CTN>::make(NP, seq_stride(nphi), nphi);
+  FftGeom g;
+  g.n = nphi; g.batch = NP; g.bs = seq_stride(nphi); g.es = 1; g.pad = 1; g.jfast = true;
   const int* __restrict__ rev = a.fd.rev;
-
-  // the band between the two Hermitian halves is zero
-  for (int idx = tid; idx < NP * nphi; idx += PTHREADS) {
-    int b = idx / nphi, m = idx - b * nphi;
-    if (m >= M && m <= nphi - M) sm[g.addr(b, __ldg(rev + m))] = make_double2(0.0, 0.0);
-  }
-  for (int base = tid; base < M * NP; base += PTHREADS * (UNR / 2)) {
-    double2 se[UNR / 2], so[UNR / 2];
-#pragma unroll
-    for (int u = 0; u < UNR / 2; ++u) {
-      int idx = base + u * PTHREADS;
-      se[u] = so[u] = make_double2(0.0, 0.0);
-      int b = idx % NP, m = idx / NP;
-      if (idx < M * NP && b < np) {
-        se[u] = __ldg(G + (((size_t)m * 2 + 0) * a.nz + k) * a.ldn + p0 + b);
-        so[u] = __ldg(G + (((size_t)m * 2 + 1) * a.nz + k) * a.ldn + p0 + b);
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < UNR / 2; ++u) {
-      int idx = base + u * PTHREADS;
-      if (idx >= M * NP) continue;
-      int b = idx % NP, m = idx / NP;
-      double2 Fi = cadd(se[u], so[u]), Fm = csub(se[u], so[u]);
-      if (m == 0) {
-        sm[g.addr(b, __ldg(rev))] = make_double2(Fi.x, Fm.x);
-      } else {
-        // z = x + i y with x, y the real fields of ring i and its mirror
-        sm[g.addr(b, __ldg(rev + m))] = make_double2(Fi.x - Fm.y, Fi.y + Fm.x);
-        sm[g.addr(b, __ldg(rev + nphi - m))] = make_double2(Fi.x + Fm.y, -Fi.y + Fm.x);
-      }
+  for (int i = tid; i < NP * g.bs; i += PTHREADS) sm[i] = make_double2(0.0, 0.0);
+  __syncthreads();
+  for (int idx = tid; idx < M * NP; idx += PTHREADS) {
+    int b = idx % NP, m = idx / NP;
+    if (b >= np) continue;
+    double2 Se = G[(((size_t)m * 2 + 0) * a.nz + k) * a.ldn + p0 + b];
+    double2 So = G[(((size_t)m * 2 + 1) * a.nz + k) * a.ldn + p0 + b];
+    double2 Fi = cadd(Se, So), Fm = csub(Se, So);
+    if (m == 0) {
+      sm[g.addr(b, __ldg(rev))] = make_double2(Fi.x, Fm.x);
+    } else {
+      sm[g.addr(b, __ldg(rev + m))] = make_double2(Fi.x - Fm.y, Fi.y + Fm.x);
+      sm[g.addr(b, __ldg(rev + nphi - m))] = make_double2(Fi.x + Fm.y, -Fi.y + Fm.x);
     }
   }
   __syncthreads();
-  if constexpr (CTN > 0) ct::dit<double2, CTN, CTN>(sm, g, a.fd.twp, +1);
-  else fft_dit(sm, a.fd, g, +1);
-
+  fft_dit(sm, a.fd, g, +1);
   double* plane = a.gout[f] + (size_t)k * nphi * nlat;
   const double* smd = reinterpret_cast<const double*>(sm);
   for (int idx = tid; idx < nphi * 2 * NP; idx += PTHREADS) {
@@ -187,11 +242,11 @@ __global__ void __launch_bounds__(PTHREADS, 2) phi_inv_kernel(PhiArgs a) {
   }
 }
 
+// ring pairs per CTA: the largest of 8, 4, 2, 1 that divides nlat/2 and
+// keeps NP*nphi <= PMAXC
 int pairs_per_cta(const sph_plan* p) {
-  int cap = PMAXC / p->nphi;
-  if (cap > 8) cap = 8;
-  for (int np = cap; np >= 1; --np)
-    if (p->nlat2 % np == 0) return np;
+  for (int np = 8; np > 1; np >>= 1)
+    if (p->nlat2 % np == 0 && np * p->nphi <= PMAXC) return np;
   return 1;
 }
 
@@ -201,22 +256,38 @@ bool smem_attr(K fn) {
          cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100) == cudaSuccess;
 }
 
-template <int CTN>
-int launch_fwd_n(const PhiArgs& a, dim3 grid, size_t smem, cudaStream_t st) {
-  static bool once = smem_attr(phi_fwd_kernel<CTN>);
-  if (!once) return SPH_ECUDA;
-  phi_fwd_kernel<CTN><<<grid, PTHREADS, smem, st>>>(a);
+template <typename K>
+int run(K kernel, const PhiArgs& a, dim3 grid, size_t smem, cudaStream_t st) {
+  if (!smem_attr(kernel)) return SPH_ECUDA;
+  kernel<<<grid, PTHREADS, smem, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
 
-template <int CTN>
+template <int N>
+int launch_fwd_n(const PhiArgs& a, dim3 grid, size_t smem, cudaStream_t st) {
+  if constexpr (N > 0) {
+    switch (a.NP) {
+      case 8: if constexpr (8 * N <= PMAXC) return run(phi_fwd_ct<N, 8>, a, grid, smem, st); break;
+      case 4: if constexpr (4 * N <= PMAXC) return run(phi_fwd_ct<N, 4>, a, grid, smem, st); break;
+      case 2: if constexpr (2 * N <= PMAXC) return run(phi_fwd_ct<N, 2>, a, grid, smem, st); break;
+      case 1: return run(phi_fwd_ct<N, 1>, a, grid, smem, st);
+    }
+  }
+  return run(phi_fwd_kernel<0>, a, grid, smem, st);
+}
+
+template <int N>
 int launch_inv_n(const PhiArgs& a, dim3 grid, size_t smem, cudaStream_t st) {
-  static bool once = smem_attr(phi_inv_kernel<CTN>);
-  if (!once) return SPH_ECUDA;
-  phi_inv_kernel<CTN><<<grid, PTHREADS, smem, st>>>(a);
-  SPH_LAUNCH_OK();
-  return SPH_OK;
+  if constexpr (N > 0) {
+    switch (a.NP) {
+      case 8: if constexpr (8 * N <= PMAXC) return run(phi_inv_ct<N, 8>, a, grid, smem, st); break;
+      case 4: if constexpr (4 * N <= PMAXC) return run(phi_inv_ct<N, 4>, a, grid, smem, st); break;
+      case 2: if constexpr (2 * N <= PMAXC) return run(phi_inv_ct<N, 2>, a, grid, smem, st); break;
+      case 1: return run(phi_inv_ct<N, 1>, a, grid, smem, st);
+    }
+  }
+  return run(phi_inv_kernel<0>, a, grid, smem, st);
 }
 
 #define PHI_SIZES(X) X(12) X(24) X(48) X(96) X(192) X(384) X(768) X(1536) X(3072) X(6144)
