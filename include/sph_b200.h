@@ -124,6 +124,25 @@ int sph_fftp2d_qst_to_vec(sph_plan* plan, const double* q, const double* s, cons
  * (lm,r): continuation + forward + (i kz)^p + inverse, one kernel) or 'k'
  * (a,b in (lm,kz): b = (i kz)^p a, Nyquist kept). a is preserved. */
 int sph_derivr(sph_plan* plan, const double* a, double* b, int p, char esp, void* stream);
+/* No counterpart in the reference.  The same radial derivative as
+ * sph_derivr(a, b, p, 'r') for a caller that has no plan and cannot
+ * allocate device memory: for example a host whose device memory belongs
+ * to another allocator (an OpenMP-offload runtime mapping every array, as
+ * the reference's gdevice layer does, or a pool that already holds the
+ * HBM), where a plan's cudaMalloc'd tables are not an option.  The tables
+ * the kernel reads (twiddles, digit-reversal order, (i kz)^p, the FC-Gram
+ * operator dir, host Cz x oz column-major) are rebuilt on every call in
+ * one file-scope device array of 224 KiB, which every GPU that loads this
+ * library holds until the process exits; nothing in it needs to start at
+ * zero.  Limits: nz <= 4096, Cz*oz <= 2048, 1 <= p <= 4 (SPH_EINVAL
+ * beyond).  Grid as in sph_plan_create (z(k) = rint + k dz,
+ * dz = (rext-rint)/(nz-Cz-1)).  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls share the one array, so calls
+ * that overlap on the GPU (other streams, other host threads) race.
+ * Calls no cudaMalloc/cudaFree and allocates no host memory. */
+int sph_derivr_noalloc(const double* a, double* b, int nlm, int nz, int Cz, int oz, double rint,
+                       double rext, const double* dir, int p, void* stream);
 /* laplang (pseudospec_hd.f90:138-172): b = -l(l+1) a */
 int sph_laplang(sph_plan* plan, const double* a, double* b, void* stream);
 /* multr (pseudospec_hd.f90:175-208): b = z^p a */

@@ -12,6 +12,8 @@
 //     inverse, without the reference's temporary copy;
 //   fc_filter_r (pseudospec_hd.f90:443-467) and dlr (pseudospec_hd.f90:254-288)
 //     likewise.
+#include <mutex>
+
 #include "fft_ct.cuh"
 
 namespace {
@@ -215,4 +217,152 @@ int launch_zfft(const sph_plan* p, int mode, const double2* in, double2* out, in
       return launch_mode<Z_DLR>(a, nblocks, smem, st);
   }
   return SPH_EINVAL;
+}
+
+// ---------------------------------------------------------------- no-alloc derivative
+// Radial derivative for callers that cannot allocate device memory: the
+// device-resident tables the fused derivative kernel reads (twiddles,
+// digit-reversal order, (i kz)^p factors, the FC-Gram operator) live in one
+// file-scope array instead of a plan's cudaMalloc'd buffers.  The host side
+// stages them in fixed static buffers, so the call allocates nothing on the
+// host either.
+namespace {
+
+constexpr int NA_MAX_NZ = 4096;  // longest radial transform
+constexpr int NA_MAX_CD = 2048;  // largest Cz*oz
+constexpr size_t NA_TW = 0;                                              // double2[nz]
+constexpr size_t NA_TWP = NA_TW + (size_t)NA_MAX_NZ * sizeof(double2);   // double2[< nz]
+constexpr size_t NA_KF = NA_TWP + (size_t)NA_MAX_NZ * sizeof(double2);   // double2[nz]
+constexpr size_t NA_DIR = NA_KF + (size_t)NA_MAX_NZ * sizeof(double2);   // double[Cz*oz]
+constexpr size_t NA_REV = NA_DIR + (size_t)NA_MAX_CD * sizeof(double);   // int[nz]
+constexpr size_t NA_BYTES = NA_REV + (size_t)NA_MAX_NZ * sizeof(int);    // 224 KiB
+
+static __device__ __align__(256) unsigned char g_noalloc_tables[NA_BYTES];
+
+// host staging, laid out like the device array; serialised by na_mutex
+static unsigned char na_host[NA_BYTES];
+static std::mutex na_mutex;
+static void* na_dev[64];  // device address of g_noalloc_tables, per device
+
+int na_setup(int dev) {
+  if (dev < 0 || dev >= 64) return SPH_EINVAL;
+  if (na_dev[dev]) return SPH_OK;
+  void* ptr = nullptr;
+  if (cudaGetSymbolAddress(&ptr, g_noalloc_tables) != cudaSuccess || !ptr) return SPH_ECUDA;
+  na_dev[dev] = ptr;
+  return SPH_OK;
+}
+
+}  // namespace
+
+extern "C" int sph_derivr_noalloc(const double* a, double* b, int nlm, int nz, int Cz, int oz, double rint,
+                                  double rext, const double* dir, int p, void* stream) {
+  if (!a || !b || nlm < 1 || nz < 2 || nz > NA_MAX_NZ || p < 1 || p > 4) return SPH_EINVAL;
+  if (Cz < 0 || oz < 0 || (Cz > 0 && (oz < 1 || nz - Cz < oz || !dir)) || (size_t)Cz * oz > NA_MAX_CD)
+    return SPH_EINVAL;
+  // radix plan (8s, then 4, 2, 3, other primes), as sph_plan_create builds it
+  FftDesc fd = {};
+  fd.n = nz;
+  {
+    int r = nz, Ns = 1;
+    for (int q : {8, 4, 2, 3})
+      while (r % q == 0) {
+        if (fd.npass >= SPH_MAX_PASSES) return SPH_EINVAL;
+        fd.pass[fd.npass++] = {q, Ns};
+        Ns *= q;
+        r /= q;
+      }
+    for (int q = 5; r > 1; q += 2)
+      while (r % q == 0) {
+        if (q > 64 || fd.npass >= SPH_MAX_PASSES) return SPH_EINVAL;
+        fd.pass[fd.npass++] = {q, Ns};
+        Ns *= q;
+        r /= q;
+      }
+  }
+  int LB = 64;
+  while (LB > 1 && LB * nz > ZMAXCOL) LB >>= 1;
+  if (LB * nz > ZMAXCOL) return SPH_EINVAL;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return SPH_ECUDA;
+  std::lock_guard<std::mutex> lock(na_mutex);
+  int rc = na_setup(dev);
+  if (rc != SPH_OK) return rc;
+
+  const long double pi = 3.141592653589793238462643383279502884L;
+  double2* tw = reinterpret_cast<double2*>(na_host + NA_TW);
+  double2* twp = reinterpret_cast<double2*>(na_host + NA_TWP);
+  double2* kf = reinterpret_cast<double2*>(na_host + NA_KF);
+  double* dr = reinterpret_cast<double*>(na_host + NA_DIR);
+  int* rev = reinterpret_cast<int*>(na_host + NA_REV);
+  for (int e = 0; e < nz; ++e) {
+    long double ang = -2.0L * pi * e / nz;
+    tw[e] = make_double2((double)cosl(ang), (double)sinl(ang));
+  }
+  int ntp = 0;  // per-pass twiddles [pass][j][r-1] = W_L^{j r}
+  for (int L = nz; L > 1;) {
+    int R = L % 8 == 0 ? 8 : L % 4 == 0 ? 4 : L % 2 == 0 ? 2 : L % 3 == 0 ? 3 : L;
+    int S = L / R;
+    for (int j = 0; j < S; ++j)
+      for (int r = 1; r < R; ++r) {
+        long double ang = -2.0L * pi * (long double)((long)j * r) / L;
+        twp[ntp++] = make_double2((double)cosl(ang), (double)sinl(ang));
+      }
+    L = S;
+  }
+  for (int k = 0; k < nz; ++k) {
+    int t = k, s = nz, pos = 0;
+    for (int ip = 0; ip < fd.npass; ++ip) {
+      s /= fd.pass[ip].R;
+      pos += (t % fd.pass[ip].R) * s;
+      t /= fd.pass[ip].R;
+    }
+    rev[k] = pos;
+  }
+  // kz as box_init builds it (src/pseudo/pseudospec_mod.f90:196-227), times i^p
+  const int N = nz - Cz;
+  const double dz = N > 1 ? (rext - rint) / (nz - Cz - 1) : 1.0;
+  const double Dkz = 2.0 * 3.14159265358979323846 / (dz * nz);
+  for (int k = 0; k < nz; ++k) {
+    double kzk;
+    if (nz % 2 == 0) kzk = (double)(k < nz / 2 ? k : k - nz) * Dkz;
+    else kzk = (double)(k < (nz + 1) / 2 ? k : k - nz) * Dkz;
+    double kp = 1.0;
+    for (int q = 0; q < p; ++q) kp *= kzk;
+    double re = (p % 4 == 0) ? 1 : (p % 4 == 2) ? -1 : 0;
+    double im = (p % 4 == 1) ? 1 : (p % 4 == 3) ? -1 : 0;
+    kf[k] = make_double2(re * kp, im * kp);
+  }
+  for (int q = 0; q < Cz * oz; ++q) dr[q] = dir[q];
+
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned char* dbase = static_cast<unsigned char*>(na_dev[dev]);
+  const size_t spans[][2] = {{NA_TW, (size_t)nz * sizeof(double2)},
+                             {NA_TWP, (size_t)(ntp > 0 ? ntp : 1) * sizeof(double2)},
+                             {NA_KF, (size_t)nz * sizeof(double2)},
+                             {NA_DIR, (size_t)(Cz * oz > 0 ? Cz * oz : 1) * sizeof(double)},
+                             {NA_REV, (size_t)nz * sizeof(int)}};
+  for (auto& sp : spans)
+    if (cudaMemcpyAsync(dbase + sp[0], na_host + sp[0], sp[1], cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return SPH_ECUDA;
+
+  fd.tw = reinterpret_cast<const double2*>(dbase + NA_TW);
+  fd.twp = reinterpret_cast<const double2*>(dbase + NA_TWP);
+  fd.rev = reinterpret_cast<const int*>(dbase + NA_REV);
+  ZArgs z = {};
+  z.in = reinterpret_cast<const double2*>(a);
+  z.out = reinterpret_cast<double2*>(b);
+  z.nlm = nlm;
+  z.nz = nz;
+  z.N = N;
+  z.C = Cz;
+  z.d = oz;
+  z.LB = LB;
+  z.order = p;
+  z.dir = reinterpret_cast<const double*>(dbase + NA_DIR);
+  z.kfac = reinterpret_cast<const double2*>(dbase + NA_KF);
+  z.fd = fd;
+  const int nblocks = (nlm + LB - 1) / LB;
+  const size_t smem = (size_t)LB * nz * sizeof(double2);
+  return launch_mode<Z_DERIV>(z, nblocks, smem, st);
 }

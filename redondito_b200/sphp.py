@@ -45,6 +45,7 @@ SYMBOLS = (
     "sph_setup_bc", "sph_dirichlet", "sph_invDl", "sph_v_imposebc", "sph_v_imposebc_fast",
     "sph_nl_rhs", "sph_rk3_step",
     "sph_timer_enable", "sph_timer_reset", "sph_timer_read",
+    "sph_derivr_noalloc",
 )
 TIMER_CLASSES = ("phi_fwd", "phi_inv", "leg_analysis", "leg_synthesis", "vec_analysis",
                  "vec_synthesis", "zfft", "ops")
@@ -104,6 +105,7 @@ def lib(build_if_missing=True):
             "sph_timer_enable": [P, I],
             "sph_timer_reset": [P],
             "sph_timer_read": [P, pD, pI],
+            "sph_derivr_noalloc": [Vp, Vp, I, I, I, I, D, D, pD, I, Vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -260,6 +262,19 @@ def fftp2d_qst_to_vec(plan, q, s, t, vr, vt, vp, stream=None):
 # ---------------------------------------------------------------- operators
 def derivr(plan, a, b, p, esp, stream=None):
     _call("sph_derivr", plan.h, _s(plan, a), _s(plan, b), int(p), esp.encode()[:1], _stream(stream))
+
+
+def derivr_noalloc(a, b, nz, Cz, oz, rint, rext, dir, p, stream=None):
+    """Radial derivative without a plan and without allocation (see
+    sph_derivr_noalloc in include/sph_b200.h); a, b complex128 (nz, nlm)."""
+    nlm = a.shape[1]
+    if tuple(b.shape) != tuple(a.shape) or a.shape[0] != nz:
+        raise ValueError("a and b must both be (nz, nlm)")
+    d = None
+    if Cz > 0:
+        d = (ctypes.c_double * (Cz * oz))(*dir)
+    _call("sph_derivr_noalloc", ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(b.data_ptr()), nlm, nz,
+          Cz, oz, float(rint), float(rext), d, int(p), _stream(stream))
 
 
 def laplang(plan, a, b, stream=None):
