@@ -54,8 +54,12 @@ typedef struct sph_plan sph_plan;
  *   rint, rext   : shell radii; z(k) = rint + k*dz, dz = (rext-rint)/(nz-Cz-1)
  *   dir          : host pointer, Cz x oz column-major continuation operator
  *                  dir = A.Q^T (see sph_fcgram_load_tables); NULL if Cz == 0
- *   precision    : SPH_FP64 or SPH_MIXED (Legendre on tensor cores in
- *                  compensated bf16 / scaled fp16, FFTs in fp32)
+ *   precision    : SPH_FP64, or SPH_MIXED: Legendre contractions on the
+ *                  tensor cores as three fp16 products of power-of-two
+ *                  scaled hi/lo splits with fp32 accumulation, phi FFTs in
+ *                  fp32 (relative L2 error ~1e-7); z transforms and
+ *                  operators stay FP64.  SPH_MIXED needs nphi = 3*2^a,
+ *                  12 <= nphi <= 6144.
  * Allocates the plan's device tables and scratch with cudaMalloc on the
  * current device. */
 int sph_plan_create(sph_plan** plan, int lmax, int nlat, int nphi, int nz, int Cz, int oz,
@@ -213,6 +217,14 @@ int sph_rk3_step(sph_plan* plan, double* Z, double* W, double* phi, double nu, d
 int sph_timer_enable(sph_plan* plan, int on);
 int sph_timer_reset(sph_plan* plan);
 int sph_timer_read(sph_plan* plan, double* ms, int* launches);
+
+/* Device status of a plan (no reference counterpart: the reference's
+ * kernels have no bounded waits).  The tensor-core kernels of an SPH_MIXED
+ * plan bound every wait on a shared-memory barrier; one that gives up
+ * records it in the plan.  Synchronises the device, then returns
+ * SPH_ETIMEDOUT if any wait gave up since the plan was created (the
+ * outputs of those calls are invalid) and clears the record, else SPH_OK. */
+int sph_plan_status(sph_plan* plan);
 
 #ifdef __cplusplus
 }

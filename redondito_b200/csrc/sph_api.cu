@@ -163,6 +163,7 @@ static int upload(T** dst, const T* src, size_t n) {
 
 static void plan_free(sph_plan* p) {
   for (auto e : p->ev_pool) cudaEventDestroy(e);
+  mixed_free(p);
   void* ptrs[] = {p->P, p->dP, p->mPs, p->wfold, p->wfull, p->d_dir, p->d_z, p->kfac, p->filt,
                   p->zinv2, p->d_ell, p->d_mbase, p->twz, p->twphi, p->twzf, p->twphif, p->revz,
                   p->revphi, p->twpz, p->twpphi, p->twpzf, p->twpphif, p->tilesA,
@@ -196,6 +197,7 @@ extern "C" int sph_plan_create(sph_plan** out, int lmax, int nlat, int nphi, int
   if (Cz < 0 || oz < 0 || (Cz > 0 && (oz < 1 || nz - Cz < oz || !dir))) return SPH_EINVAL;
   if (precision != SPH_FP64 && precision != SPH_MIXED) return SPH_EINVAL;
   if (nz > 4096 || nphi > 8192) return SPH_EINVAL;
+  if (precision == SPH_MIXED && !mixed_nphi_ok(nphi)) return SPH_EINVAL;
   sph_plan* p = new sph_plan();
   p->lmax = lmax;
   p->nlat = nlat;
@@ -354,6 +356,7 @@ extern "C" int sph_plan_create(sph_plan** out, int lmax, int nlat, int nphi, int
   if (rc == SPH_OK && cudaMemset(p->G, 0, SPH_MAX_FIELDS * p->Gfield * sizeof(double2)) != cudaSuccess)
     rc = SPH_ECUDA;
   if (rc == SPH_OK && cudaMalloc((void**)&p->energy, sizeof(double)) != cudaSuccess) rc = SPH_ENOMEM;
+  if (rc == SPH_OK && precision == SPH_MIXED) rc = mixed_setup(p, hP, hdP, hmPs);
   if (rc != SPH_OK) {
     plan_free(p);
     return rc;
@@ -441,6 +444,14 @@ void timer_stop(const sph_plan* cp, int slot, cudaStream_t st) {
   cudaEventRecord(p->ev_pool[2 * slot + 1], st);
 }
 
+extern "C" int sph_plan_status(sph_plan* p) {
+  if (!p) return SPH_EINVAL;
+  SPH_CUDA_OK(cudaDeviceSynchronize());
+  const int rc = mixed_status(p);
+  if (rc == SPH_ETIMEDOUT) SPH_CUDA_OK(cudaMemset(p->dflag, 0, sizeof(int)));
+  return rc;
+}
+
 extern "C" int sph_timer_enable(sph_plan* p, int on) {
   if (!p) return SPH_EINVAL;
   p->timing = on ? 1 : 0;
@@ -482,14 +493,22 @@ extern "C" int sph_timer_read(sph_plan* p, double* ms, int* launches) {
 extern "C" int sph_fftp2d_real_to_complex_xy(sph_plan* p, const double* in, double* out, void* s) {
   if (!p || !in || !out) return SPH_EINVAL;
   const double* g[1] = {in};
+  if (p->precision == SPH_MIXED) {
+    RC(launch_phi_fwd32(p, g, 1, ST(s)));
+    return launch_tc_analysis(p, 0, D2(out), nullptr, ST(s));
+  }
   RC(launch_phi_fwd(p, g, 1, ST(s)));
   return launch_leg_analysis(p, 0, D2(out), ST(s));
 }
 
 extern "C" int sph_fftp2d_complex_to_real_xy(sph_plan* p, const double* in, double* out, void* s) {
   if (!p || !in || !out) return SPH_EINVAL;
-  RC(launch_leg_synthesis(p, CD2(in), 0, ST(s)));
   double* g[1] = {out};
+  if (p->precision == SPH_MIXED) {
+    RC(launch_tc_synthesis(p, 0, CD2(in), nullptr, ST(s)));
+    return launch_phi_inv32(p, g, 1, ST(s));
+  }
+  RC(launch_leg_synthesis(p, CD2(in), 0, ST(s)));
   return launch_phi_inv(p, g, 1, ST(s));
 }
 
@@ -517,6 +536,11 @@ extern "C" int sph_fftp2d_vec_to_qst(sph_plan* p, const double* vr, const double
                                      double* q, double* sO, double* t, void* s) {
   if (!p || !vr || !vt || !vp || !q || !sO || !t) return SPH_EINVAL;
   const double* g[3] = {vr, vt, vp};
+  if (p->precision == SPH_MIXED) {
+    RC(launch_phi_fwd32(p, g, 3, ST(s)));
+    RC(launch_tc_analysis(p, 0, D2(q), nullptr, ST(s)));
+    return launch_tc_analysis(p, 1, D2(sO), D2(t), ST(s));
+  }
   RC(launch_phi_fwd(p, g, 3, ST(s)));
   RC(launch_leg_analysis(p, 0, D2(q), ST(s)));
   return launch_vec_analysis(p, D2(sO), D2(t), ST(s));
@@ -525,9 +549,14 @@ extern "C" int sph_fftp2d_vec_to_qst(sph_plan* p, const double* vr, const double
 extern "C" int sph_fftp2d_qst_to_vec(sph_plan* p, const double* q, const double* sI, const double* t,
                                      double* vr, double* vt, double* vp, void* s) {
   if (!p || !vr || !vt || !vp || !q || !sI || !t) return SPH_EINVAL;
+  double* g[3] = {vr, vt, vp};
+  if (p->precision == SPH_MIXED) {
+    RC(launch_tc_synthesis(p, 0, CD2(q), nullptr, ST(s)));
+    RC(launch_tc_synthesis(p, 1, CD2(sI), CD2(t), ST(s)));
+    return launch_phi_inv32(p, g, 3, ST(s));
+  }
   RC(launch_leg_synthesis(p, CD2(q), 0, ST(s)));
   RC(launch_vec_synthesis(p, CD2(sI), CD2(t), ST(s)));
-  double* g[3] = {vr, vt, vp};
   return launch_phi_inv(p, g, 3, ST(s));
 }
 

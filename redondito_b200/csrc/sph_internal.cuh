@@ -2,6 +2,7 @@
 // shared by the CUDA sources of the transform core.
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -33,6 +34,24 @@ struct FftDesc {
 // Legendre GEMM work tile: one (m, row block) pair.
 struct LegTile {
   int m, r0;
+};
+
+// Mixed-precision (tcgen05) work item: one m, one parity (or output fold),
+// one block of at most 256 MMA rows; its Legendre table tiles sit in HBM as
+// nk consecutive blocks of [hi | lo] fp16 (2 x nr x 32 halves each, 8x8 core
+// matrices, K-major), pre-scaled by the power of two tscale.
+struct TcItem {
+  int m, par, r0, nr, nvalid, nk, nk1, out;
+  long long boff;  // first table block, in halves
+  float tscale;
+  int pad_;
+};
+
+struct TcSet {
+  TcItem* items = nullptr;  // device
+  int nitems = 0;
+  __half* blocks = nullptr;  // device
+  size_t nhalves = 0;
 };
 
 struct sph_plan {
@@ -90,6 +109,13 @@ struct sph_plan {
   double* binv = nullptr;   // [lmax][N-4][N]  M_l column-major per l
   double* d2bor = nullptr;  // [N][4]
   double* energy = nullptr; // device accumulator (1 double)
+  // mixed precision: fp16 hi/lo tables for the tcgen05 GEMMs, fp32 folded
+  // coefficients G32 (reusing the G allocation), running data maxima
+  TcSet tcAS, tcAV, tcSS, tcSV;  // analysis scalar/vector, synthesis scalar/vector
+  int ldn8 = 0;                  // node stride of G32 (nlat/2 rounded up to 8)
+  size_t G32field = 0;           // float2 elements per G32 field
+  float* dmax = nullptr;         // [4] max |value| per data operand (bit-compared)
+  int* dflag = nullptr;          // device status word (bounded waits that gave up)
   // stage timers (sph_timer_*): event pairs recorded around each launch
   int timing = 0;
   std::vector<cudaEvent_t> ev_pool;
@@ -158,6 +184,18 @@ int launch_qst_scale(const sph_plan* p, const double2* in, double2* out, int rpo
                      double sc, cudaStream_t st);
 int launch_energy(const sph_plan* p, const double* ur, const double* ut, const double* up,
                   double* acc, cudaStream_t st);
+
+// mixed precision (k_mixed.cu)
+int mixed_setup(sph_plan* p, const std::vector<double>& hP, const std::vector<double>& hdP,
+                const std::vector<double>& hmPs);
+void mixed_free(sph_plan* p);
+int launch_phi_fwd32(const sph_plan* p, const double* const* grids, int nfields, cudaStream_t st);
+int launch_phi_inv32(const sph_plan* p, double* const* grids, int nfields, cudaStream_t st);
+int launch_tc_analysis(const sph_plan* p, int vector, double2* out, double2* out2, cudaStream_t st);
+int launch_tc_synthesis(const sph_plan* p, int vector, const double2* in, const double2* in2,
+                        cudaStream_t st);
+int mixed_status(const sph_plan* p);
+bool mixed_nphi_ok(int nphi);  // phi lengths the fp32 phi kernels are built for
 
 #define SPH_CUDA_OK(call)                     \
   do {                                        \

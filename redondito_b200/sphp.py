@@ -45,7 +45,7 @@ SYMBOLS = (
     "sph_setup_bc", "sph_dirichlet", "sph_invDl", "sph_v_imposebc", "sph_v_imposebc_fast",
     "sph_nl_rhs", "sph_rk3_step",
     "sph_timer_enable", "sph_timer_reset", "sph_timer_read",
-    "sph_derivr_noalloc",
+    "sph_derivr_noalloc", "sph_plan_status",
 )
 TIMER_CLASSES = ("phi_fwd", "phi_inv", "leg_analysis", "leg_synthesis", "vec_analysis",
                  "vec_synthesis", "zfft", "ops")
@@ -106,6 +106,7 @@ def lib(build_if_missing=True):
             "sph_timer_reset": [P],
             "sph_timer_read": [P, pD, pI],
             "sph_derivr_noalloc": [Vp, Vp, I, I, I, I, D, D, pD, I, Vp],
+            "sph_plan_status": [P],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -356,6 +357,12 @@ def timer_enable(plan, on=True):
 
 def timer_reset(plan):
     _call("sph_timer_reset", plan.h)
+
+
+def plan_status(plan):
+    """Raises SphError(SPH_ETIMEDOUT) if a bounded device wait of the plan's
+    tensor-core kernels gave up since the last check."""
+    _call("sph_plan_status", plan.h)
 
 
 def timer_read(plan):
