@@ -6,8 +6,8 @@ and a vector field (3 components) at lmax = 511, Gauss grid 768 x 1536,
 nz = 256 radial points with FC-Gram C = 25, d = 5 continuation, r in
 [0.35, 1].  The state lives in (lm, kz) space; a pair is
     scalar: fftp3d_complex_to_real + fftp3d_real_to_complex
-    vector: 3 x fftp1d_complex_to_real_z + fftp2d_qst_to_vec
-            + fftp2d_vec_to_qst + 3 x fftp1d_real_to_complex_z
+    vector: fftp3d_qst_to_vec + fftp3d_vec_to_qst (the z transforms of q,
+            s, t composed with the 2D vector transforms)
 Synthetic seeded inputs stand in for a simulation state: coefficients
 N(0,1) (l+1)^-2.5 (real for m = 0) with 1% of the (r, l, m) entries set to
 amplitude 1e3 and random phase, taken to (lm, kz) by the forward z
@@ -206,13 +206,9 @@ def pair(S, P, st, grids):
     a, q, s, t = st
     g0, g1, g2, g3 = grids
     S.fftp3d_complex_to_real(P, a, g0)
-    for x in (q, s, t):
-        S.fftp1d_complex_to_real_z(P, x)
-    S.fftp2d_qst_to_vec(P, q, s, t, g1, g2, g3)
+    S.fftp3d_qst_to_vec(P, q, s, t, g1, g2, g3)
     S.fftp3d_real_to_complex(P, g0, a)
-    S.fftp2d_vec_to_qst(P, g1, g2, g3, q, s, t)
-    for x in (q, s, t):
-        S.fftp1d_real_to_complex_z(P, x)
+    S.fftp3d_vec_to_qst(P, g1, g2, g3, q, s, t)
 
 
 def fp64_peak():

@@ -121,6 +121,20 @@ int sph_fftp2d_vec_to_qst(sph_plan* plan, const double* vr, const double* vt, co
 int sph_fftp2d_qst_to_vec(sph_plan* plan, const double* q, const double* s, const double* t,
                           double* vr, double* vt, double* vp, void* stream);
 
+/* 3D vector transforms (no reference counterpart: the reference composes
+ * them in its nonlinear-term code as fftp2d_vec_to_qst followed by
+ * fftp1d_real_to_complex_z on q, s and t, and fftp1d_complex_to_real_z on
+ * q, s, t followed by fftp2d_qst_to_vec; these entry points compute exactly
+ * those compositions).  sph_fftp3d_qst_to_vec transforms q, s, t in place
+ * in z, like sph_fftp3d_complex_to_real.  On SPH_MIXED plans with FC-Gram
+ * continuation the forward one continues the physical planes in FP64 before
+ * the angular analysis, which keeps the continuation from amplifying the
+ * angular round-off (the same holds for sph_fftp3d_real_to_complex). */
+int sph_fftp3d_vec_to_qst(sph_plan* plan, const double* vr, const double* vt, const double* vp, double* q,
+                          double* s, double* t, void* stream);
+int sph_fftp3d_qst_to_vec(sph_plan* plan, double* q, double* s, double* t, double* vr, double* vt, double* vp,
+                          void* stream);
+
 /* ---------------------------------------------------------------- operators
  * src/pseudo/pseudospec_hd.f90.  Spectral arrays are (nlm,nz) complex. */
 

@@ -81,8 +81,15 @@ struct LegArgs {
   double2* out2;
   const LegTile* tiles;
   const int* mbase;
-  int lmax, ldn, nz, nlm;
+  const int* kzl;  // planes to transform (nullptr: all nz)
+  int lmax, ldn, nz, nlm, nkz;
 };
+
+// plane of local index kl (blockIdx.y * KZ + offset); ok = within the selection
+__device__ __forceinline__ int plane_of(const LegArgs& a, int kl, bool& ok) {
+  ok = kl < a.nkz;
+  return a.kzl ? (ok ? __ldg(a.kzl + kl) : 0) : kl;
+}
 
 constexpr int STAGES = 3;
 
@@ -121,8 +128,9 @@ __global__ void __launch_bounds__(128) leg_analysis_kernel(LegArgs a) {
     }
     for (int c = tid; c < 2 * KZ * K; c += 128) {  // B: [par][plane][node] complex
       int i_ = c % K, r = c / K, kzl = r % KZ, pr = r / KZ;
-      int kz = kz0 + kzl, i = k0 + i_;
-      bool ok = kz < a.nz && i < a.ldn;
+      bool ok;
+      int kz = plane_of(a, kz0 + kzl, ok), i = k0 + i_;
+      ok = ok && i < a.ldn;
       const double2* src = ok ? G + ((size_t)pr * a.nz + kz) * a.ldn + i : a.G;
       cp16(Bs + ((pr * KZ + kzl) * LDB + i_) * 2, src, ok);
     }
@@ -172,8 +180,9 @@ __global__ void __launch_bounds__(128) leg_analysis_kernel(LegArgs a) {
   const int nvalid = min(L, a.lmax + 1 - l0);
   for (int idx = tid; idx < KZ * L; idx += 128) {
     int pl = idx / L, ll = idx - pl * L;
-    int kz = kz0 + pl;
-    if (kz >= a.nz || ll >= nvalid) continue;
+    bool okz;
+    int kz = plane_of(a, kz0 + pl, okz);
+    if (!okz || ll >= nvalid) continue;
     double2 v = Cs[idx];
     if (m == 0) v.y = 0.0;  // m = 0 coefficients of a real field are real
     a.out[(size_t)kz * a.nlm + base_lm + l0 + ll] = v;
@@ -213,8 +222,9 @@ __global__ void __launch_bounds__(256) leg_synthesis_kernel(LegArgs a) {
     }
     for (int c = tid; c < K * KZ; c += 256) {
       int q = c % K, pl = c / K;
-      int l = lk + q, kz = kz0 + pl;
-      bool ok = l <= a.lmax && kz < a.nz;
+      bool ok;
+      int l = lk + q, kz = plane_of(a, kz0 + pl, ok);
+      ok = ok && l <= a.lmax;
       const double2* src = ok ? a.spec + (size_t)kz * a.nlm + base_lm + l : a.spec;
       cp16(Bs + ((q & 1) * (K / 2) + (q >> 1)) * LDB + 2 * pl, src, ok);
     }
@@ -255,8 +265,9 @@ __global__ void __launch_bounds__(256) leg_synthesis_kernel(LegArgs a) {
 #pragma unroll
     for (int nt = 0; nt < 4; ++nt) {
       int i = i0 + mh * 32 + mt * 8 + g;
-      int kz = kz0 + nh * 16 + nt * 4 + t;
-      if (i < a.ldn && kz < a.nz) G[(size_t)kz * a.ldn + i] = make_double2(acc[mt][nt][0], acc[mt][nt][1]);
+      bool okz;
+      int kz = plane_of(a, kz0 + nh * 16 + nt * 4 + t, okz);
+      if (i < a.ldn && okz) G[(size_t)kz * a.ldn + i] = make_double2(acc[mt][nt][0], acc[mt][nt][1]);
     }
 }
 
@@ -317,8 +328,9 @@ __global__ void __launch_bounds__(256) vec_analysis_kernel(LegArgs a) {
     }
     for (int c = tid; c < 2 * 2 * KZ * K; c += 256) {  // 2 fields x 2 folds x 32 planes x 8 nodes
       int i_ = c % K, r = c / K, kzl = r % KZ, r2 = r / KZ, fo = r2 & 1, fl = r2 >> 1;
-      int kz = kz0 + kzl, i = k0 + i_;
-      bool ok = kz < a.nz && i < a.ldn;
+      bool ok;
+      int kz = plane_of(a, kz0 + kzl, ok), i = k0 + i_;
+      ok = ok && i < a.ldn;
       const double2* Gf = fl ? Gp : Gt;
       const double2* src = ok ? Gf + ((size_t)fo * a.nz + kz) * a.ldn + i : a.G;
       cp16(Bs + (((fl * 2 + fo) * KZ + kzl) * LDB + i_) * 2, src, ok);
@@ -368,8 +380,9 @@ __global__ void __launch_bounds__(256) vec_analysis_kernel(LegArgs a) {
   const int nvalid = min(L, a.lmax + 1 - l0);
   for (int idx = tid; idx < 2 * KZ * L; idx += 256) {
     int ll = idx % L, r = idx / L, pl = r % KZ, o = r / KZ;
-    int kz = kz0 + pl;
-    if (kz >= a.nz || ll >= nvalid) continue;
+    bool okz;
+    int kz = plane_of(a, kz0 + pl, okz);
+    if (!okz || ll >= nvalid) continue;
     int l = l0 + ll;
     double f = l ? 1.0 / ((double)l * (double)(l + 1)) : 0.0;
     double2 v = Cs[idx];
@@ -433,8 +446,9 @@ __global__ void __launch_bounds__(256) vec_synthesis_kernel(LegArgs a) {
     }
     for (int c = tid; c < 2 * K * KZ; c += 256) {
       int qq = c % K, r = c / K, pl = r % KZ, fl = r / KZ;
-      int l = lk + qq, kz = kz0 + pl;
-      bool ok = l <= a.lmax && kz < a.nz && l > 0;
+      bool ok;
+      int l = lk + qq, kz = plane_of(a, kz0 + pl, ok);
+      ok = ok && l <= a.lmax && l > 0;
       const double2* sp = fl ? a.spec2 : a.spec;
       const double2* src = ok ? sp + (size_t)kz * a.nlm + base_lm + l : a.spec;
       cp16(Bs + (fl * K + (qq & 1) * (K / 2) + (qq >> 1)) * LDB + 2 * pl, src, ok);
@@ -480,8 +494,9 @@ __global__ void __launch_bounds__(256) vec_synthesis_kernel(LegArgs a) {
 #pragma unroll
     for (int nt = 0; nt < 4; ++nt) {
       int i = i0 + mt * 8 + g;
-      int kz = kz0 + nh * 16 + nt * 4 + t;
-      if (kz < a.nz && i < a.ldn) G[(size_t)kz * a.ldn + i] = make_double2(acc[mt][nt][0], acc[mt][nt][1]);
+      bool okz;
+      int kz = plane_of(a, kz0 + nh * 16 + nt * 4 + t, okz);
+      if (okz && i < a.ldn) G[(size_t)kz * a.ldn + i] = make_double2(acc[mt][nt][0], acc[mt][nt][1]);
     }
 }
 
@@ -498,6 +513,8 @@ LegArgs base_args(const sph_plan* p) {
   a.ldn = p->ldn;
   a.nz = p->nz;
   a.nlm = p->nlm;
+  a.kzl = p->sel_kz;
+  a.nkz = p->sel_kz ? p->sel_n : p->nz;
   return a;
 }
 
@@ -516,7 +533,7 @@ int launch_leg_analysis(const sph_plan* p, int gfield, double2* spec, cudaStream
   a.tiles = p->tilesA;
   static bool once = set_smem(leg_analysis_kernel, an::SMEM);
   if (!once) return SPH_ECUDA;
-  dim3 grid(p->ntilesA, (p->nz + an::KZ - 1) / an::KZ);
+  dim3 grid(p->ntilesA, (a.nkz + an::KZ - 1) / an::KZ);
   TimedLaunch tl(p, T_LEG_ANA, st);
   leg_analysis_kernel<<<grid, 128, an::SMEM, st>>>(a);
   SPH_LAUNCH_OK();
@@ -530,7 +547,7 @@ int launch_leg_synthesis(const sph_plan* p, const double2* spec, int gfield, cud
   a.tiles = p->tilesS;
   static bool once = set_smem(leg_synthesis_kernel, sy::SMEM);
   if (!once) return SPH_ECUDA;
-  dim3 grid(p->ntilesS, (p->nz + sy::KZ - 1) / sy::KZ);
+  dim3 grid(p->ntilesS, (a.nkz + sy::KZ - 1) / sy::KZ);
   TimedLaunch tl(p, T_LEG_SYN, st);
   leg_synthesis_kernel<<<grid, 256, sy::SMEM, st>>>(a);
   SPH_LAUNCH_OK();
@@ -544,7 +561,7 @@ int launch_vec_analysis(const sph_plan* p, double2* s, double2* t, cudaStream_t 
   a.tiles = p->tilesA;
   static bool once = set_smem(vec_analysis_kernel, va::SMEM);
   if (!once) return SPH_ECUDA;
-  dim3 grid(p->ntilesA, (p->nz + va::KZ - 1) / va::KZ);
+  dim3 grid(p->ntilesA, (a.nkz + va::KZ - 1) / va::KZ);
   TimedLaunch tl(p, T_VEC_ANA, st);
   vec_analysis_kernel<<<grid, 256, va::SMEM, st>>>(a);
   SPH_LAUNCH_OK();
@@ -558,7 +575,7 @@ int launch_vec_synthesis(const sph_plan* p, const double2* s, const double2* t, 
   a.tiles = p->tilesS32;
   static bool once = set_smem(vec_synthesis_kernel, vs::SMEM);
   if (!once) return SPH_ECUDA;
-  dim3 grid(p->ntilesS32, (p->nz + vs::KZ - 1) / vs::KZ);
+  dim3 grid(p->ntilesS32, (a.nkz + vs::KZ - 1) / vs::KZ);
   TimedLaunch tl(p, T_VEC_SYN, st);
   vec_synthesis_kernel<<<grid, 256, vs::SMEM, st>>>(a);
   SPH_LAUNCH_OK();

@@ -1,24 +1,37 @@
 // k_mixed.cu -- the mixed-precision form (SPH_MIXED) of the angular transforms.
 //
-// * phi FFTs in fp32 (twiddles derived in FP64 on the host) between the FP64
-//   grid and fp32 folded coefficients G32[field][m][parity][plane][node].
+// * phi FFTs in fp32 (twiddles derived in FP64 on the host).
 // * Legendre contractions on the 5th-generation tensor cores
-//   (tcgen05.mma kind::f16, fp32 accumulation in TMEM).  Each operand x is
-//   scaled by a power of two s and split as x s = hi + lo (both fp16); the
-//   product uses hi*hi + hi*lo + lo*hi, which keeps about 22 significant
-//   bits of each operand.  The Legendre tables are split on the host, per
-//   work item scaled by a power of two, and stored as ready-made
-//   shared-memory tiles (8x8 core matrices, K-major) that one bulk copy
-//   moves per K step.  The data operand is split on the fly by four producer
-//   warps with a per-field power-of-two scale from the data's maximum.
-// * Outputs are unscaled exactly (powers of two) and written in FP64
-//   (spectra) or fp32 (G32).
+//   (tcgen05.mma kind::f16 with bf16 operands, fp32 accumulation in TMEM).
+//   Every operand value x is split into three bf16 pieces x = hi + mid + lo
+//   (8 significant bits each, so an fp32 value is represented exactly and
+//   no scaling is needed: bf16 has the fp32 exponent range).  A product
+//   keeps the six piece products of order <= 2 (hi.hi, hi.mid, mid.hi,
+//   hi.lo, mid.mid, lo.hi), about 24 bits.  The tensor cores align the
+//   addends of one MMA to the largest exponent and truncate below it, so
+//   hi.hi (16-bit products, kept exactly against the running sum) and the
+//   five small products accumulate in two separate TMEM column ranges; the
+//   epilogue adds them in FP64.
+// * The data operand is split ONCE, by the kernel that produces it, into
+//   ready-made shared-memory tiles: 3 pieces x [128 rows = 64 planes x
+//   (re, im)] x [32 K] bf16 in the no-swizzle K-major core-matrix layout,
+//   24 KB per tile, one bulk copy per K step.  The phi FFT writes the
+//   analysis tiles (K = Gauss nodes); spec_to_tiles writes the synthesis
+//   tiles (K = degrees l of one parity).  The Legendre tables are split on
+//   the host into the same layout.
+// * One persistent CTA per SM walks its work units (item x 64 planes); TMEM
+//   holds two accumulator sets, so the epilogue of a unit overlaps the main
+//   loop of the next.  Vector transforms keep the dP and mPs parts in
+//   separate accumulators and apply the +-i factors in the epilogue.
 //
-// MMA orientation: M = 128 data columns (64 planes x re/im), N = rows of one
-// parity (analysis: l; synthesis: nodes), K = nodes (analysis) or l
-// (synthesis), so the triangular shape of one m wastes at most 15 rows.
+// Warp roles of the tensor-core kernel: 0 bulk copies (one lane), 1 TMEM
+// allocation and MMA issue (one lane), 2-5 epilogue (TMEM lane quarters
+// 2, 3, 0, 1).
+#include <cuda_bf16.h>
+
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <thread>
 
 #include "fft_ct.cuh"
@@ -26,45 +39,48 @@
 
 namespace {
 
-constexpr int TK = 32;          // K tile (two k16 MMA steps)
-constexpr int MCOLS = 128;      // data columns per CTA (64 planes x re/im)
+constexpr int TK = 32;                              // K tile (two k16 MMA steps)
+constexpr int MCOLS = 128;                          // data columns per unit (64 planes x re/im)
 constexpr int PLANES = MCOLS / 2;
-constexpr int NRMAX = 256;      // largest N of one work item
+constexpr int NPIECE = 3;                           // bf16 pieces per value
+constexpr int PIECE_HALVES = MCOLS * TK;            // 4096 (8 KB)
+constexpr int TILE_HALVES = NPIECE * PIECE_HALVES;  // one data tile (24 KB)
+constexpr int NR_S = 128;                           // MMA N of scalar items
+constexpr int NR_V = 64;                            // MMA N of vector items (two parts)
+constexpr int A_BYTES = TILE_HALVES * 2;
+constexpr int B_BYTES = NPIECE * NR_S * TK * 2;     // 24 KB
 constexpr int STAGES = 4;
-constexpr int A_BYTES = MCOLS * TK * 2;        // 8 KB (one of hi/lo)
-constexpr int B_BYTES = 2 * NRMAX * TK * 2;    // 32 KB (hi | lo)
-constexpr int STAGE_BYTES = 2 * A_BYTES + B_BYTES;
-constexpr int TC_SMEM = STAGES * STAGE_BYTES + 256;
-constexpr int NPROD = 128;               // producer / epilogue threads (warps 0-3)
-constexpr int TC_THREADS = NPROD + 32;   // + one MMA-issue warp
-constexpr int UNITS = PLANES * (TK / 8) / NPROD;  // 8-element chunks per producer thread per tile
+constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int STG_WORDS = 32 * 17;                  // epilogue staging per warp (doubles)
+constexpr int OFF_STG = STAGES * STAGE_BYTES;
+constexpr int OFF_BAR = OFF_STG + 4 * STG_WORDS * 8;
+constexpr int NBARS = 2 * STAGES + 2 + 2 + 1;
+constexpr int TC_SMEM = OFF_BAR + NBARS * 8 + 16;
+constexpr int TC_THREADS = 6 * 32;
+constexpr int NEPI = 128;                           // epilogue threads
+constexpr int TMEM_COLS = 512;                      // two accumulator sets of 256 columns
 
 enum { ANA_S = 0, ANA_V = 1, SYN_S = 2, SYN_V = 3 };
 
 struct TcArgs {
   const TcItem* items;
-  const __half* blocks;
-  const float2* G32;     // folded coefficients (analysis input)
-  float2* G32w;          // (synthesis output)
+  const __nv_bfloat16* blocks;  // table tiles
+  const __nv_bfloat16* tiles;   // data tiles (analysis or synthesis layout)
+  size_t tfield;                // halves per field of the synthesis data tiles
+  const long long* toff;        // synthesis: [m][parity] first tile of the block
+  float2* G32w;                 // synthesis output (folded coefficients)
   size_t G32field;
-  const double2* in;     // spectra (synthesis input)
-  const double2* in2;
-  double2* out;          // spectra (analysis output)
+  double2* out;                 // analysis output (spectra)
   double2* out2;
   const int* mbase;
-  const float* dmax;     // maxima of the data operands
   int* flag;
-  int lmax, nz, nlm, ldn8;
+  int lmax, nz, nlm, ldn8, nkn, ncb, nunits;
 };
 
-// largest power of two s with mx * s < 2^14 (fp16 max 65504 leaves room for
-// the rounding of hi)
-__device__ __forceinline__ float pow2_scale(float mx) {
-  if (!(mx > 0.f) || !(mx < 3.0e38f)) return 1.f;
-  int e;
-  frexpf(mx, &e);  // mx = f 2^e, f in [0.5, 1)
-  return ldexpf(1.f, 14 - e);
+__host__ __device__ inline int rows_of(int lmax, int m, int par) {
+  return m + par > lmax ? 0 : (lmax - m - par) / 2 + 1;
 }
+__host__ __device__ inline int ntiles_of(int lmax, int m, int par) { return (rows_of(lmax, m, par) + TK - 1) / TK; }
 
 __device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
   asm volatile(
@@ -79,279 +95,313 @@ __device__ __forceinline__ void mbar_arrive_tx(uint64_t* b, uint32_t bytes) {
                "r"(bytes)
                : "memory");
 }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
-__host__ __device__ inline uint32_t tmem_cols(int nr) {
-  uint32_t c = 32;
-  while ((int)c < nr) c <<= 1;
-  return c;
+// x (fp32) = hi + mid + lo, each bf16 (round to nearest); exact for finite
+// x whose pieces stay in the bf16 normal range (|x| > ~2^-110).
+__device__ __forceinline__ void split3(float x, __nv_bfloat16& h, __nv_bfloat16& m, __nv_bfloat16& l) {
+  h = __float2bfloat16_rn(x);
+  const float r = x - __bfloat162float(h);
+  m = __float2bfloat16_rn(r);
+  l = __float2bfloat16_rn(r - __bfloat162float(m));
 }
 
-// Split 8 scaled values into hi/lo fp16 and store one 16-byte chunk each.
-__device__ __forceinline__ void store_split8(unsigned char* Ahi, unsigned char* Alo, int row, int chunk,
-                                             const float (&v)[8]) {
-  __align__(16) __half h[8], l[8];
+// Store NV consecutive K values of one row of a data tile, all three pieces.
+template <int NV>
+__device__ __forceinline__ void store_tile_row(__nv_bfloat16* tile, int row, int kk0, const float* v) {
+  static_assert(NV == 1 || NV == 2 || NV == 4 || NV == 8, "row chunk");
+  __align__(16) __nv_bfloat16 p[NPIECE][NV];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) tc05::split16(v[j], h[j], l[j]);
-  const uint32_t off = tc05::kmaj_off(row, chunk * 8, MCOLS);
-  *reinterpret_cast<uint4*>(Ahi + off) = *reinterpret_cast<const uint4*>(h);
-  *reinterpret_cast<uint4*>(Alo + off) = *reinterpret_cast<const uint4*>(l);
-}
-
-// forms of a complex data value: v, -v, i v, -i v
-enum { F_PLAIN = 0, F_NEG = 1, F_MULI = 2, F_MULMI = 3 };
-__device__ __forceinline__ float2 form_rt(float2 v, int f) {
-  switch (f) {
-    case F_NEG: return make_float2(-v.x, -v.y);
-    case F_MULI: return make_float2(-v.y, v.x);
-    case F_MULMI: return make_float2(v.y, -v.x);
-    default: return v;
+  for (int j = 0; j < NV; ++j) split3(v[j], p[0][j], p[1][j], p[2][j]);
+  const uint32_t off = tc05::kmaj_off(row, kk0, MCOLS) / 2;
+#pragma unroll
+  for (int s = 0; s < NPIECE; ++s) {
+    __nv_bfloat16* d = tile + s * PIECE_HALVES + off;
+    if constexpr (NV == 8) *reinterpret_cast<uint4*>(d) = *reinterpret_cast<const uint4*>(p[s]);
+    if constexpr (NV == 4) *reinterpret_cast<uint2*>(d) = *reinterpret_cast<const uint2*>(p[s]);
+    if constexpr (NV == 2) *reinterpret_cast<uint32_t*>(d) = *reinterpret_cast<const uint32_t*>(p[s]);
+    if constexpr (NV == 1) *d = p[s][0];
   }
 }
 
-// One CTA: one work item (blockIdx.y) x 64 planes (blockIdx.x).
+// ---------------------------------------------------------------- data tiles
+// Analysis tiles: [field][m][fold][plane block][node tile]
+__host__ __device__ inline size_t ana_tile(int lmax, int ncb, int nkn, int field, int m, int fold, int cb, int kt) {
+  return ((((size_t)field * (lmax + 1) + m) * 2 + fold) * ncb + cb) * nkn + kt;
+}
+// Synthesis tiles: per field, [m][parity] blocks of ncb x ntiles(m, parity)
+__device__ __forceinline__ size_t syn_tile(const long long* toff, int lmax, int m, int par, int cb, int kt) {
+  return (size_t)toff[2 * m + par] + (size_t)cb * ntiles_of(lmax, m, par) + kt;
+}
+
+// data tile and part (0: dP or scalar, 1: mPs) of K step kt of an item
+template <int MODE>
+__device__ __forceinline__ const __nv_bfloat16* a_tile(const TcArgs& a, const TcItem& it, int cb, int kt) {
+  if (MODE == ANA_S)
+    return a.tiles + ana_tile(a.lmax, a.ncb, a.nkn, 0, it.m, it.par, cb, kt) * TILE_HALVES;
+  if (MODE == SYN_S) return a.tiles + syn_tile(a.toff, a.lmax, it.m, it.par, cb, kt) * TILE_HALVES;
+  const bool first = kt < it.nk1;
+  const int kk = first ? kt : kt - it.nk1;
+  if (MODE == ANA_V) {
+    // S: dP . Vt_(1-p) - i mPs . Vp_p      T: -dP . Vp_(1-p) - i mPs . Vt_p
+    const int fold = first ? 1 - it.par : it.par;
+    const int field = first ? (it.out ? 2 : 1) : (it.out ? 1 : 2);
+    return a.tiles + ana_tile(a.lmax, a.ncb, a.nkn, field, it.m, fold, cb, kk) * TILE_HALVES;
+  }
+  // Vt_q = dP . S + i mPs . T      Vp_q = -dP . T + i mPs . S   (fields S = 0, T = 1)
+  const int par = first ? 1 - it.par : it.par;
+  const int field = first ? (it.out ? 1 : 0) : (it.out ? 0 : 1);
+  return a.tiles + (size_t)field * a.tfield + syn_tile(a.toff, a.lmax, it.m, par, cb, kk) * TILE_HALVES;
+}
+
+// Walks the K steps of this CTA's work units in order (units with no K
+// steps are skipped).
+struct TileCur {
+  int u, kt;
+  TcItem it;
+  __device__ void skip(const TcArgs& a) {
+    while (u < a.nunits && kt >= it.nk) {
+      u += gridDim.x;
+      kt = 0;
+      if (u < a.nunits) it = a.items[u / a.ncb];
+    }
+  }
+  __device__ void init(const TcArgs& a) {
+    u = blockIdx.x;
+    kt = 0;
+    if (u < a.nunits) it = a.items[u / a.ncb];
+    skip(a);
+  }
+  __device__ void next(const TcArgs& a) {
+    ++kt;
+    skip(a);
+  }
+  __device__ bool valid(const TcArgs& a) const { return u < a.nunits; }
+};
+
+// ---------------------------------------------------------------- tensor-core kernel
 template <int MODE>
 __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm(TcArgs a) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  uint64_t* fullA = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);  // producers arrived
-  uint64_t* fullB = fullA + STAGES;                                             // table copy landed
-  uint64_t* empty = fullB + STAGES;                                             // MMAs of the stage done
-  uint64_t* done = empty + STAGES;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
-  int* abort_flag = reinterpret_cast<int*>(tslot + 1);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + OFF_BAR);
+  uint64_t* full = bars;                 // [STAGES] data + table tiles landed
+  uint64_t* empty = full + STAGES;       // [STAGES] MMAs of the stage done
+  uint64_t* accFull = empty + STAGES;    // [2] accumulator set complete
+  uint64_t* accEmpty = accFull + 2;      // [2] accumulator set drained (count NEPI)
+  uint64_t* fin = accEmpty + 2;          // all MMAs of this CTA done
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(fin + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
 
   constexpr bool analysis = (MODE == ANA_S || MODE == ANA_V);
-  const TcItem it = a.items[blockIdx.y];
-  const int k0 = blockIdx.x * PLANES;  // first plane
+  constexpr bool vector = (MODE == ANA_V || MODE == SYN_V);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  // TMEM: the hi*lo + lo*hi accumulator at column 0 and one or two hi*hi
-  // accumulators (alternate K tiles) at columns xoff, 2*xoff.  Keeping them
-  // apart shortens the chains of fp32 roundings of each running sum.
-  const uint32_t xoff = tmem_cols(it.nr);
-  const int nmain = xoff <= 128 ? 2 : 1;
-  const uint32_t ncols = tmem_cols((nmain + 1) * (int)xoff);
 
-  // once any CTA of the plan has given up a wait, the rest do no work
+  // once any CTA of the plan has given up a wait, later launches do no work
   if (tid == 0) *abort_flag = *(volatile int*)a.flag;
   __syncthreads();
   if (*abort_flag) return;
   __syncthreads();
 
-  if (warp == 0) tc05::tmem_alloc(tslot, ncols);
-  if (tid == 32) {
+  if (warp == 1) tc05::tmem_alloc(tslot, TMEM_COLS);
+  if (tid == 0) {
     for (int s = 0; s < STAGES; ++s) {
-      tc05::mbar_init(&fullA[s], NPROD);
-      tc05::mbar_init(&fullB[s], 1);
+      tc05::mbar_init(&full[s], 1);
       tc05::mbar_init(&empty[s], 1);
     }
-    tc05::mbar_init(done, 1);
-    *abort_flag = 0;
+    for (int s = 0; s < 2; ++s) {
+      tc05::mbar_init(&accFull[s], 1);
+      tc05::mbar_init(&accEmpty[s], NEPI);
+    }
+    tc05::mbar_init(fin, 1);
     tc05::mbar_fence_init();
   }
   tc05::fence_before();
   __syncthreads();
   tc05::fence_after();
   const uint32_t tbase = *tslot;
+  auto fail = [&]() {
+    atomicExch(a.flag, 1);
+    *abort_flag = 1;
+  };
 
-  float dscale;
-  if (MODE == ANA_S) dscale = pow2_scale(a.dmax[0]);
-  else if (MODE == ANA_V) dscale = pow2_scale(fmaxf(a.dmax[1], a.dmax[2]));
-  else dscale = pow2_scale(a.dmax[3]);
-
-  const uint32_t bbytes = (uint32_t)it.nr * TK * 2 * 2;
-  const size_t base_lm = (size_t)a.mbase[it.m] - it.m;
-  int issued = 0;  // table copies issued (thread 0)
-
-  if (warp < 4) {
-    // ------------------------------------------------------------ producers
-    for (int kt = 0; kt < it.nk; ++kt) {
-      const int s = kt % STAGES, use = kt / STAGES;
-      if (use > 0 && !tc05::mbar_wait(&empty[s], (use - 1) & 1)) {
-        atomicExch(a.flag, 1);
-        *abort_flag = 1;
-        break;
-      }
-      if (*abort_flag) break;
-      unsigned char* Ahi = smem + s * STAGE_BYTES;
-      unsigned char* Alo = Ahi + A_BYTES;
-      unsigned char* Bs = Alo + A_BYTES;
-      if (tid == 0) {
-        mbar_arrive_tx(&fullB[s], bbytes);
-        bulk_copy(Bs, a.blocks + it.boff + (size_t)kt * 2 * it.nr * TK, bbytes, &fullB[s]);
-        issued = kt + 1;
-      }
-      // A tile: 64 planes x 4 chunks of 8 K values; the chunk index runs
-      // fastest so that four lanes read 256 contiguous bytes of one plane
-      float re[UNITS][8], im[UNITS][8];
-#pragma unroll
-      for (int u = 0; u < UNITS; ++u) {
-        const int unit = tid + NPROD * u, ch = unit & 3, pl = unit >> 2, k = k0 + pl;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) re[u][j] = im[u][j] = 0.f;
-        if (k >= a.nz) continue;
-        if (analysis) {
-          int f = F_PLAIN, fold = it.par, node0, field = 0;
-          if (MODE == ANA_S) {
-            node0 = kt * TK + ch * 8;
-          } else {
-            // S: [dP . Vt_(1-p) ; mPs . (-i Vp_p)]   T: [dP . (-Vp_(1-p)) ; mPs . (-i Vt_p)]
-            const bool first = kt < it.nk1;
-            node0 = (first ? kt : kt - it.nk1) * TK + ch * 8;
-            fold = first ? 1 - it.par : it.par;
-            field = first ? (it.out ? 2 : 1) : (it.out ? 1 : 2);
-            f = first ? (it.out ? F_NEG : F_PLAIN) : F_MULMI;
-          }
-          if (node0 < a.ldn8) {
-            const float4* r4 = reinterpret_cast<const float4*>(
-                a.G32 + (size_t)field * a.G32field + (((size_t)it.m * 2 + fold) * a.nz + k) * a.ldn8 + node0);
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              const float4 q = __ldg(r4 + j);
-              const float2 v0 = form_rt(make_float2(q.x, q.y), f), v1 = form_rt(make_float2(q.z, q.w), f);
-              re[u][2 * j] = v0.x * dscale;
-              im[u][2 * j] = v0.y * dscale;
-              re[u][2 * j + 1] = v1.x * dscale;
-              im[u][2 * j + 1] = v1.y * dscale;
-            }
-          }
-        } else {
-          // K = l of one parity.  Vector: Vt_q = [dP . S ; mPs . (i T)], Vp_q = [dP . (-T) ; mPs . (i S)]
-          int f = F_PLAIN, par = it.par, q0;
-          const double2* spec = a.in;
-          if (MODE == SYN_S) {
-            q0 = kt * TK + ch * 8;
-          } else {
-            const bool first = kt < it.nk1;
-            q0 = (first ? kt : kt - it.nk1) * TK + ch * 8;
-            par = first ? 1 - it.par : it.par;
-            if (first) {
-              spec = it.out ? a.in2 : a.in;
-              f = it.out ? F_NEG : F_PLAIN;
-            } else {
-              spec = it.out ? a.in : a.in2;
-              f = F_MULI;
-            }
-          }
-          const double2* col = spec + (size_t)k * a.nlm + base_lm;
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const int l = it.m + par + 2 * (q0 + j);
-            if (l <= a.lmax && (MODE == SYN_S || l > 0)) {
-              const double2 d = __ldg(col + l);
-              const float2 v =
-                  form_rt(make_float2((float)(d.x * (double)dscale), (float)(d.y * (double)dscale)), f);
-              re[u][j] = v.x;
-              im[u][j] = v.y;
-            }
-          }
+  if (warp == 0) {
+    // ------------------------------------------------------------ bulk copies
+    if (lane == 0) {
+      TileCur cur;
+      cur.init(a);
+      int g = 0;
+      for (; cur.valid(a); ++g, cur.next(a)) {
+        const int s = g % STAGES, n = g / STAGES;
+        if (n > 0 && (*abort_flag || !tc05::mbar_wait(&empty[s], (n - 1) & 1))) {
+          fail();
+          break;
         }
+        const __nv_bfloat16* At = a_tile<MODE>(a, cur.it, cur.u % a.ncb, cur.kt);
+        const uint32_t bbytes = (uint32_t)(NPIECE * cur.it.nr * TK * 2);
+        unsigned char* st = smem + s * STAGE_BYTES;
+        mbar_arrive_tx(&full[s], A_BYTES + bbytes);
+        bulk_copy(st, At, A_BYTES, &full[s]);
+        bulk_copy(st + A_BYTES, a.blocks + cur.it.boff + (size_t)cur.kt * NPIECE * cur.it.nr * TK, bbytes,
+                  &full[s]);
       }
-#pragma unroll
-      for (int u = 0; u < UNITS; ++u) {
-        const int unit = tid + NPROD * u, ch = unit & 3, pl = unit >> 2;
-        store_split8(Ahi, Alo, 2 * pl, ch, re[u]);
-        store_split8(Ahi, Alo, 2 * pl + 1, ch, im[u]);
-      }
-      fence_proxy_async();
-      tc05::mbar_arrive(&fullA[s]);
+      // after a failure, copies may still be in flight: let them land
+      if (*abort_flag)
+        for (int t = max(0, g - STAGES); t < g; ++t)
+          tc05::mbar_wait(&full[t % STAGES], (t / STAGES) & 1, 100000000ull);
     }
-  } else if (warp == 4 && lane == 0) {
+    __syncwarp();
+  } else if (warp == 1) {
     // ------------------------------------------------------------ MMA issue
-    const uint32_t idesc = tc05::idesc_f16(MCOLS, it.nr);
-    const uint32_t lboA = (MCOLS / 8) * 128, lboB = (uint32_t)(it.nr / 8) * 128;
-    for (int kt = 0; kt < it.nk; ++kt) {
-      const int s = kt % STAGES, use = kt / STAGES;
-      if (!tc05::mbar_wait(&fullA[s], use & 1) || !tc05::mbar_wait(&fullB[s], use & 1)) {
-        atomicExch(a.flag, 1);
-        *abort_flag = 1;
+    if (lane == 0) {
+      int g = 0, uc = 0;
+      bool ok = true;
+      for (int u = blockIdx.x; u < a.nunits && ok; u += gridDim.x, ++uc) {
+        const TcItem it = a.items[u / a.ncb];
+        const int buf = uc & 1;
+        if (uc >= 2 && !tc05::mbar_wait(&accEmpty[buf], ((uc >> 1) - 1) & 1)) {
+          ok = false;
+          break;
+        }
+        tc05::fence_after();
+        const uint32_t tacc = tbase + (uint32_t)buf * 256;
+        const uint32_t idesc = tc05::idesc_bf16(MCOLS, it.nr);
+        const uint32_t lboA = (MCOLS / 8) * 128, lboB = (uint32_t)(it.nr / 8) * 128;
+        const uint32_t bpiece = (uint32_t)it.nr * TK * 2;
+        for (int kt = 0; kt < it.nk; ++kt, ++g) {
+          const int s = g % STAGES;
+          if (*abort_flag || !tc05::mbar_wait(&full[s], (g / STAGES) & 1)) {
+            ok = false;
+            break;
+          }
+          tc05::fence_after();
+          const int part = (vector && kt >= it.nk1) ? 1 : 0;
+          const bool first = kt == (part ? it.nk1 : 0);
+          const uint32_t tmain = tacc + (uint32_t)part * 128;
+          const uint32_t tcross = tmain + (vector ? 64u : 128u);
+          unsigned char* At = smem + s * STAGE_BYTES;
+          unsigned char* Bt = At + A_BYTES;
+#pragma unroll
+          for (int j = 0; j < TK / 16; ++j) {
+            uint64_t ad[NPIECE], bd[NPIECE];
+#pragma unroll
+            for (int p = 0; p < NPIECE; ++p) {
+              ad[p] = tc05::smem_desc(At + p * PIECE_HALVES * 2 + j * 2 * lboA, lboA, 128);
+              bd[p] = tc05::smem_desc(Bt + p * bpiece + j * 2 * lboB, lboB, 128);
+            }
+            const uint32_t acc0 = (first && j == 0) ? 0u : 1u;
+            tc05::mma_f16(tmain, ad[0], bd[0], idesc, acc0);
+            tc05::mma_f16(tcross, ad[0], bd[1], idesc, acc0);
+            tc05::mma_f16(tcross, ad[1], bd[0], idesc, 1u);
+            tc05::mma_f16(tcross, ad[0], bd[2], idesc, 1u);
+            tc05::mma_f16(tcross, ad[1], bd[1], idesc, 1u);
+            tc05::mma_f16(tcross, ad[2], bd[0], idesc, 1u);
+          }
+          tc05::commit(&empty[s]);
+        }
+        if (!ok) break;
+        tc05::commit(&accFull[buf]);
+      }
+      if (!ok) fail();
+      tc05::commit(fin);
+      tc05::mbar_wait(fin, 0, 100000000ull);
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------ epilogue
+    // Per chunk of 16 rows: TMEM -> registers (this lane's component), the
+    // vector forms, then through a per-warp staging area so that the global
+    // stores of a half-warp cover 16 consecutive rows of one plane.
+    const int q = warp & 3;       // TMEM lane quarter of this warp
+    const int n = 32 * q + lane;  // data column: plane n/2 of the unit, component n&1
+    const bool odd = lane & 1;
+    double* stg = reinterpret_cast<double*>(smem + OFF_STG) + (warp - 2) * STG_WORDS;  // [32 lanes][17]
+    const int j_out = lane & 15, ph = lane >> 4;  // store phase: row, plane half
+    int uc = 0;
+    for (int u = blockIdx.x; u < a.nunits; u += gridDim.x, ++uc) {
+      const TcItem it = a.items[u / a.ncb];
+      const int buf = uc & 1;
+      bool ok = !*abort_flag && tc05::mbar_wait(&accFull[buf], (uc >> 1) & 1);
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok) {
+        fail();
         break;
       }
       tc05::fence_after();
-      unsigned char* Ahi = smem + s * STAGE_BYTES;
-      unsigned char* Alo = Ahi + A_BYTES;
-      unsigned char* Bhi = Alo + A_BYTES;
-      unsigned char* Blo = Bhi + (size_t)it.nr * TK * 2;
-#pragma unroll
-      for (int j = 0; j < TK / 16; ++j) {
-        const uint64_t ah = tc05::smem_desc(Ahi + j * 2 * lboA, lboA, 128);
-        const uint64_t al = tc05::smem_desc(Alo + j * 2 * lboA, lboA, 128);
-        const uint64_t bh = tc05::smem_desc(Bhi + j * 2 * lboB, lboB, 128);
-        const uint64_t bl = tc05::smem_desc(Blo + j * 2 * lboB, lboB, 128);
-        const int mi = 1 + (kt & (nmain - 1));
-        tc05::mma_f16(tbase + mi * xoff, ah, bh, idesc, (kt >= nmain || j) ? 1u : 0u);
-        tc05::mma_f16(tbase, ah, bl, idesc, (kt | j) ? 1u : 0u);
-        tc05::mma_f16(tbase, al, bh, idesc, 1u);
-      }
-      tc05::commit(&empty[s]);
-    }
-    if (it.nk > 0) tc05::commit(done);
-  }
-
-  // ------------------------------------------------------------ epilogue
-  if (warp < 4) {
-    bool ok = it.nk == 0 || (!*abort_flag && tc05::mbar_wait(done, 0));
-    ok = __all_sync(0xffffffffu, ok);
-    if (!ok) atomicExch(a.flag, 1);
-    tc05::fence_after();
-    if (ok) {
-      const double inv = 1.0 / ((double)it.tscale * (double)dscale);
-      const int n = 32 * warp + lane;  // data column: plane k0 + n/2, component n&1
-      const int k = k0 + (n >> 1);
+      const int kbase = (u % a.ncb) * PLANES + 16 * q;  // first plane of this warp
+      const size_t base_lm = (size_t)a.mbase[it.m] - it.m;
+      const uint32_t ta = tbase + (uint32_t)buf * 256 + ((uint32_t)(32 * q) << 16);
+      const bool have0 = vector ? it.nk1 > 0 : it.nk > 0;
+      const bool have1 = vector && it.nk > it.nk1;
       for (int c = 0; c < it.nr; c += 16) {
-        float v[16], x[16];
-        if (it.nk > 0) {
-          const uint32_t ta = tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)c;
-          tc05::tmem_ld16(ta + xoff, v);
-          tc05::tmem_ld16(ta, x);
-          if (nmain == 2 && it.nk > 1) {
-            float v2[16];
-            tc05::tmem_ld16(ta + 2 * xoff, v2);
-#pragma unroll
-            for (int j = 0; j < 16; ++j) x[j] += v2[j];
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < 16; ++j) v[j] = x[j] = 0.f;  // empty fold: written as zeros
+        uint32_t v0[16], x0[16], v1[16], x1[16];
+        if (have0) {
+          tc05::tmem_ld16_nw(ta + c, v0);
+          tc05::tmem_ld16_nw(ta + (vector ? 64 : 128) + c, x0);
         }
-        float w[16], y[16];
+        if (have1) {
+          tc05::tmem_ld16_nw(ta + 128 + c, v1);
+          tc05::tmem_ld16_nw(ta + 192 + c, x1);
+        }
+        tc05::tmem_wait_ld();
+        tc05::tmem_regs(v0);
+        tc05::tmem_regs(x0);
+        tc05::tmem_regs(v1);
+        tc05::tmem_regs(x1);
+        const double s0 = (vector && it.out) ? -1.0 : 1.0;  // part 0 form: +1 or -1
+        // part 1 times -i (analysis: re' = im, im' = -re) or +i (synthesis:
+        // re' = -im, im' = re): each lane takes its partner's value
+        const double sg = (analysis != odd) ? 1.0 : -1.0;
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
-          w[j] = __shfl_xor_sync(0xffffffffu, v[j], 1);
-          y[j] = __shfl_xor_sync(0xffffffffu, x[j], 1);
-        }
-        if ((lane & 1) || k >= a.nz) continue;
-        if (analysis) {
-          double2* out = (MODE == ANA_V && it.out) ? a.out2 : a.out;
-#pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int q = c + j;
-            if (q >= it.nvalid) break;
-            const int l = it.m + it.par + 2 * (it.r0 + q);
-            double f = inv;
-            if (MODE == ANA_V) f = l ? inv / ((double)l * (double)(l + 1)) : 0.0;
-            out[(size_t)k * a.nlm + base_lm + l] =
-                make_double2(((double)v[j] + (double)x[j]) * f, it.m == 0 ? 0.0 : ((double)w[j] + (double)y[j]) * f);
+          double r = 0.0;
+          if (analysis) {
+            if (have0) r = s0 * ((double)__uint_as_float(v0[j]) + (double)__uint_as_float(x0[j]));
+            if (vector) {
+              const double y = have1 ? (double)__uint_as_float(v1[j]) + (double)__uint_as_float(x1[j]) : 0.0;
+              r += sg * __shfl_xor_sync(0xffffffffu, y, 1);
+            }
+          } else {
+            float rf = have0 ? (float)s0 * (__uint_as_float(v0[j]) + __uint_as_float(x0[j])) : 0.f;
+            if (vector) {
+              const float y = have1 ? __uint_as_float(v1[j]) + __uint_as_float(x1[j]) : 0.f;
+              rf += (float)sg * __shfl_xor_sync(0xffffffffu, y, 1);
+            }
+            r = rf;
           }
-        } else {
-          const int field = (MODE == SYN_V) ? 1 + it.out : 0;
-          float2* G = a.G32w + (size_t)field * a.G32field + (((size_t)it.m * 2 + it.par) * a.nz + k) * a.ldn8;
-          const float finv = (float)inv;
-#pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int i = it.r0 + c + j;
-            if (i < a.ldn8) G[i] = make_float2((v[j] + x[j]) * finv, (w[j] + y[j]) * finv);
+          stg[lane * 17 + j] = r;
+        }
+        __syncwarp();
+        // 16 planes x 16 rows: lanes 0-15 rows of plane 2i, lanes 16-31 of plane 2i+1
+#pragma unroll 4
+        for (int i = 0; i < 8; ++i) {
+          const int pl = 2 * i + ph, k = kbase + pl;
+          const double re = stg[(2 * pl) * 17 + j_out], im = stg[(2 * pl + 1) * 17 + j_out];
+          const int rr = c + j_out;
+          if (k >= a.nz) continue;
+          if (analysis) {
+            if (rr >= it.nvalid) continue;
+            const int l = it.m + it.par + 2 * (it.r0 + rr);
+            double f = 1.0;
+            if (MODE == ANA_V) f = l ? 1.0 / ((double)l * (double)(l + 1)) : 0.0;
+            double2* out = (MODE == ANA_V && it.out) ? a.out2 : a.out;
+            out[(size_t)k * a.nlm + base_lm + l] = make_double2(re * f, it.m == 0 ? 0.0 : im * f);
+          } else {
+            const int field = (MODE == SYN_V) ? 1 + it.out : 0;
+            const int node = it.r0 + rr;
+            if (node < a.ldn8)
+              a.G32w[(size_t)field * a.G32field + (((size_t)it.m * 2 + it.par) * a.nz + k) * a.ldn8 + node] =
+                  make_float2((float)re, (float)im);
           }
         }
+        __syncwarp();
       }
+      tc05::fence_before();
+      tc05::mbar_arrive(&accEmpty[buf]);
     }
-    // after a bounded wait gave up, table copies may still be in flight
-    if (tid == 0 && *abort_flag)
-      for (int kt = max(0, issued - STAGES); kt < issued; ++kt)
-        tc05::mbar_wait(&fullB[kt % STAGES], (kt / STAGES) & 1, 100000000ull);
   }
   tc05::fence_before();
   __syncthreads();
-  if (warp == 0) tc05::tmem_free(tbase, ncols);
+  tc05::fence_after();
+  if (warp == 1) tc05::tmem_free(tbase, TMEM_COLS);
 }
 
 // ---------------------------------------------------------------- fp32 phi FFTs
@@ -365,20 +415,23 @@ __host__ __device__ inline int seq_stride(int nphi) {
 
 struct Phi32Args {
   const double* gin[SPH_MAX_FIELDS];
+  const double* gin_hi[SPH_MAX_FIELDS];  // planes k >= ksplit (continued planes)
+  int ksplit;
   double* gout[SPH_MAX_FIELDS];
-  float2* G32;
-  const float2* G32c;
+  __nv_bfloat16* tiles;  // analysis data tiles (forward output)
+  const float2* G32c;    // folded coefficients (inverse input)
   size_t G32field;
-  float* dmax;  // per-field maxima of |G32| (forward)
-  int nlat, ldn8, nz, lmax, NP;
+  int nlat, ldn8, nz, lmax, NP, ncb, nkn;
   const double* wfold;
   const float2* twp;
 };
 
-__device__ __forceinline__ void atomic_max_pos(float* addr, float v) {
-  atomicMax(reinterpret_cast<unsigned int*>(addr), __float_as_uint(v));
-}
-
+// Forward: ring pairs p0..p0+NP-1 of plane k, field f.  The samples are
+// placed at their digit-reversed positions and transformed by the
+// decimation-in-time passes, so the spectrum comes out in natural order; the
+// thread of degree m then reads Z(m), Z(-m) of its NP ring pairs from
+// consecutive addresses, folds both parities and writes them, split, as row
+// chunks of the analysis tiles.
 template <int N, int NP>
 __global__ void __launch_bounds__(PTHREADS, 2) phi_fwd32(Phi32Args a) {
   extern __shared__ float2 sf[];
@@ -386,7 +439,8 @@ __global__ void __launch_bounds__(PTHREADS, 2) phi_fwd32(Phi32Args a) {
   const int nlat = a.nlat;
   const int p0 = blockIdx.x * NP, k = blockIdx.y, f = blockIdx.z;
   const int tid = threadIdx.x;
-  const double* plane = a.gin[f] + (size_t)k * N * nlat;
+  const double* plane =
+      k < a.ksplit ? a.gin[f] + (size_t)k * N * nlat : a.gin_hi[f] + (size_t)(k - a.ksplit) * N * nlat;
   const ct::Geo<N, 1, true> g{NP, seq_stride(N), 1};
   float* smf = reinterpret_cast<float*>(sf);
   {
@@ -408,32 +462,38 @@ __global__ void __launch_bounds__(PTHREADS, 2) phi_fwd32(Phi32Args a) {
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         int j = j0 + (u0 + u) * JSTEP;
-        if (u0 + u < NJ && j < N) smf[2 * g.addr(b, j) + half] = (float)v[u];
+        if (u0 + u < NJ && j < N) smf[2 * g.addr(b, ct::rev_pos<N>(j)) + half] = (float)v[u];
       }
     }
   }
   __syncthreads();
-  ct::dif<float2, N, N>(sf, g, a.twp, -1);
+  ct::dit<float2, N, N>(sf, g, a.twp, -1);
 
-  float2* G = a.G32 + (size_t)f * a.G32field + (size_t)k * a.ldn8 + p0;
-  const size_t mstride = (size_t)2 * a.nz * a.ldn8, pstride = (size_t)a.nz * a.ldn8;
-  const int b = tid % NP;
-  const float W = (float)__ldg(a.wfold + p0 + b);
-  float mx = 0.f;
-  for (int m = tid / NP; m <= a.lmax; m += PTHREADS / NP) {
-    const float2 Z = sf[g.addr(b, ct::rev_pos<N>(m))];
-    const float2 Zc = sf[g.addr(b, ct::rev_pos<N>(m == 0 ? 0 : N - m))];
-    // F(ring) = (Z + conj Z(-m))/2, F(mirror) = -i (Z - conj Z(-m))/2
-    const float2 Fi = make_float2(0.5f * (Z.x + Zc.x), 0.5f * (Z.y - Zc.y));
-    const float2 Fm = make_float2(0.5f * (Z.y + Zc.y), -0.5f * (Z.x - Zc.x));
-    const float2 ge = make_float2((Fi.x + Fm.x) * W, (Fi.y + Fm.y) * W);
-    const float2 go = make_float2((Fi.x - Fm.x) * W, (Fi.y - Fm.y) * W);
-    G[m * mstride + b] = ge;
-    G[m * mstride + pstride + b] = go;
-    mx = fmaxf(mx, fmaxf(fmaxf(fabsf(ge.x), fabsf(ge.y)), fmaxf(fabsf(go.x), fabsf(go.y))));
+  float W[NP];
+#pragma unroll
+  for (int b = 0; b < NP; ++b) W[b] = (float)__ldg(a.wfold + p0 + b);
+  const int cb = k / PLANES, row = 2 * (k % PLANES), kt = p0 / TK, kk0 = p0 % TK;
+  for (int m = tid; m <= a.lmax; m += PTHREADS) {
+    float er[NP], ei[NP], orr[NP], oi[NP];
+#pragma unroll
+    for (int b = 0; b < NP; ++b) {
+      const float2 Z = sf[g.addr(b, m)];
+      const float2 Zc = sf[g.addr(b, m == 0 ? 0 : N - m)];
+      // F(ring) = (Z + conj Z(-m))/2, F(mirror) = -i (Z - conj Z(-m))/2
+      const float fir = 0.5f * (Z.x + Zc.x), fii = 0.5f * (Z.y - Zc.y);
+      const float fmr = 0.5f * (Z.y + Zc.y), fmi = -0.5f * (Z.x - Zc.x);
+      er[b] = (fir + fmr) * W[b];
+      ei[b] = (fii + fmi) * W[b];
+      orr[b] = (fir - fmr) * W[b];
+      oi[b] = (fii - fmi) * W[b];
+    }
+    __nv_bfloat16* t0 = a.tiles + ana_tile(a.lmax, a.ncb, a.nkn, f, m, 0, cb, kt) * TILE_HALVES;
+    __nv_bfloat16* t1 = a.tiles + ana_tile(a.lmax, a.ncb, a.nkn, f, m, 1, cb, kt) * TILE_HALVES;
+    store_tile_row<NP>(t0, row, kk0, er);
+    store_tile_row<NP>(t0, row + 1, kk0, ei);
+    store_tile_row<NP>(t1, row, kk0, orr);
+    store_tile_row<NP>(t1, row + 1, kk0, oi);
   }
-  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  if ((tid & 31) == 0 && mx > 0.f) atomic_max_pos(a.dmax + f, mx);
 }
 
 template <int N, int NP>
@@ -473,26 +533,90 @@ __global__ void __launch_bounds__(PTHREADS, 2) phi_inv32(Phi32Args a) {
   for (int j = j0; j < N; j += JSTEP) plane[(size_t)j * nlat + ring] = (double)smf[2 * g.addr(b, j) + half];
 }
 
-// maximum of |re|, |im| over one or two spectral fields (synthesis data scale)
-__global__ void spec_max_kernel(const double2* a, const double2* b, size_t n, float* out) {
-  float mx = 0.f;
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-    double2 v = a[q];
-    mx = fmaxf(mx, (float)fmax(fabs(v.x), fabs(v.y)));
-    if (b) {
-      v = b[q];
-      mx = fmaxf(mx, (float)fmax(fabs(v.x), fabs(v.y)));
+// FC-Gram continuation of physical planes (FP64), one grid point per
+// thread: out(ii) = sum_jj dir(ii,jj) f(N-d+jj) + dir(C-1-ii,jj) f(d-1-jj),
+// the same operator the z transform applies to spectral planes
+// (fcgram_mod.f90 / pseudospec continuation step), here before the
+// analysis so that its round-off is not amplified.
+__global__ void cont_phys_kernel(const double* __restrict__ f0, const double* __restrict__ f1,
+                                 const double* __restrict__ f2, double* out, const double* __restrict__ dir, int C,
+                                 int d, int N, size_t npts) {
+  const int f = blockIdx.y;
+  const double* in = f == 0 ? f0 : (f == 1 ? f1 : f2);
+  double* o = out + (size_t)f * C * npts;
+  for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < npts; x += (size_t)gridDim.x * blockDim.x) {
+    double hi[32], lo[32];
+#pragma unroll 8
+    for (int jj = 0; jj < d; ++jj) {
+      hi[jj] = __ldg(in + (size_t)(N - d + jj) * npts + x);
+      lo[jj] = __ldg(in + (size_t)(d - 1 - jj) * npts + x);
+    }
+    for (int ii = 0; ii < C; ++ii) {
+      double acc = 0.0;
+      for (int jj = 0; jj < d; ++jj)
+        acc = (acc + __ldg(dir + ii + C * jj) * hi[jj]) + __ldg(dir + (C - 1 - ii) + C * jj) * lo[jj];
+      o[(size_t)ii * npts + x] = acc;
     }
   }
-  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  if ((threadIdx.x & 31) == 0 && mx > 0.f) atomic_max_pos(out, mx);
+}
+
+// Spectra (lm order) -> synthesis data tiles.  Thread c of block (m, k, field)
+// takes l = m + 16c .. m + 16c + 15, i.e. 8 values of each parity (q = 8c ..
+// 8c + 7), and writes one row chunk per parity and component; values past
+// lmax are written as zeros.
+__global__ void spec_to_tiles(const double2* __restrict__ in, const double2* __restrict__ in2,
+                              __nv_bfloat16* tiles, size_t tfield, const long long* __restrict__ toff,
+                              const int* __restrict__ mbase, int lmax, int nlm) {
+  const int m = blockIdx.x, k = blockIdx.y, f = blockIdx.z;
+  const double2* src = (f ? in2 : in) + (size_t)k * nlm + mbase[m] - m;
+  __nv_bfloat16* T = tiles + (size_t)f * tfield;
+  const int cb = k / PLANES, row = 2 * (k % PLANES);
+  const int nc = ntiles_of(lmax, m, 0) * (TK / 8);  // chunks of 8 q (parity 0 has the most rows)
+  for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+    double2 v[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int l = m + 16 * c + j;
+      v[j] = l <= lmax ? __ldg(src + l) : make_double2(0.0, 0.0);
+    }
+    const int kt = c / (TK / 8), kk0 = (c % (TK / 8)) * 8;
+#pragma unroll
+    for (int par = 0; par < 2; ++par) {
+      if (kt >= ntiles_of(lmax, m, par)) continue;
+      float re[8], im[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        re[j] = (float)v[2 * j + par].x;
+        im[j] = (float)v[2 * j + par].y;
+      }
+      __nv_bfloat16* t = T + syn_tile(toff, lmax, m, par, cb, kt) * TILE_HALVES;
+      store_tile_row<8>(t, row, kk0, re);
+      store_tile_row<8>(t, row + 1, kk0, im);
+    }
+  }
 }
 
 // ---------------------------------------------------------------- host tables
-// Builds one work set: items (heaviest first) and their fp16 hi/lo table
-// blocks.  value(it, row, kt, kk) is the FP64 table entry of MMA row `row`,
-// K element kt*32+kk.  An item with out = 1 right after its out = 0 twin
-// shares the twin's blocks and scale.
+__host__ inline uint16_t bf16_bits(double x) {
+  // x already rounded to 8 significant bits: exact in fp32 and bf16
+  const float f = (float)x;
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return (uint16_t)(u >> 16);
+}
+// round to 8 significant bits, nearest even; tiny values flush to zero
+__host__ inline double round8(double x) {
+  if (!(std::fabs(x) >= 0x1p-110)) return 0.0;
+  int e;
+  const double m = std::frexp(x, &e);  // |m| in [0.5, 1)
+  return std::ldexp(std::nearbyint(std::ldexp(m, 8)), e - 8);
+}
+
+// Builds one work set: items (heaviest first) and their bf16 table blocks
+// (per K step: [hi | mid | lo] x nr rows x 32, core-matrix K-major).
+// value(it, row, kt, kk) is the FP64 table entry of MMA row `row`, K element
+// kt*32+kk.  An item with out = 1 right after its out = 0 twin shares the
+// twin's blocks.
 template <typename ItemsFn, typename ValFn>
 int build_set(TcSet& set, ItemsFn make_items, ValFn value) {
   std::vector<TcItem> raw;
@@ -510,64 +634,48 @@ int build_set(TcSet& set, ItemsFn make_items, ValFn value) {
   for (int h : heads) {
     TcItem it = raw[h];
     it.boff = (long long)total;
-    total += (size_t)it.nk * 2 * it.nr * TK;
+    it.tscale = 1.f;
+    total += (size_t)it.nk * NPIECE * it.nr * TK;
     own.push_back((int)items.size());
     items.push_back(it);
     if (h + 1 < (int)raw.size() && is_twin(h + 1)) {
       TcItem tw = raw[h + 1];
       tw.boff = it.boff;
+      tw.tscale = 1.f;
       items.push_back(tw);
     }
   }
-  std::vector<__half> hb(total);
+  std::vector<uint16_t> hb(total, 0);
   const int nth = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
   std::vector<std::thread> th;
   for (int t = 0; t < nth; ++t)
     th.emplace_back([&, t]() {
-      std::vector<double> tile;
       for (size_t x = t; x < own.size(); x += nth) {
-        TcItem& it = items[own[x]];
-        double mx = 0.0;
-        tile.assign((size_t)it.nk * it.nr * TK, 0.0);
-        for (int kt = 0; kt < it.nk; ++kt)
-          for (int r = 0; r < it.nr; ++r)
-            for (int kk = 0; kk < TK; ++kk) {
-              const double v = r < it.nvalid ? value(it, r, kt, kk) : 0.0;
-              tile[((size_t)kt * it.nr + r) * TK + kk] = v;
-              mx = std::max(mx, std::fabs(v));
-            }
-        int e = 0;
-        if (mx > 0) std::frexp(mx, &e);
-        const double s = mx > 0 ? std::ldexp(1.0, 14 - e) : 1.0;
-        it.tscale = (float)s;
+        const TcItem& it = items[own[x]];
         for (int kt = 0; kt < it.nk; ++kt) {
-          __half* hi = hb.data() + it.boff + (size_t)kt * 2 * it.nr * TK;
-          __half* lo = hi + (size_t)it.nr * TK;
-          for (int r = 0; r < it.nr; ++r)
+          uint16_t* blk = hb.data() + it.boff + (size_t)kt * NPIECE * it.nr * TK;
+          for (int r = 0; r < it.nvalid; ++r)
             for (int kk = 0; kk < TK; ++kk) {
-              const double v = tile[((size_t)kt * it.nr + r) * TK + kk] * s;
-              const __half h = __double2half(v);
-              const __half l = __double2half(v - (double)__half2float(h));
+              const double v = value(it, r, kt, kk);
+              const double h = round8(v), md = round8(v - h), lo = round8(v - h - md);
               const uint32_t off = tc05::kmaj_off(r, kk, it.nr) / 2;
-              hi[off] = h;
-              lo[off] = l;
+              blk[off] = bf16_bits(h);
+              blk[(size_t)it.nr * TK + off] = bf16_bits(md);
+              blk[(size_t)2 * it.nr * TK + off] = bf16_bits(lo);
             }
         }
       }
     });
   for (auto& x : th) x.join();
-  for (size_t x = 1; x < items.size(); ++x)
-    if (items[x].out == 1 && items[x].boff == items[x - 1].boff) items[x].tscale = items[x - 1].tscale;
   set.nitems = (int)items.size();
   set.nhalves = total;
   if (cudaMalloc((void**)&set.items, std::max<size_t>(1, items.size()) * sizeof(TcItem)) != cudaSuccess)
     return SPH_ENOMEM;
-  if (cudaMalloc((void**)&set.blocks, std::max<size_t>(1, total) * sizeof(__half)) != cudaSuccess)
-    return SPH_ENOMEM;
+  if (cudaMalloc((void**)&set.blocks, std::max<size_t>(1, total) * 2) != cudaSuccess) return SPH_ENOMEM;
   if (!items.empty() &&
       cudaMemcpy(set.items, items.data(), items.size() * sizeof(TcItem), cudaMemcpyHostToDevice) != cudaSuccess)
     return SPH_ECUDA;
-  if (total && cudaMemcpy(set.blocks, hb.data(), total * sizeof(__half), cudaMemcpyHostToDevice) != cudaSuccess)
+  if (total && cudaMemcpy(set.blocks, hb.data(), total * 2, cudaMemcpyHostToDevice) != cudaSuccess)
     return SPH_ECUDA;
   return SPH_OK;
 }
@@ -594,25 +702,25 @@ int mixed_setup(sph_plan* p, const std::vector<double>& hP, const std::vector<do
   p->ldn8 = (n2 + 7) & ~7;
   p->G32field = (size_t)(lmax + 1) * 2 * p->nz * p->ldn8;
   if (p->G32field * sizeof(float2) > p->Gfield * sizeof(double2)) return SPH_EINVAL;
-  const int nkn = (p->ldn8 + TK - 1) / TK;  // K tiles over the nodes
-  // synthesis node blocks: as few as keep N <= 256, of equal size
-  const int nblk = (n2 + NRMAX - 1) / NRMAX;
-  const int iblk = round16((n2 + nblk - 1) / nblk);
+  const int nkn = (n2 + TK - 1) / TK;  // K tiles over the nodes
+  const int ncb = (p->nz + PLANES - 1) / PLANES;
+  p->nkn = nkn;
   auto lm = [&](int l, int m) { return (size_t)p->mbase[m] + (l - m); };
-  auto rows = [&](int m, int par) { return m + par > lmax ? 0 : (lmax - m - par) / 2 + 1; };
+  auto rows = [&](int m, int par) { return rows_of(lmax, m, par); };
 
-  // analysis: rows = l of one parity, K = nodes (vector: [dP nodes | mPs nodes])
+  // analysis: rows = l of one parity, K = nodes (vector: [dP . fold 1-p | mPs . fold p])
   auto ana_items = [&](bool vec) {
     return [&, vec](std::vector<TcItem>& v) {
+      const int NR = vec ? NR_V : NR_S;
       for (int m = 0; m <= lmax; ++m)
         for (int par = 0; par < 2; ++par) {
           const int L = rows(m, par);
-          for (int r0 = 0; r0 < L; r0 += NRMAX) {
+          for (int r0 = 0; r0 < L; r0 += NR) {
             TcItem it = {};
             it.m = m;
             it.par = par;
             it.r0 = r0;
-            it.nvalid = std::min(NRMAX, L - r0);
+            it.nvalid = std::min(NR, L - r0);
             it.nr = round16(it.nvalid);
             it.nk = vec ? 2 * nkn : nkn;
             it.nk1 = nkn;
@@ -635,24 +743,24 @@ int mixed_setup(sph_plan* p, const std::vector<double>& hP, const std::vector<do
       return T[lm(l, it.m) * ldn + i];
     };
   };
-  // synthesis: rows = nodes, K = l of one parity (vector: [l of 1-q via dP | l of q via mPs])
+  // synthesis: rows = nodes, K = l of one parity (vector: [dP . l of 1-q | mPs . l of q])
   auto syn_items = [&](bool vec) {
     return [&, vec](std::vector<TcItem>& v) {
+      const int NR = vec ? NR_V : NR_S;
       for (int m = 0; m <= lmax; ++m)
         for (int q = 0; q < 2; ++q) {
-          const int Lq = rows(m, q), L1 = rows(m, 1 - q);
-          for (int i0 = 0; i0 < n2; i0 += iblk) {
+          for (int i0 = 0; i0 < n2; i0 += NR) {
             TcItem it = {};
             it.m = m;
             it.par = q;
             it.r0 = i0;
-            it.nvalid = std::min(iblk, n2 - i0);
+            it.nvalid = std::min(NR, n2 - i0);
             it.nr = round16(it.nvalid);
             if (vec) {
-              it.nk1 = (L1 + TK - 1) / TK;
-              it.nk = it.nk1 + (Lq + TK - 1) / TK;
+              it.nk1 = ntiles_of(lmax, m, 1 - q);
+              it.nk = it.nk1 + ntiles_of(lmax, m, q);
             } else {
-              it.nk = (Lq + TK - 1) / TK;  // 0: the fold is written as zeros
+              it.nk = ntiles_of(lmax, m, q);  // 0: the fold is written as zeros
               it.nk1 = it.nk;
             }
             v.push_back(it);
@@ -684,10 +792,35 @@ int mixed_setup(sph_plan* p, const std::vector<double>& hP, const std::vector<do
   if (rc == SPH_OK) rc = build_set(p->tcAV, ana_items(true), ana_val(true));
   if (rc == SPH_OK) rc = build_set(p->tcSS, syn_items(false), syn_val(false));
   if (rc == SPH_OK) rc = build_set(p->tcSV, syn_items(true), syn_val(true));
-  if (rc == SPH_OK && cudaMalloc((void**)&p->dmax, 4 * sizeof(float)) != cudaSuccess) rc = SPH_ENOMEM;
+  // data tiles: analysis [3 fields][m][fold][cb][nkn]; synthesis 2 fields of [m][par][cb][ntiles]
+  std::vector<long long> off(2 * (lmax + 1));
+  long long nsyn = 0;
+  for (int m = 0; m <= lmax; ++m)
+    for (int par = 0; par < 2; ++par) {
+      off[2 * m + par] = nsyn;
+      nsyn += (long long)ncb * ntiles_of(lmax, m, par);
+    }
+  p->Tsynfield = (size_t)nsyn * TILE_HALVES;
+  const size_t nana = ana_tile(lmax, ncb, nkn, SPH_MAX_FIELDS, 0, 0, 0, 0) * TILE_HALVES;
+  const size_t bytes_ana = nana * 2, bytes_syn = 2 * p->Tsynfield * 2;
+  if (rc == SPH_OK && cudaMalloc((void**)&p->Tana, bytes_ana) != cudaSuccess) rc = SPH_ENOMEM;
+  if (rc == SPH_OK && cudaMemset(p->Tana, 0, bytes_ana) != cudaSuccess) rc = SPH_ECUDA;
+  if (rc == SPH_OK && cudaMalloc((void**)&p->Tsyn, std::max<size_t>(16, bytes_syn)) != cudaSuccess) rc = SPH_ENOMEM;
+  if (rc == SPH_OK && cudaMemset(p->Tsyn, 0, std::max<size_t>(16, bytes_syn)) != cudaSuccess) rc = SPH_ECUDA;
+  if (rc == SPH_OK && cudaMalloc((void**)&p->d_toff, off.size() * sizeof(long long)) != cudaSuccess) rc = SPH_ENOMEM;
+  if (rc == SPH_OK &&
+      cudaMemcpy(p->d_toff, off.data(), off.size() * sizeof(long long), cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = SPH_ECUDA;
+  if (rc == SPH_OK && p->C > 0 && p->d <= 32 &&
+      cudaMalloc((void**)&p->contg, (size_t)SPH_MAX_FIELDS * p->C * p->nphi * p->nlat * sizeof(double)) !=
+          cudaSuccess)
+    rc = SPH_ENOMEM;
   if (rc == SPH_OK && cudaMalloc((void**)&p->dflag, sizeof(int)) != cudaSuccess) rc = SPH_ENOMEM;
   if (rc == SPH_OK && cudaMemset(p->dflag, 0, sizeof(int)) != cudaSuccess) rc = SPH_ECUDA;
-  if (rc == SPH_OK && cudaMemset(p->dmax, 0, 4 * sizeof(float)) != cudaSuccess) rc = SPH_ECUDA;
+  int dev = 0;
+  if (rc == SPH_OK && (cudaGetDevice(&dev) != cudaSuccess ||
+                       cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess))
+    rc = SPH_ECUDA;
   return rc;
 }
 
@@ -698,10 +831,14 @@ void mixed_free(sph_plan* p) {
     s->items = nullptr;
     s->blocks = nullptr;
   }
-  if (p->dmax) cudaFree(p->dmax);
-  if (p->dflag) cudaFree(p->dflag);
-  p->dmax = nullptr;
+  void* ptrs[] = {p->dflag, p->Tana, p->Tsyn, p->d_toff, p->contg};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  p->contg = nullptr;
   p->dflag = nullptr;
+  p->Tana = nullptr;
+  p->Tsyn = nullptr;
+  p->d_toff = nullptr;
 }
 
 int mixed_status(const sph_plan* p) {
@@ -714,29 +851,33 @@ namespace {
 
 TcArgs tc_args(const sph_plan* p) {
   TcArgs a = {};
-  a.G32 = reinterpret_cast<const float2*>(p->G);
   a.G32w = reinterpret_cast<float2*>(p->G);
   a.G32field = p->G32field;
+  a.toff = p->d_toff;
+  a.tfield = p->Tsynfield;
   a.mbase = p->d_mbase;
-  a.dmax = p->dmax;
   a.flag = p->dflag;
   a.lmax = p->lmax;
   a.nz = p->nz;
   a.nlm = p->nlm;
   a.ldn8 = p->ldn8;
+  a.nkn = p->nkn;
+  a.ncb = (p->nz + PLANES - 1) / PLANES;
   return a;
 }
 
 template <int MODE>
-int run_tc(const TcSet& set, TcArgs a, int nz, cudaStream_t st) {
+int run_tc(const sph_plan* p, const TcSet& set, TcArgs a, cudaStream_t st) {
   static const bool attr_ok =
       cudaFuncSetAttribute(tc_gemm<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM) == cudaSuccess;
   if (!attr_ok) return SPH_ECUDA;
-  if (set.nitems == 0) return SPH_OK;
-  if (set.nitems > 65535) return SPH_EINVAL;
+  const long long nunits = (long long)set.nitems * a.ncb;
+  if (nunits == 0) return SPH_OK;
+  if (nunits > (1ll << 30)) return SPH_EINVAL;
   a.items = set.items;
-  a.blocks = set.blocks;
-  dim3 grid((nz + PLANES - 1) / PLANES, set.nitems);
+  a.blocks = reinterpret_cast<const __nv_bfloat16*>(set.blocks);
+  a.nunits = (int)nunits;
+  const int grid = (int)std::min<long long>(nunits, std::max(1, p->nsm));
   tc_gemm<MODE><<<grid, TC_THREADS, TC_SMEM, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;
@@ -788,26 +929,45 @@ int phi32_dispatch(const sph_plan* p, const Phi32Args& a, dim3 grid, size_t smem
 
 Phi32Args phi32_args(const sph_plan* p) {
   Phi32Args a = {};
-  a.G32 = reinterpret_cast<float2*>(p->G);
+  a.tiles = reinterpret_cast<__nv_bfloat16*>(p->Tana);
   a.G32c = reinterpret_cast<const float2*>(p->G);
   a.G32field = p->G32field;
-  a.dmax = p->dmax;
   a.nlat = p->nlat;
   a.ldn8 = p->ldn8;
   a.nz = p->nz;
   a.lmax = p->lmax;
   a.NP = phi_pairs(p);
+  a.ncb = (p->nz + PLANES - 1) / PLANES;
+  a.nkn = p->nkn;
   a.wfold = p->wfold;
   a.twp = p->fphi.twpf;
+  a.ksplit = p->nz;
   return a;
 }
 
 }  // namespace
 
-int launch_phi_fwd32(const sph_plan* p, const double* const* grids, int nfields, cudaStream_t st) {
+int launch_cont_phys(const sph_plan* p, const double* const* grids, int nfields, cudaStream_t st) {
+  if (!p->contg || p->C <= 0 || p->d > 32 || nfields < 1 || nfields > SPH_MAX_FIELDS) return SPH_EINVAL;
+  const size_t npts = (size_t)p->nphi * p->nlat;
+  const double* f[SPH_MAX_FIELDS] = {grids[0], nfields > 1 ? grids[1] : grids[0], nfields > 2 ? grids[2] : grids[0]};
+  TimedLaunch tl(p, T_OPS, st);
+  const int blocks = (int)std::min<size_t>((npts + 255) / 256, 148 * 8);
+  cont_phys_kernel<<<dim3(blocks, nfields), 256, 0, st>>>(f[0], f[1], f[2], p->contg, p->d_dir, p->C, p->d, p->N,
+                                                        npts);
+  SPH_LAUNCH_OK();
+  return SPH_OK;
+}
+
+int launch_phi_fwd32(const sph_plan* p, const double* const* grids, int nfields, cudaStream_t st,
+                     const double* const* grids_hi) {
   Phi32Args a = phi32_args(p);
   for (int f = 0; f < nfields; ++f) a.gin[f] = grids[f];
-  SPH_CUDA_OK(cudaMemsetAsync(p->dmax, 0, 3 * sizeof(float), st));  // field f -> maximum slot f
+  a.ksplit = p->nz;
+  if (grids_hi) {
+    a.ksplit = p->N;
+    for (int f = 0; f < nfields; ++f) a.gin_hi[f] = grids_hi[f];
+  }
   dim3 grid(p->nlat2 / a.NP, p->nz, nfields);
   const size_t smem = (size_t)a.NP * seq_stride(p->nphi) * sizeof(float2);
   TimedLaunch tl(p, T_PHI_FWD, st);
@@ -825,24 +985,22 @@ int launch_phi_inv32(const sph_plan* p, double* const* grids, int nfields, cudaS
 
 int launch_tc_analysis(const sph_plan* p, int vector, double2* out, double2* out2, cudaStream_t st) {
   TcArgs a = tc_args(p);
+  a.tiles = reinterpret_cast<const __nv_bfloat16*>(p->Tana);
   a.out = out;
   a.out2 = out2;
   TimedLaunch tl(p, vector ? T_VEC_ANA : T_LEG_ANA, st);
-  return vector ? run_tc<ANA_V>(p->tcAV, a, p->nz, st) : run_tc<ANA_S>(p->tcAS, a, p->nz, st);
+  return vector ? run_tc<ANA_V>(p, p->tcAV, a, st) : run_tc<ANA_S>(p, p->tcAS, a, st);
 }
 
 int launch_tc_synthesis(const sph_plan* p, int vector, const double2* in, const double2* in2, cudaStream_t st) {
   TcArgs a = tc_args(p);
-  a.in = in;
-  a.in2 = in2;
+  a.tiles = reinterpret_cast<const __nv_bfloat16*>(p->Tsyn);
   {
     TimedLaunch tl(p, T_OPS, st);
-    SPH_CUDA_OK(cudaMemsetAsync(p->dmax + 3, 0, sizeof(float), st));
-    const size_t n = spec_elems(p);
-    const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
-    spec_max_kernel<<<blocks, 256, 0, st>>>(in, vector ? in2 : nullptr, n, p->dmax + 3);
+    spec_to_tiles<<<dim3(p->lmax + 1, p->nz, vector ? 2 : 1), 32, 0, st>>>(
+        in, in2, reinterpret_cast<__nv_bfloat16*>(p->Tsyn), p->Tsynfield, p->d_toff, p->d_mbase, p->lmax, p->nlm);
     SPH_LAUNCH_OK();
   }
   TimedLaunch tl(p, vector ? T_VEC_SYN : T_LEG_SYN, st);
-  return vector ? run_tc<SYN_V>(p->tcSV, a, p->nz, st) : run_tc<SYN_S>(p->tcSS, a, p->nz, st);
+  return vector ? run_tc<SYN_V>(p, p->tcSV, a, st) : run_tc<SYN_S>(p, p->tcSS, a, st);
 }

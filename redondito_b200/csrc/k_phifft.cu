@@ -36,6 +36,7 @@ struct PhiArgs {
   const double2* Gc;
   size_t Gfield;
   int nlat, nlat2, ldn, nphi, nz, lmax, NP;
+  const int* kzl;  // planes to transform (nullptr: all nz)
   const double* wfold;
   FftDesc fd;
 };
@@ -50,7 +51,7 @@ __global__ void __launch_bounds__(PTHREADS, 2) phi_fwd_ct(PhiArgs a) {
   constexpr int Q = 2 * NP;             // rings per CTA
   constexpr int JSTEP = PTHREADS / Q;   // phi stride of one thread
   const int nlat = a.nlat;
-  const int p0 = blockIdx.x * NP, k = blockIdx.y, f = blockIdx.z;
+  const int p0 = blockIdx.x * NP, k = a.kzl ? __ldg(a.kzl + blockIdx.y) : blockIdx.y, f = blockIdx.z;
   const int tid = threadIdx.x;
   const double* plane = a.gin[f] + (size_t)k * N * nlat;
   const ct::Geo<N, 1, true> g{NP, seq_stride(N), 1};
@@ -104,7 +105,7 @@ __global__ void __launch_bounds__(PTHREADS, 2) phi_inv_ct(PhiArgs a) {
   constexpr int Q = 2 * NP;
   constexpr int JSTEP = PTHREADS / Q;
   const int nlat = a.nlat;
-  const int p0 = blockIdx.x * NP, k = blockIdx.y, f = blockIdx.z;
+  const int p0 = blockIdx.x * NP, k = a.kzl ? __ldg(a.kzl + blockIdx.y) : blockIdx.y, f = blockIdx.z;
   const int tid = threadIdx.x;
   const ct::Geo<N, 1, true> g{NP, seq_stride(N), 1};
   const int M = a.lmax + 1;
@@ -165,7 +166,7 @@ __global__ void __launch_bounds__(PTHREADS, 2) phi_fwd_kernel(PhiArgs a) {
   extern __shared__ double2 sm[];
   const int NP = a.NP, nphi = a.nphi, nlat = a.nlat, nlat2 = a.nlat2;
   const int p0 = blockIdx.x * NP;
-  const int k = blockIdx.y;
+  const int k = a.kzl ? __ldg(a.kzl + blockIdx.y) : blockIdx.y;
   const int f = blockIdx.z;
   const int tid = threadIdx.x;
   const double* plane = a.gin[f] + (size_t)k * nphi * nlat;
@@ -203,7 +204,7 @@ __global__ void __launch_bounds__(PTHREADS, 2) phi_inv_kernel(PhiArgs a) {
   extern __shared__ double2 sm[];
   const int NP = a.NP, nphi = a.nphi, nlat = a.nlat, nlat2 = a.nlat2;
   const int p0 = blockIdx.x * NP;
-  const int k = blockIdx.y;
+  const int k = a.kzl ? __ldg(a.kzl + blockIdx.y) : blockIdx.y;
   const int f = blockIdx.z;
   const int tid = threadIdx.x;
   const int np = min(NP, nlat2 - p0);
@@ -306,6 +307,7 @@ PhiArgs make_args(const sph_plan* p) {
   a.NP = pairs_per_cta(p);
   a.wfold = p->wfold;
   a.fd = p->fphi;
+  a.kzl = p->sel_kz;
   return a;
 }
 
@@ -316,7 +318,7 @@ int launch_phi_fwd(const sph_plan* p, const double* const* grids, int nfields, c
   if (p->nphi > PMAXC) return SPH_EINVAL;
   PhiArgs a = make_args(p);
   for (int f = 0; f < nfields; ++f) a.gin[f] = grids[f];
-  dim3 grid(p->nlat2 / a.NP, p->nz, nfields);
+  dim3 grid(p->nlat2 / a.NP, p->sel_kz ? p->sel_n : p->nz, nfields);
   size_t smem = (size_t)a.NP * seq_stride(p->nphi) * sizeof(double2);
   TimedLaunch tl(p, T_PHI_FWD, st);
   switch (p->nphi) {
@@ -333,7 +335,7 @@ int launch_phi_inv(const sph_plan* p, double* const* grids, int nfields, cudaStr
   if (p->nphi > PMAXC) return SPH_EINVAL;
   PhiArgs a = make_args(p);
   for (int f = 0; f < nfields; ++f) a.gout[f] = grids[f];
-  dim3 grid(p->nlat2 / a.NP, p->nz, nfields);
+  dim3 grid(p->nlat2 / a.NP, p->sel_kz ? p->sel_n : p->nz, nfields);
   size_t smem = (size_t)a.NP * seq_stride(p->nphi) * sizeof(double2);
   TimedLaunch tl(p, T_PHI_INV, st);
   switch (p->nphi) {

@@ -181,14 +181,14 @@ int launch_mode(const ZArgs& a, int nblocks, size_t smem, cudaStream_t st) {
 }  // namespace
 
 int launch_zfft(const sph_plan* p, int mode, const double2* in, double2* out, int order,
-                cudaStream_t st) {
+                cudaStream_t st, bool cont) {
   ZArgs a;
   a.in = in;
   a.out = out;
   a.nlm = p->nlm;
   a.nz = p->nz;
-  a.N = p->N;
-  a.C = p->C;
+  a.N = cont ? p->N : p->nz;
+  a.C = cont ? p->C : 0;
   a.d = p->d;
   a.order = order;
   a.dir = p->d_dir;

@@ -167,7 +167,7 @@ static void plan_free(sph_plan* p) {
   void* ptrs[] = {p->P, p->dP, p->mPs, p->wfold, p->wfull, p->d_dir, p->d_z, p->kfac, p->filt,
                   p->zinv2, p->d_ell, p->d_mbase, p->twz, p->twphi, p->twzf, p->twphif, p->revz,
                   p->revphi, p->twpz, p->twpphi, p->twpzf, p->twpphif, p->tilesA,
-                  p->tilesA32, p->tilesS, p->tilesS32, p->G, p->binv, p->d2bor, p->energy};
+                  p->tilesA32, p->tilesS, p->tilesS32, p->G, p->binv, p->d2bor, p->energy, p->d_bplanes};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (auto& q : p->sp)
@@ -308,6 +308,7 @@ extern "C" int sph_plan_create(sph_plan** out, int lmax, int nlat, int nphi, int
   int rc = SPH_OK;
 #define UP(dst, vec)                                              \
   if (rc == SPH_OK) rc = upload(&(dst), (vec).data(), (vec).size());
+#define UPLOAD_OK(dst, vec) UP(dst, vec)
   UP(p->P, hP);
   UP(p->dP, hdP);
   UP(p->mPs, hmPs);
@@ -334,7 +335,6 @@ extern "C" int sph_plan_create(sph_plan** out, int lmax, int nlat, int nphi, int
   UP(p->tilesS, tS);
   UP(p->tilesS32, tS32);
   if (Cz > 0) UP(p->d_dir, p->dir);
-#undef UP
   p->ntilesA = (int)tA.size();
   p->ntilesA32 = (int)tA32.size();
   p->ntilesS = (int)tS.size();
@@ -357,6 +357,15 @@ extern "C" int sph_plan_create(sph_plan** out, int lmax, int nlat, int nphi, int
     rc = SPH_ECUDA;
   if (rc == SPH_OK && cudaMalloc((void**)&p->energy, sizeof(double)) != cudaSuccess) rc = SPH_ENOMEM;
   if (rc == SPH_OK && precision == SPH_MIXED) rc = mixed_setup(p, hP, hdP, hmPs);
+  if (rc == SPH_OK && precision == SPH_MIXED && Cz > 0 && oz > 0) {
+    std::vector<int> bp;
+    for (int k = 0; k < p->N; ++k)
+      if (k < oz || k >= p->N - oz) bp.push_back(k);
+    p->nbplanes = (int)bp.size();
+    UPLOAD_OK(p->d_bplanes, bp);
+  }
+#undef UPLOAD_OK
+#undef UP
   if (rc != SPH_OK) {
     plan_free(p);
     return rc;
@@ -490,12 +499,30 @@ extern "C" int sph_timer_read(sph_plan* p, double* ms, int* launches) {
 #define D2(x) reinterpret_cast<double2*>(x)
 #define CD2(x) reinterpret_cast<const double2*>(x)
 
+// Selects the planes that feed the FC-Gram continuation for the FP64
+// launchers while it lives (mixed plans recompute them in FP64).
+struct BoundaryPlanes {
+  const sph_plan* p;
+  explicit BoundaryPlanes(const sph_plan* p_) : p(p_) {
+    p->sel_kz = p->d_bplanes;
+    p->sel_n = p->nbplanes;
+  }
+  ~BoundaryPlanes() {
+    p->sel_kz = nullptr;
+    p->sel_n = 0;
+  }
+};
+
 extern "C" int sph_fftp2d_real_to_complex_xy(sph_plan* p, const double* in, double* out, void* s) {
   if (!p || !in || !out) return SPH_EINVAL;
   const double* g[1] = {in};
   if (p->precision == SPH_MIXED) {
     RC(launch_phi_fwd32(p, g, 1, ST(s)));
-    return launch_tc_analysis(p, 0, D2(out), nullptr, ST(s));
+    RC(launch_tc_analysis(p, 0, D2(out), nullptr, ST(s)));
+    if (!p->nbplanes || !p->bpass) return SPH_OK;
+    BoundaryPlanes sel(p);
+    RC(launch_phi_fwd(p, g, 1, ST(s)));
+    return launch_leg_analysis(p, 0, D2(out), ST(s));
   }
   RC(launch_phi_fwd(p, g, 1, ST(s)));
   return launch_leg_analysis(p, 0, D2(out), ST(s));
@@ -506,7 +533,11 @@ extern "C" int sph_fftp2d_complex_to_real_xy(sph_plan* p, const double* in, doub
   double* g[1] = {out};
   if (p->precision == SPH_MIXED) {
     RC(launch_tc_synthesis(p, 0, CD2(in), nullptr, ST(s)));
-    return launch_phi_inv32(p, g, 1, ST(s));
+    RC(launch_phi_inv32(p, g, 1, ST(s)));
+    if (!p->nbplanes || !p->bpass) return SPH_OK;
+    BoundaryPlanes sel(p);
+    RC(launch_leg_synthesis(p, CD2(in), 0, ST(s)));
+    return launch_phi_inv(p, g, 1, ST(s));
   }
   RC(launch_leg_synthesis(p, CD2(in), 0, ST(s)));
   return launch_phi_inv(p, g, 1, ST(s));
@@ -523,6 +554,16 @@ extern "C" int sph_fftp1d_complex_to_real_z(sph_plan* p, double* inout, void* s)
 }
 
 extern "C" int sph_fftp3d_real_to_complex(sph_plan* p, const double* in, double* out, void* s) {
+  if (p && in && out && p->precision == SPH_MIXED && p->C > 0 && p->contg) {
+    // continue the physical planes first (FP64): the continuation then acts
+    // on exact data and the angular round-off of every plane stays local
+    const double* g[1] = {in};
+    const double* gh[1] = {p->contg};
+    RC(launch_cont_phys(p, g, 1, ST(s)));
+    RC(launch_phi_fwd32(p, g, 1, ST(s), gh));
+    RC(launch_tc_analysis(p, 0, D2(out), nullptr, ST(s)));
+    return launch_zfft(p, Z_FWD, CD2(out), D2(out), 0, ST(s), false);
+  }
   RC(sph_fftp2d_real_to_complex_xy(p, in, out, s));
   return sph_fftp1d_real_to_complex_z(p, out, s);
 }
@@ -539,7 +580,12 @@ extern "C" int sph_fftp2d_vec_to_qst(sph_plan* p, const double* vr, const double
   if (p->precision == SPH_MIXED) {
     RC(launch_phi_fwd32(p, g, 3, ST(s)));
     RC(launch_tc_analysis(p, 0, D2(q), nullptr, ST(s)));
-    return launch_tc_analysis(p, 1, D2(sO), D2(t), ST(s));
+    RC(launch_tc_analysis(p, 1, D2(sO), D2(t), ST(s)));
+    if (!p->nbplanes || !p->bpass) return SPH_OK;
+    BoundaryPlanes sel(p);
+    RC(launch_phi_fwd(p, g, 3, ST(s)));
+    RC(launch_leg_analysis(p, 0, D2(q), ST(s)));
+    return launch_vec_analysis(p, D2(sO), D2(t), ST(s));
   }
   RC(launch_phi_fwd(p, g, 3, ST(s)));
   RC(launch_leg_analysis(p, 0, D2(q), ST(s)));
@@ -553,11 +599,42 @@ extern "C" int sph_fftp2d_qst_to_vec(sph_plan* p, const double* q, const double*
   if (p->precision == SPH_MIXED) {
     RC(launch_tc_synthesis(p, 0, CD2(q), nullptr, ST(s)));
     RC(launch_tc_synthesis(p, 1, CD2(sI), CD2(t), ST(s)));
-    return launch_phi_inv32(p, g, 3, ST(s));
+    RC(launch_phi_inv32(p, g, 3, ST(s)));
+    if (!p->nbplanes || !p->bpass) return SPH_OK;
+    BoundaryPlanes sel(p);
+    RC(launch_leg_synthesis(p, CD2(q), 0, ST(s)));
+    RC(launch_vec_synthesis(p, CD2(sI), CD2(t), ST(s)));
+    return launch_phi_inv(p, g, 3, ST(s));
   }
   RC(launch_leg_synthesis(p, CD2(q), 0, ST(s)));
   RC(launch_vec_synthesis(p, CD2(sI), CD2(t), ST(s)));
   return launch_phi_inv(p, g, 3, ST(s));
+}
+
+extern "C" int sph_fftp3d_vec_to_qst(sph_plan* p, const double* vr, const double* vt, const double* vp,
+                                     double* q, double* sO, double* t, void* s) {
+  if (!p || !vr || !vt || !vp || !q || !sO || !t) return SPH_EINVAL;
+  if (p->precision == SPH_MIXED && p->C > 0 && p->contg) {
+    const double* g[3] = {vr, vt, vp};
+    const double* gh[3] = {p->contg, p->contg + (size_t)p->C * p->nphi * p->nlat,
+                           p->contg + (size_t)2 * p->C * p->nphi * p->nlat};
+    RC(launch_cont_phys(p, g, 3, ST(s)));
+    RC(launch_phi_fwd32(p, g, 3, ST(s), gh));
+    RC(launch_tc_analysis(p, 0, D2(q), nullptr, ST(s)));
+    RC(launch_tc_analysis(p, 1, D2(sO), D2(t), ST(s)));
+    for (double* x : {q, sO, t}) RC(launch_zfft(p, Z_FWD, CD2(x), D2(x), 0, ST(s), false));
+    return SPH_OK;
+  }
+  RC(sph_fftp2d_vec_to_qst(p, vr, vt, vp, q, sO, t, s));
+  for (double* x : {q, sO, t}) RC(sph_fftp1d_real_to_complex_z(p, x, s));
+  return SPH_OK;
+}
+
+extern "C" int sph_fftp3d_qst_to_vec(sph_plan* p, double* q, double* sI, double* t, double* vr, double* vt,
+                                     double* vp, void* s) {
+  if (!p || !vr || !vt || !vp || !q || !sI || !t) return SPH_EINVAL;
+  for (double* x : {q, sI, t}) RC(sph_fftp1d_complex_to_real_z(p, x, s));
+  return sph_fftp2d_qst_to_vec(p, q, sI, t, vr, vt, vp, s);
 }
 
 // ---------------------------------------------------------------- operators
@@ -811,8 +888,18 @@ extern "C" int sph_v_imposebc_fast(sph_plan* p, double* tor, double* phi, double
 }
 
 // ---------------------------------------------------------------- NL + RK3
+// Mixed plans: inside the NL step the planes that feed the FC-Gram
+// continuation are transformed in FP64 as well, so that the radial
+// derivatives of the step do not amplify their angular round-off.
+struct BoundaryPass {
+  const sph_plan* p;
+  explicit BoundaryPass(const sph_plan* p_) : p(p_) { p->bpass = 1; }
+  ~BoundaryPass() { p->bpass = 0; }
+};
+
 static int nl_rhs_impl(sph_plan* p, const double2* Z, const double2* W, const double2* F, double nu,
                        double2* rz, double2* rf, cudaStream_t st) {
+  BoundaryPass bp(p);
   double2 *s0 = p->sp[0], *s1 = p->sp[1], *s2 = p->sp[2], *s3 = p->sp[3], *s4 = p->sp[4];
   double* g[9];
   for (int i = 0; i < 9; ++i) g[i] = p->gr[i];

@@ -37,9 +37,11 @@ struct LegTile {
 };
 
 // Mixed-precision (tcgen05) work item: one m, one parity (or output fold),
-// one block of at most 256 MMA rows; its Legendre table tiles sit in HBM as
-// nk consecutive blocks of [hi | lo] fp16 (2 x nr x 32 halves each, 8x8 core
-// matrices, K-major), pre-scaled by the power of two tscale.
+// one block of at most 128 (scalar) or 64 (vector) MMA rows; its Legendre
+// table tiles sit in HBM as nk consecutive blocks of [hi | mid | lo] bf16
+// (3 x nr x 32 values each, 8x8 core matrices, K-major).  Vector items come
+// in twins (out = 0: S or Vt, out = 1: T or Vp) sharing their blocks; their
+// first nk1 K steps are the dP part, the rest the mPs part.
 struct TcItem {
   int m, par, r0, nr, nvalid, nk, nk1, out;
   long long boff;  // first table block, in halves
@@ -50,7 +52,7 @@ struct TcItem {
 struct TcSet {
   TcItem* items = nullptr;  // device
   int nitems = 0;
-  __half* blocks = nullptr;  // device
+  uint16_t* blocks = nullptr;  // device, bf16 bit patterns
   size_t nhalves = 0;
 };
 
@@ -109,13 +111,29 @@ struct sph_plan {
   double* binv = nullptr;   // [lmax][N-4][N]  M_l column-major per l
   double* d2bor = nullptr;  // [N][4]
   double* energy = nullptr; // device accumulator (1 double)
-  // mixed precision: fp16 hi/lo tables for the tcgen05 GEMMs, fp32 folded
-  // coefficients G32 (reusing the G allocation), running data maxima
+  // mixed precision: bf16 table tiles for the tcgen05 GEMMs, bf16 data tiles
+  // (analysis: written by the phi FFT; synthesis: from the spectra), fp32
+  // folded coefficients G32 of the synthesis (reusing the G allocation)
   TcSet tcAS, tcAV, tcSS, tcSV;  // analysis scalar/vector, synthesis scalar/vector
   int ldn8 = 0;                  // node stride of G32 (nlat/2 rounded up to 8)
+  int nkn = 0;                   // K tiles of 32 nodes
   size_t G32field = 0;           // float2 elements per G32 field
-  float* dmax = nullptr;         // [4] max |value| per data operand (bit-compared)
+  uint16_t* Tana = nullptr;      // [3][m][fold][plane block][node tile] x 24 KB
+  uint16_t* Tsyn = nullptr;      // [2][m][parity][plane block][l tile] x 24 KB
+  size_t Tsynfield = 0;          // bf16 values per synthesis field
+  long long* d_toff = nullptr;   // [lmax+1][2] first synthesis tile of each block
   int* dflag = nullptr;          // device status word (bounded waits that gave up)
+  int nsm = 0;                   // SMs of the plan's device (persistent grids)
+  // planes that feed the FC-Gram continuation ([0, oz) and [N-oz, N)); a
+  // mixed plan transforms them again in FP64, because the continuation
+  // operator (norm ~1e4) amplifies their round-off into every radial mode
+  int* d_bplanes = nullptr;
+  int nbplanes = 0;
+  // plane selection of the FP64 phi and Legendre launchers (nullptr: all nz)
+  mutable const int* sel_kz = nullptr;
+  mutable int sel_n = 0;
+  mutable int bpass = 0;         // mixed 2D transforms recompute d_bplanes in FP64
+  double* contg = nullptr;       // [3][Cz][nphi][nlat] physically continued planes (mixed)
   // stage timers (sph_timer_*): event pairs recorded around each launch
   int timing = 0;
   std::vector<cudaEvent_t> ev_pool;
@@ -155,8 +173,9 @@ __device__ __forceinline__ double2 cmul_si(double2 a, int sign) {
 // ---------------------------------------------------------------- launchers
 // z transforms (k_zfft.cu)
 enum ZMode { Z_FWD = 0, Z_INV = 1, Z_DERIV = 2, Z_FILTER = 3, Z_DLR = 4 };
+// cont = false: the planes past N are taken as given (already continued)
 int launch_zfft(const sph_plan* p, int mode, const double2* in, double2* out, int order,
-                cudaStream_t st);
+                cudaStream_t st, bool cont = true);
 
 // phi transforms (k_phifft.cu): grid fields -> folded coefficients and back
 int launch_phi_fwd(const sph_plan* p, const double* const* grids, int nfields, cudaStream_t st);
@@ -189,7 +208,12 @@ int launch_energy(const sph_plan* p, const double* ur, const double* ut, const d
 int mixed_setup(sph_plan* p, const std::vector<double>& hP, const std::vector<double>& hdP,
                 const std::vector<double>& hmPs);
 void mixed_free(sph_plan* p);
-int launch_phi_fwd32(const sph_plan* p, const double* const* grids, int nfields, cudaStream_t st);
+// grids_hi: planes k >= N of field f come from grids_hi[f] + (k - N) planes
+int launch_phi_fwd32(const sph_plan* p, const double* const* grids, int nfields, cudaStream_t st,
+                     const double* const* grids_hi = nullptr);
+// FC-Gram continuation of physical fields: planes N..nz-1 of each field into
+// p->contg (field f at f * Cz planes), from its planes 0..oz-1 and N-oz..N-1
+int launch_cont_phys(const sph_plan* p, const double* const* grids, int nfields, cudaStream_t st);
 int launch_phi_inv32(const sph_plan* p, double* const* grids, int nfields, cudaStream_t st);
 int launch_tc_analysis(const sph_plan* p, int vector, double2* out, double2* out2, cudaStream_t st);
 int launch_tc_synthesis(const sph_plan* p, int vector, const double2* in, const double2* in2,

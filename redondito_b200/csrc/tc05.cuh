@@ -31,7 +31,7 @@ __device__ __forceinline__ uint64_t smem_desc(const void* base, uint32_t lbo_byt
 }
 
 // Instruction descriptor, kind::f16: A = B = fp16, D = fp32, both K-major,
-// M rows (64 or 128), N columns (multiple of 8 up to 256).
+// M rows (64 or 128), N columns (multiple of 16 up to 256 for M = 128).
 __host__ __device__ constexpr uint32_t idesc_f16(int M, int N) {
   return (1u << 4)                      // D format f32
          | (0u << 7) | (0u << 10)       // A, B format f16
@@ -39,6 +39,9 @@ __host__ __device__ constexpr uint32_t idesc_f16(int M, int N) {
          | ((uint32_t)(N >> 3) << 17)   // N / 8
          | ((uint32_t)(M >> 4) << 24);  // M / 16
 }
+
+// The same with A = B = bf16.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) { return idesc_f16(M, N) | (1u << 7) | (1u << 10); }
 
 // D[tmem] (+)= A[smem] * B[smem]; issued by one thread.
 __device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -81,6 +84,23 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// The same without the wait: several loads, then one tmem_wait_ld().
+__device__ __forceinline__ void tmem_ld16_nw(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+// Orders later uses of r after tmem_wait_ld() (volatile asm keeps its place).
+__device__ __forceinline__ void tmem_regs(uint32_t (&r)[16]) {
+  asm volatile(""
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                 "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                 "+r"(r[15]));
 }
 
 // ---------------------------------------------------------------- mbarriers

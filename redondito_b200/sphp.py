@@ -45,7 +45,7 @@ SYMBOLS = (
     "sph_setup_bc", "sph_dirichlet", "sph_invDl", "sph_v_imposebc", "sph_v_imposebc_fast",
     "sph_nl_rhs", "sph_rk3_step",
     "sph_timer_enable", "sph_timer_reset", "sph_timer_read",
-    "sph_derivr_noalloc", "sph_plan_status",
+    "sph_derivr_noalloc", "sph_plan_status", "sph_fftp3d_vec_to_qst", "sph_fftp3d_qst_to_vec",
 )
 TIMER_CLASSES = ("phi_fwd", "phi_inv", "leg_analysis", "leg_synthesis", "vec_analysis",
                  "vec_synthesis", "zfft", "ops")
@@ -107,6 +107,8 @@ def lib(build_if_missing=True):
             "sph_timer_read": [P, pD, pI],
             "sph_derivr_noalloc": [Vp, Vp, I, I, I, I, D, D, pD, I, Vp],
             "sph_plan_status": [P],
+            "sph_fftp3d_vec_to_qst": [P] + [Vp] * 6 + [Vp],
+            "sph_fftp3d_qst_to_vec": [P] + [Vp] * 6 + [Vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -257,6 +259,18 @@ def fftp2d_vec_to_qst(plan, vr, vt, vp, q, s, t, stream=None):
 
 def fftp2d_qst_to_vec(plan, q, s, t, vr, vt, vp, stream=None):
     _call("sph_fftp2d_qst_to_vec", plan.h, _s(plan, q), _s(plan, s), _s(plan, t),
+          _g(plan, vr), _g(plan, vt), _g(plan, vp), _stream(stream))
+
+
+def fftp3d_vec_to_qst(plan, vr, vt, vp, q, s, t, stream=None):
+    """fftp2d_vec_to_qst followed by the z transform of q, s and t."""
+    _call("sph_fftp3d_vec_to_qst", plan.h, _g(plan, vr), _g(plan, vt), _g(plan, vp),
+          _s(plan, q), _s(plan, s), _s(plan, t), _stream(stream))
+
+
+def fftp3d_qst_to_vec(plan, q, s, t, vr, vt, vp, stream=None):
+    """Inverse z transform of q, s, t (in place), then fftp2d_qst_to_vec."""
+    _call("sph_fftp3d_qst_to_vec", plan.h, _s(plan, q), _s(plan, s), _s(plan, t),
           _g(plan, vr), _g(plan, vt), _g(plan, vp), _stream(stream))
 
 

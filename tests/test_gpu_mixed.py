@@ -1,8 +1,9 @@
 """SPH_MIXED plans (tensor-core Legendre contractions, fp32 phi FFTs) against
-the CPU oracle on the same seeded inputs.  The mixed form keeps about 22
-significant bits per operand and accumulates in fp32, so its outputs are
-held to relative L2 <= 1e-6 (TOL_MIXED); outputs that also pass through the
-FP64 z transforms with FC-Gram continuation keep the same bound."""
+the CPU oracle on the same seeded inputs.  The mixed form splits every
+operand into three bf16 pieces (about 24 significant bits) and accumulates
+in fp32, so its transforms are held to relative L2 <= 1e-6 (TOL_MIXED),
+the 3D transforms with FC-Gram continuation included; right-hand sides that
+take radial derivatives are held to TOL_NL."""
 import numpy as np
 import pytest
 
@@ -78,7 +79,7 @@ def test_mixed_vector(lmax, nz, nlat, nphi):
 
 
 def test_mixed_full_angular_size():
-    """lmax 511 on the 768 x 1536 grid (two planes): the 256-row items."""
+    """lmax 511 on the 768 x 1536 grid (two planes): 256 rows per parity."""
     from redondito_b200 import sphp as S
     P, G = _pair(511, 2, 768, 1536)
     rng = np.random.default_rng(511)
@@ -94,6 +95,50 @@ def test_mixed_full_angular_size():
     print(f"lmax=511 synthesis {e_syn:.2e} round trip {e_rt:.2e}")
     assert e_syn < TOL_MIXED
     assert e_rt < 2 * TOL_MIXED
+
+
+def test_mixed_3d_vector_pair_with_continuation():
+    from redondito_b200 import sphp as S
+    P, G = _pair(63, 70, 96, 192, C=25, d=5)
+    rng = np.random.default_rng(78)
+    qst = [P.z_forward(random_spec(P, rng)) for _ in range(3)]
+    for x in qst[1:]:
+        x[:, 0] = 0
+    ref_grids = P.qst_synthesis(*(P.z_inverse(x) for x in qst))
+    g = [G.new_grid() for _ in range(3)]
+    S.fftp3d_qst_to_vec(G, *(dev(x) for x in qst), *g)
+    e_inv = [rel_l2(host(a), b) for a, b in zip(g, ref_grids)]
+    ref = [P.z_forward(x) for x in P.qst_analysis(*ref_grids)]
+    out = [G.new_spec() for _ in range(3)]
+    S.fftp3d_vec_to_qst(G, *(dev(x) for x in ref_grids), *out)
+    S.plan_status(G)
+    e_fwd = [rel_l2(host(a), b) for a, b in zip(out, ref)]
+    print(f"3D vector inverse {max(e_inv):.2e} forward {max(e_fwd):.2e}")
+    assert max(e_inv) < TOL_MIXED
+    assert max(e_fwd) < TOL_MIXED
+
+
+def test_mixed_nl_rhs():
+    """The NL step on a mixed plan (its continuation-feeding planes in FP64):
+    the right-hand sides, which take radial derivatives of the analysed
+    products, against the FP64 oracle within TOL_NL."""
+    from redondito_b200 import sphp as S
+    TOL_NL = 1e-5
+    P, G = _pair(15, 64, 24, 48, C=25, d=5)
+    P.bc_setup()
+    S.setup_bc(G)
+    rng = np.random.default_rng(3)
+    Z = random_spec(P, rng, power=3.0)
+    W = random_spec(P, rng, power=3.0)
+    Z, phi, W = P.imposebc(Z, P.dlr(W))
+    rz_ref, rf_ref, e_ref = P.nl_rhs(Z, W, phi, 1e-3)
+    rz, rf = G.new_spec(), G.new_spec()
+    e = S.nl_rhs(G, dev(Z), dev(W), dev(phi), 1e-3, rz, rf)
+    S.plan_status(G)
+    print(f"NL rhs_z {rel_l2(host(rz), rz_ref):.2e} rhs_phi {rel_l2(host(rf), rf_ref):.2e} energy {abs(e - e_ref) / e_ref:.2e}")
+    assert abs(e - e_ref) / e_ref < TOL_MIXED
+    assert rel_l2(host(rz), rz_ref) < TOL_NL
+    assert rel_l2(host(rf), rf_ref) < TOL_NL
 
 
 def test_mixed_3d_pair_with_continuation():
@@ -114,7 +159,7 @@ def test_mixed_3d_pair_with_continuation():
 
 def test_mixed_zero_and_spike_inputs():
     """A zero field stays exactly zero; one large coefficient among small ones
-    is resolved to the same relative accuracy (per-field power-of-two scale)."""
+    is resolved to the same relative accuracy (bf16 pieces need no scaling)."""
     from redondito_b200 import sphp as S
     P, G = _pair(31, 4, 48, 96)
     s = G.new_spec()

@@ -258,3 +258,25 @@ def test_sht_full_angular_size(lmax, nlat, nphi):
     S.fftp2d_vec_to_qst(G, *[dev(x) for x in v_ref], *qs)
     for o, r in zip(qs, P.qst_analysis(*v_ref)):
         assert rel_l2(host(o), r) < TOL
+
+
+def test_3d_vector_pair():
+    """fftp3d_qst_to_vec / fftp3d_vec_to_qst equal the compositions of the
+    2D vector transforms with the z transforms of q, s, t."""
+    from redondito_b200 import sphp as S
+    P, G = _pair(31, 64, C=25, d=5, nlat=48, nphi=96)
+    rng = np.random.default_rng(21)
+    qst = [P.z_forward(random_spec(P, rng)) for _ in range(3)]
+    for x in qst[1:]:
+        x[:, 0] = 0
+    ref_grids = P.qst_synthesis(*(P.z_inverse(x) for x in qst))
+    d = [dev(x) for x in qst]
+    g = [G.new_grid() for _ in range(3)]
+    S.fftp3d_qst_to_vec(G, *d, *g)
+    for a, b in zip(g, ref_grids):
+        assert rel_l2(host(a), b) < TOL_CONT
+    ref = [P.z_forward(x) for x in P.qst_analysis(*ref_grids)]
+    out = [G.new_spec() for _ in range(3)]
+    S.fftp3d_vec_to_qst(G, *(dev(x) for x in ref_grids), *out)
+    for a, b in zip(out, ref):
+        assert rel_l2(host(a), b) < TOL_CONT
