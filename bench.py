@@ -43,7 +43,9 @@ sys.path.insert(0, ROOT)
 
 W = dict(lmax=511, nlat=768, nphi=1536, nz=256, Cz=25, oz=5, rint=0.35, rext=1.0)
 # a smaller case of the same kernels for ncu captures (each grid 150 MB, still > L2)
-CASES = {"c3": W, "small": dict(lmax=255, nlat=384, nphi=768, nz=64, Cz=25, oz=5, rint=0.35, rext=1.0)}
+CASES = {"c3": W, "small": dict(lmax=255, nlat=384, nphi=768, nz=64, Cz=25, oz=5, rint=0.35, rext=1.0),
+         # the benchmark's angular size on 32 planes (each grid 302 MB)
+         "angular": dict(lmax=511, nlat=768, nphi=1536, nz=32, Cz=25, oz=5, rint=0.35, rext=1.0)}
 METRIC = "3D transform pairs/s at lmax=511 nr=256"
 SEED = 20261203 + 3
 
@@ -54,11 +56,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
+                    help="mixed (the headline, with the FP64 form timed beside it) or fp64")
+    ap.add_argument("--no-fp64", action="store_true", help="mixed only: skip the FP64 comparison")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--case", default="c3", choices=sorted(CASES),
-                    help="c3: the benchmark workload; small: profiling case for ncu")
+                    help="c3: the benchmark workload; small, angular: profiling cases for ncu")
     a = ap.parse_args()
     W.update(CASES[a.case]) if a.case != "c3" else None
     return a
@@ -220,16 +224,22 @@ def fp64_peak():
         return None
 
 
-def algorithmic_work(P, nfield_passes):
-    """Bytes (HBM kernels) or flops (Legendre) per step for each kernel class."""
+def algorithmic_work(P, mixed):
+    """Bytes (HBM kernels) or flops (Legendre) per step for each kernel class:
+    compulsory reads + writes at their storage precision (grid FP64; folded
+    coefficients FP64 complex, or in the mixed form bf16 x 3 pieces (12 B per
+    complex) written by the forward phi FFT and fp32 complex read by the
+    inverse; spectra FP64 complex); useful Legendre flops 4 nz (nlat/2) nlm
+    per scalar direction (5x for a vector field)."""
     nlm, nz, nlat, nphi, lmax = P.nlm, P.nz, P.nlat, P.nphi, P.lmax
     grid_b = nlat * nphi * nz * 8
-    fold_b = (lmax + 1) * nlat * nz * 16
+    cplx = (lmax + 1) * nlat * nz  # folded coefficients of one field (both parities)
     spec_b = nlm * nz * 16
-    leg = 4.0 * nz * (nlat // 2) * nlm  # flops, one scalar direction (even/odd folded)
+    leg = 4.0 * nz * (nlat // 2) * nlm
+    fwd_fold, inv_fold = (12, 8) if mixed else (16, 16)
     return {
-        "phi_fwd": ("hbm", 4 * (grid_b + fold_b)),
-        "phi_inv": ("hbm", 4 * (grid_b + fold_b)),
+        "phi_fwd": ("hbm", 4 * (grid_b + cplx * fwd_fold)),
+        "phi_inv": ("hbm", 4 * (grid_b + cplx * inv_fold)),
         "zfft": ("hbm", 8 * 2 * spec_b),
         "leg_analysis": ("tensor", 2 * leg),
         "leg_synthesis": ("tensor", 2 * leg),
@@ -237,6 +247,60 @@ def algorithmic_work(P, nfield_passes):
         "vec_synthesis": ("tensor", 4 * leg),
         "ops": ("hbm", 0),
     }
+
+
+def time_pairs(S, P, st, grids, steps, stream, torch, dist, world):
+    """Device time of `steps` pairs (barrier + sync on both sides, max over ranks)."""
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        pair(S, P, st, grids)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=P.device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms
+
+
+def per_output_errors(S, Pm, Pd, st0, torch):
+    """Each transform of the pair once on the same inputs in both forms: the
+    inverse from the seeded spectra, the forward from the FP64 inverse's
+    grids.  Relative L2 and max-abs (relative to max |FP64|) per output."""
+    def inverse(P, spec):
+        a, q, s, t = (x.clone() for x in spec)
+        g = [P.new_grid() for _ in range(4)]
+        S.fftp3d_complex_to_real(P, a, g[0])
+        S.fftp3d_qst_to_vec(P, q, s, t, g[1], g[2], g[3])
+        return g
+
+    def forward(P, grids):
+        out = [P.new_spec() for _ in range(4)]
+        S.fftp3d_real_to_complex(P, grids[0], out[0])
+        S.fftp3d_vec_to_qst(P, grids[1], grids[2], grids[3], out[1], out[2], out[3])
+        return out
+
+    rel, mx = {}, {}
+    gd = inverse(Pd, st0)
+    gm = inverse(Pm, st0)
+    for name, a, b in zip(("grid_scalar", "grid_vr", "grid_vt", "grid_vp"), gm, gd):
+        rel[name] = float((torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)).item())
+        mx[name] = float(((a - b).abs().max() / b.abs().max()).item())
+    del gm
+    sd = forward(Pd, gd)
+    sm = forward(Pm, gd)
+    for name, a, b in zip(("spec_scalar", "Q", "S", "T"), sm, sd):
+        rel[name] = float((torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)).item())
+        mx[name] = float(((a - b).abs().max() / b.abs().max()).item())
+    torch.cuda.synchronize()
+    return rel, mx
 
 
 def main():
@@ -255,12 +319,13 @@ def main():
         dist.init_process_group("nccl", device_id=torch.device("cuda", local))
 
     prec = S.SPH_FP64 if args.precision == "fp64" else S.SPH_MIXED
-    P = S.Plan(W["lmax"], W["nz"], nlat=W["nlat"], nphi=W["nphi"], Cz=W["Cz"], oz=W["oz"],
-               rint=W["rint"], rext=W["rext"], precision=prec)
+    mk = lambda pr: S.Plan(W["lmax"], W["nz"], nlat=W["nlat"], nphi=W["nphi"], Cz=W["Cz"], oz=W["oz"],
+                           rint=W["rint"], rext=W["rext"], precision=pr)
+    P = mk(prec)
     gen = torch.Generator(device=P.device)
     gen.manual_seed(SEED + rank)
     st = make_state(S, P, torch, gen)
-    ref = [x.clone() for x in st]
+    st0 = [x.clone() for x in st]
     grids = [P.new_grid() for _ in range(4)]
     stream = torch.cuda.current_stream()
 
@@ -288,36 +353,22 @@ def main():
 
     S.timer_reset(P)
     S.timer_enable(P, True)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(args.steps):
-        pair(S, P, st, grids)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    ms = time_pairs(S, P, st, grids, args.steps, stream, torch, dist, world)
     S.timer_enable(P, False)
     clocks = clk.stop()
-    ms = e0.elapsed_time(e1)
     stage = S.timer_read(P)
-    if world > 1:
-        t = torch.tensor([ms], device=P.device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     ms_step = ms / args.steps
     value = world * args.steps / (ms * 1e-3)
 
-    # parity at full size: a pair is the identity on a forward-transformed state
-    rt = [float((torch.linalg.vector_norm(x - r) / torch.linalg.vector_norm(r)).item()) for x, r in zip(st, ref)]
+    # a pair on a forward-transformed state is the identity up to rounding
+    rt = [float((torch.linalg.vector_norm(x - r) / torch.linalg.vector_norm(r)).item()) for x, r in zip(st, st0)]
 
     # e2e through the C ABI with host buffers
     e2e = None
     if not args.no_e2e:
         host = [x.cpu().pin_memory() for x in st]
         nbytes = sum(h.numel() * h.element_size() for h in host)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
@@ -338,8 +389,26 @@ def main():
         e2e = {"value": world * args.steps / (ems * 1e-3), "unit": "pairs/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
 
+    # the FP64 form on the same state: its time, and the mixed form's error per output
+    fp64 = None
+    errors = None
+    if prec == S.SPH_MIXED and not args.no_fp64:
+        Pd = mk(S.SPH_FP64)
+        std = [x.clone() for x in st0]
+        gd = [Pd.new_grid() for _ in range(4)]
+        for _ in range(max(1, args.warmup)):
+            pair(S, Pd, std, gd)
+        msd = time_pairs(S, Pd, std, gd, args.steps, stream, torch, dist, world)
+        fp64 = {"value": world * args.steps / (msd * 1e-3), "unit": "pairs/s", "ms_per_step": msd / args.steps}
+        del std, gd
+        rel, mx = per_output_errors(S, P, Pd, st0, torch)
+        errors = {"rel_l2_vs_fp64": rel, "max_abs_vs_fp64": mx,
+                  "note": "each transform on the same inputs in both forms; the FP64 form matches "
+                          "the CPU oracle to 1e-12 (tests/test_gpu_parity.py)"}
+        Pd.close()
+
     # roofline of the dominant kernel class
-    work = algorithmic_work(P, 4)
+    work = algorithmic_work(P, prec == S.SPH_MIXED)
     dom = max(stage, key=lambda c: stage[c][0])
     bound, per_step = work[dom]
     tms, nl = stage[dom]
@@ -384,6 +453,9 @@ def main():
         "gpu_launches": launches,
         "roofline": roofline,
         "stage_share": shares,
+        "fp64": fp64,
+        "speedup_vs_fp64": (value / fp64["value"]) if fp64 else None,
+        "accuracy": errors,
         "roundtrip_rel_l2": {"scalar": rt[0], "Q": rt[1], "S": rt[2], "T": rt[3]},
         "clocks": clocks,
         "cpu_baseline": cpu,

@@ -167,7 +167,7 @@ __device__ __forceinline__ void pass(T2* buf, const Geo<N, PAD, JFAST>& g, const
 // position of frequency k after dif<N> (the rev[] table, computed from the
 // compile-time radix sequence): k = q0 + R0 (q1 + R1 (...)), pos = sum q_p s_p
 template <int N, int L = N>
-__device__ __forceinline__ int rev_pos(int k) {
+__host__ __device__ constexpr int rev_pos(int k) {
   constexpr int R = radix_of(L), S = L / R;
   if constexpr (S == 1) {
     return k;  // last digit, span 1
@@ -175,6 +175,40 @@ __device__ __forceinline__ int rev_pos(int k) {
     const int q = k % R;
     return q * S + rev_pos<N, S>(k / R);
   }
+}
+
+// Serial in-register decimation-in-frequency FFT of length R on v[R]
+// (natural order in; frequency k out at v[rev_pos<R>(k)]), the same passes
+// and twiddle table layout (pass_twiddles of length R) as the shared-memory
+// version, every index known at compile time so v stays in registers.
+template <typename T2, int R, int L = R>
+__device__ __forceinline__ void reg_dif(T2 (&v)[R], const T2* __restrict__ twp, int sign) {
+  constexpr int RR = radix_of(L), S = L / RR;
+  constexpr int TOFF = tw_entries(R) - tw_entries(L);
+#pragma unroll
+  for (int blk = 0; blk < R / L; ++blk) {
+#pragma unroll
+    for (int j = 0; j < S; ++j) {
+      T2 x[RR];
+#pragma unroll
+      for (int r = 0; r < RR; ++r) x[r] = v[blk * L + j + r * S];
+      Dft<T2, RR>::run(x, sign);
+      if constexpr (S > 1) {
+#pragma unroll
+        for (int r = 1; r < RR; ++r) x[r] = mul(x[r], twl(twp + TOFF + j * (RR - 1) + r - 1, sign));
+      }
+#pragma unroll
+      for (int r = 0; r < RR; ++r) v[blk * L + j + r * S] = x[r];
+    }
+  }
+  if constexpr (S > 1) reg_dif<T2, R, S>(v, twp, sign);
+}
+
+// Four-step split of a phi length N = N1 * N2 (N1 the power-of-two part,
+// at most 32): N1-point DFTs over the stride-N2 subsequences, the twiddle
+// W_N^(n2 k1), then N2-point DFTs; frequency k1 + N1 k2.
+__host__ __device__ constexpr int split_n1(int n) {
+  return n % 32 == 0 ? 32 : n % 16 == 0 ? 16 : n % 8 == 0 ? 8 : n % 4 == 0 ? 4 : n % 2 == 0 ? 2 : 1;
 }
 
 template <typename T2, int N, int L, int PAD, bool JFAST>

@@ -424,7 +424,170 @@ struct Phi32Args {
   int nlat, ldn8, nz, lmax, NP, ncb, nkn;
   const double* wfold;
   const float2* twp;
+  const float2* tw1;  // four-step kernels: pass twiddles of length N1 and N2,
+  const float2* tw2;  // and W_N^e = exp(-2 pi i e / N)
+  const float2* twN;
 };
+
+// Four-step phi FFT geometry (N = N1 N2, NP ring pairs per CTA).  Shared
+// memory: X[b][k1][n2] (forward) or X[b][n2][k1] (inverse) with row pitch
+// = 1 (mod 16) and sequence stride = 4 (mod 16) float2 slots, so that the
+// lanes of a warp (8 sequences x 4 rows) hit 32 distinct slots; the forward
+// kernel overwrites each row k1 with its spectrum Z(k1 + N1 k2), k2 along
+// the row.
+constexpr int up_mod16(int x, int r) { return x + (((r - x) % 16) + 16) % 16; }
+template <int N, int NP>
+struct P4 {
+  static constexpr int N1 = ct::split_n1(N), N2 = N / N1;
+  // about two work items per thread, so that two CTAs fit an SM's registers
+  static constexpr int THREADS = ((NP * (N1 > N2 ? N1 : N2) + 1) / 2 + 31) / 32 * 32;
+  static constexpr int PF = up_mod16(N2, 1), SF = up_mod16(N1 * PF, 4);
+  static constexpr int PI = up_mod16(N1, 1), SI = up_mod16(N2 * PI, 4);
+  static constexpr size_t SMEM_FWD = (size_t)NP * SF * sizeof(float2);
+  static constexpr size_t SMEM_INV = (size_t)NP * SI * sizeof(float2);
+};
+
+// Forward, four-step: (1) thread (b, n2) loads x[n2 + N2 n1] of ring pair b
+// straight from the grid into registers, an N1-point DFT, the twiddle
+// W_N^(n2 k1), one store to X; (2) thread (b, k1) an N2-point DFT of row
+// k1 giving Z(k1 + N1 k2), written back over the row; (3) thread m folds
+// both parities of the NP nodes from Z(m), Z(-m) and writes them, split, as
+// row chunks of the analysis tiles.
+template <int N, int NP>
+__global__ void __launch_bounds__(P4<N, NP>::THREADS, 2) phi4_fwd32(Phi32Args a) {
+  using C = P4<N, NP>;
+  constexpr int N1 = C::N1, N2 = C::N2;
+  extern __shared__ float2 sx[];
+  const int nlat = a.nlat;
+  const int p0 = blockIdx.x * NP, k = blockIdx.y, f = blockIdx.z;
+  const int t = threadIdx.x;
+  const double* plane =
+      k < a.ksplit ? a.gin[f] + (size_t)k * N * nlat : a.gin_hi[f] + (size_t)(k - a.ksplit) * N * nlat;
+  for (int it = t; it < NP * N2; it += C::THREADS) {
+    const int b = it % NP, n2 = it / NP;
+    const double* pr = plane + p0 + b;               // ring p0 + b (real part)
+    const double* pm = plane + (nlat - 1 - p0 - b);  // its mirror (imaginary part)
+    float2 v[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const size_t j = (size_t)(n2 + N2 * n1) * nlat;
+      v[n1] = make_float2((float)__ldg(pr + j), (float)__ldg(pm + j));
+    }
+    ct::reg_dif<float2, N1>(v, a.tw1, -1);
+    float2* X = sx + b * C::SF + n2;
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) {
+      float2 z = v[ct::rev_pos<N1>(k1)];
+      if (k1) z = ct::mul(z, __ldg(a.twN + n2 * k1));
+      X[k1 * C::PF] = z;
+    }
+  }
+  __syncthreads();
+  // step 2: each row X[b][k1][.] becomes the spectrum Z(k1 + N1 k2) in place
+  for (int it = t; it < NP * N1; it += C::THREADS) {
+    const int b2 = it % NP, k1 = it / NP;
+    float2* X = sx + b2 * C::SF + k1 * C::PF;
+    float2 w[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) w[n2] = X[n2];
+    ct::reg_dif<float2, N2>(w, a.tw2, -1);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) X[k2] = w[ct::rev_pos<N2>(k2)];
+  }
+  __syncthreads();
+  float W[NP];
+#pragma unroll
+  for (int b = 0; b < NP; ++b) W[b] = (float)__ldg(a.wfold + p0 + b);
+  const int cb = k / PLANES, row = 2 * (k % PLANES), kt = p0 / TK, kk0 = p0 % TK;
+  for (int m = t; m <= a.lmax; m += C::THREADS) {
+    float er[NP], ei[NP], orr[NP], oi[NP];
+#pragma unroll
+    for (int b = 0; b < NP; ++b) {
+      const int mc = m == 0 ? 0 : N - m;
+      const float2 Z = sx[b * C::SF + (m % N1) * C::PF + m / N1];
+      const float2 Zc = sx[b * C::SF + (mc % N1) * C::PF + mc / N1];
+      // F(ring) = (Z + conj Z(-m))/2, F(mirror) = -i (Z - conj Z(-m))/2
+      const float fir = 0.5f * (Z.x + Zc.x), fii = 0.5f * (Z.y - Zc.y);
+      const float fmr = 0.5f * (Z.y + Zc.y), fmi = -0.5f * (Z.x - Zc.x);
+      er[b] = (fir + fmr) * W[b];
+      ei[b] = (fii + fmi) * W[b];
+      orr[b] = (fir - fmr) * W[b];
+      oi[b] = (fii - fmi) * W[b];
+    }
+    __nv_bfloat16* t0 = a.tiles + ana_tile(a.lmax, a.ncb, a.nkn, f, m, 0, cb, kt) * TILE_HALVES;
+    __nv_bfloat16* t1 = a.tiles + ana_tile(a.lmax, a.ncb, a.nkn, f, m, 1, cb, kt) * TILE_HALVES;
+    store_tile_row<NP>(t0, row, kk0, er);
+    store_tile_row<NP>(t0, row + 1, kk0, ei);
+    store_tile_row<NP>(t1, row, kk0, orr);
+    store_tile_row<NP>(t1, row + 1, kk0, oi);
+  }
+}
+
+// Inverse, four-step: (1) thread (b, k1) assembles Z(k1 + N1 k2) of ring
+// pair b from the folded coefficients (zero past lmax), an N2-point DFT, the
+// twiddle W_N^(-n2 k1), one store to X; (2) thread (b, n2) an N1-point DFT
+// and the grid stores x[n2 + N2 n1] (real part: ring, imaginary: mirror).
+template <int N, int NP>
+__global__ void __launch_bounds__(P4<N, NP>::THREADS, 2) phi4_inv32(Phi32Args a) {
+  using C = P4<N, NP>;
+  constexpr int N1 = C::N1, N2 = C::N2;
+  extern __shared__ float2 sx[];
+  const int nlat = a.nlat, lmax = a.lmax;
+  const int p0 = blockIdx.x * NP, k = blockIdx.y, f = blockIdx.z;
+  const int t = threadIdx.x;
+  for (int it = t; it < NP * N1; it += C::THREADS) {
+    const int b = it % NP, k1 = it / NP;
+    const float2* G = a.G32c + (size_t)f * a.G32field + (size_t)k * a.ldn8 + p0 + b;
+    const size_t mstride = (size_t)2 * a.nz * a.ldn8, pstride = (size_t)a.nz * a.ldn8;
+    float2 w[N2];
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) {
+      const int m = k1 + N1 * k2;
+      const bool lo = m <= lmax, hi = N - m <= lmax;
+      const int mm = lo ? m : N - m;
+      float2 z = make_float2(0.f, 0.f);
+      if (lo || hi) {
+        const float2 se = __ldg(G + mm * mstride), so = __ldg(G + mm * mstride + pstride);
+        const float2 Fi = make_float2(se.x + so.x, se.y + so.y), Fm = make_float2(se.x - so.x, se.y - so.y);
+        if (m == 0) z = make_float2(Fi.x, Fm.x);
+        else if (lo) z = make_float2(Fi.x - Fm.y, Fi.y + Fm.x);
+        else z = make_float2(Fi.x + Fm.y, -Fi.y + Fm.x);
+      }
+      w[k2] = z;
+    }
+    ct::reg_dif<float2, N2>(w, a.tw2, +1);
+    float2* X = sx + b * C::SI + k1;
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) {
+      float2 z = w[ct::rev_pos<N2>(n2)];
+      if (n2) {
+        float2 tw = __ldg(a.twN + n2 * k1);
+        tw.y = -tw.y;
+        z = ct::mul(z, tw);
+      }
+      X[n2 * C::PI] = z;
+    }
+  }
+  __syncthreads();
+  for (int it = t; it < NP * N2; it += C::THREADS) {
+    const int b = it % NP, n2 = it / NP;
+    float2 v[N1];
+    const float2* X = sx + b * C::SI + n2 * C::PI;
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) v[k1] = X[k1];
+    ct::reg_dif<float2, N1>(v, a.tw1, +1);
+    double* plane = a.gout[f] + (size_t)k * N * nlat;
+    double* pr = plane + p0 + b;
+    double* pm = plane + (nlat - 1 - p0 - b);
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const size_t j = (size_t)(n2 + N2 * n1) * nlat;
+      const float2 z = v[ct::rev_pos<N1>(n1)];
+      pr[j] = (double)z.x;
+      pm[j] = (double)z.y;
+    }
+  }
+}
 
 // Forward: ring pairs p0..p0+NP-1 of plane k, field f.  The samples are
 // placed at their digit-reversed positions and transformed by the
@@ -899,8 +1062,37 @@ int run_phi(K kernel, const Phi32Args& a, dim3 grid, size_t smem, cudaStream_t s
   return SPH_OK;
 }
 
+template <typename K>
+int run_phi4(K kernel, const Phi32Args& a, dim3 grid, int threads, size_t smem, cudaStream_t st) {
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+      cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess)
+    return SPH_ECUDA;
+  kernel<<<grid, threads, smem, st>>>(a);
+  SPH_LAUNCH_OK();
+  return SPH_OK;
+}
+
+template <int N, int NP, bool FWD>
+int phi4_np(const Phi32Args& a, dim3 grid, cudaStream_t st) {
+  using C = P4<N, NP>;
+  if constexpr (FWD) return run_phi4(phi4_fwd32<N, NP>, a, grid, C::THREADS, C::SMEM_FWD, st);
+  else return run_phi4(phi4_inv32<N, NP>, a, grid, C::THREADS, C::SMEM_INV, st);
+}
+
 template <int N, bool FWD>
 int phi32_n(const Phi32Args& a, dim3 grid, size_t smem, cudaStream_t st) {
+  // the four-step form for the forward transform; the inverse keeps the
+  // shared-memory passes (more resident warps hide its grid stores better)
+  if constexpr (FWD && N <= 1536) {
+    if (a.tw1 && a.tw2) {
+      switch (a.NP) {
+        case 8: return phi4_np<N, 8, FWD>(a, grid, st);
+        case 4: return phi4_np<N, 4, FWD>(a, grid, st);
+        case 2: return phi4_np<N, 2, FWD>(a, grid, st);
+        case 1: return phi4_np<N, 1, FWD>(a, grid, st);
+      }
+    }
+  }
   switch (a.NP) {
     case 8:
       if constexpr (8 * N <= PMAXC) return run_phi(FWD ? phi_fwd32<N, 8> : phi_inv32<N, 8>, a, grid, smem, st);
@@ -942,6 +1134,9 @@ Phi32Args phi32_args(const sph_plan* p) {
   a.wfold = p->wfold;
   a.twp = p->fphi.twpf;
   a.ksplit = p->nz;
+  a.tw1 = p->tw4f;
+  a.tw2 = p->tw4f ? p->tw4f + p->tw4off : nullptr;
+  a.twN = p->twphif;
   return a;
 }
 

@@ -12,6 +12,7 @@
 #include <cstdlib>
 #include <thread>
 
+#include "fft_ct.cuh"
 #include "sph_internal.cuh"
 
 typedef long double ld;
@@ -166,7 +167,7 @@ static void plan_free(sph_plan* p) {
   mixed_free(p);
   void* ptrs[] = {p->P, p->dP, p->mPs, p->wfold, p->wfull, p->d_dir, p->d_z, p->kfac, p->filt,
                   p->zinv2, p->d_ell, p->d_mbase, p->twz, p->twphi, p->twzf, p->twphif, p->revz,
-                  p->revphi, p->twpz, p->twpphi, p->twpzf, p->twpphif, p->tilesA,
+                  p->revphi, p->twpz, p->twpphi, p->twpzf, p->twpphif, p->tw4f, p->tw4d, p->tilesA,
                   p->tilesA32, p->tilesS, p->tilesS32, p->G, p->binv, p->d2bor, p->energy, p->d_bplanes};
   for (void* q : ptrs)
     if (q) cudaFree(q);
@@ -298,6 +299,16 @@ extern "C" int sph_plan_create(sph_plan** out, int lmax, int nlat, int nphi, int
   std::vector<float2> tpzf, tppf;
   pass_twiddles(nz, tpz, tpzf);
   pass_twiddles(nphi, tpp, tppf);
+  std::vector<double2> t4, t4b;
+  std::vector<float2> t4f, t4fb;
+  {
+    const int n1 = ct::split_n1(nphi), n2 = nphi / n1;
+    pass_twiddles(n1, t4, t4f);
+    p->tw4off = (int)t4.size();
+    pass_twiddles(n2, t4b, t4fb);
+    t4.insert(t4.end(), t4b.begin(), t4b.end());
+    t4f.insert(t4f.end(), t4fb.begin(), t4fb.end());
+  }
   auto tA = row_tiles(lmax, 64, true, n2);
   auto tA32 = row_tiles(lmax, 32, true, n2);
   auto tS = row_tiles(lmax, 64, false, n2);
@@ -330,6 +341,8 @@ extern "C" int sph_plan_create(sph_plan** out, int lmax, int nlat, int nphi, int
   UP(p->twpphi, tpp);
   UP(p->twpzf, tpzf);
   UP(p->twpphif, tppf);
+  UP(p->tw4f, t4f);
+  UP(p->tw4d, t4);
   UP(p->tilesA, tA);
   UP(p->tilesA32, tA32);
   UP(p->tilesS, tS);

@@ -87,6 +87,10 @@ struct sph_plan {
   double2* twpphi = nullptr;
   float2* twpzf = nullptr;
   float2* twpphif = nullptr;
+  // four-step phi FFT (nphi = N1 N2): pass twiddles of length N1, then N2 at tw4off
+  float2* tw4f = nullptr;
+  double2* tw4d = nullptr;
+  int tw4off = 0;
   FftDesc fz, fphi;
   // Legendre work lists (device)
   LegTile* tilesA = nullptr;   // analysis: (m, l0) blocks of 64 l
