@@ -240,6 +240,31 @@ int sph_timer_read(sph_plan* plan, double* ms, int* launches);
  * outputs of those calls are invalid) and clears the record, else SPH_OK. */
 int sph_plan_status(sph_plan* plan);
 
+/* ---------------------------------------------------------------- batches
+ * Many independent shell problems in one CUDA graph (no reference
+ * counterpart: the reference runs one problem per set of MPI ranks).
+ * Problem p is a plan (all of the same precision, timers off) with
+ * nfields[p] = 1..3 scalar fields; the per-field device arrays are given in
+ * (problem, field) order: spec (nlm x nz complex, (lm, kz) spectra), grid
+ * (nlat x nphi x nz) and dspec (nlm x nz complex).  sph_batch_run computes
+ * for every field
+ *   spec  -> z inverse in place (fftp1d_complex_to_real_z),
+ *   dspec  = derivr(spec, 1, 'r')  (radial derivative, radial space),
+ *   grid   = angular synthesis of spec (spec, grid: fftp3d_complex_to_real),
+ *   spec   = fftp3d_real_to_complex(grid),
+ * with the Legendre contractions of all problems in one grouped launch per
+ * direction and the rest on parallel graph branches.  The graph is built
+ * once by sph_batch_create (the arrays and plans must outlive the batch);
+ * a plan's scratch is used by its batch, so do not run other work on the
+ * same plans concurrently.  sph_batch_status synchronises the device and
+ * returns SPH_ETIMEDOUT if a bounded device wait of the batch gave up. */
+typedef struct sph_batch sph_batch;
+int sph_batch_create(sph_batch** batch, int nprob, sph_plan* const* plans, const int* nfields,
+                     double* const* spec, double* const* grid, double* const* dspec);
+int sph_batch_run(sph_batch* batch, void* stream);
+int sph_batch_status(sph_batch* batch);
+int sph_batch_destroy(sph_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -83,7 +83,38 @@ struct LegArgs {
   const int* mbase;
   const int* kzl;  // planes to transform (nullptr: all nz)
   int lmax, ldn, nz, nlm, nkz;
+  int ntiles;      // tiles of this work set (grouped launches)
 };
+
+// Grouped launches: the CTAs of several plans' work sets in one grid; job j
+// owns CTAs prefix[j] .. prefix[j+1]-1, laid out (plane block, tile).
+struct LegGroup {
+  const LegArgs* jobs;
+  const int* prefix;
+  int njobs;
+};
+
+// This CTA's arguments and (tile, plane block) indices.
+template <bool G>
+__device__ __forceinline__ void leg_cta(const LegArgs& a0, const LegGroup& grp, LegArgs& a, int& bx, int& by) {
+  if constexpr (!G) {
+    a = a0;
+    bx = blockIdx.x;
+    by = blockIdx.y;
+  } else {
+    int lo = 0, hi = grp.njobs - 1;
+    const int c = blockIdx.x;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(grp.prefix + mid) <= c) lo = mid;
+      else hi = mid - 1;
+    }
+    a = grp.jobs[lo];
+    const int local = c - __ldg(grp.prefix + lo);
+    bx = local % a.ntiles;
+    by = local / a.ntiles;
+  }
+}
 
 // plane of local index kl (blockIdx.y * KZ + offset); ok = within the selection
 __device__ __forceinline__ int plane_of(const LegArgs& a, int kl, bool& ok) {
@@ -104,12 +135,16 @@ constexpr int STAGE = A_SZ + B_SZ;
 constexpr int SMEM = STAGES * STAGE * 8;
 }  // namespace an
 
-__global__ void __launch_bounds__(128) leg_analysis_kernel(LegArgs a) {
+template <bool GROUP>
+__global__ void __launch_bounds__(128) leg_analysis_kernel(LegArgs a0, LegGroup grp) {
   using namespace an;
   extern __shared__ __align__(16) double sm[];
-  const LegTile tile = a.tiles[blockIdx.x];
+  LegArgs a;
+  int bx, by;
+  leg_cta<GROUP>(a0, grp, a, bx, by);
+  const LegTile tile = a.tiles[bx];
   const int m = tile.m, l0 = tile.r0;
-  const int kz0 = blockIdx.y * KZ;
+  const int kz0 = by * KZ;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
   const int par = warp >> 1, nh = warp & 1;
   const double2* G = a.G + (size_t)a.gfield * a.Gfield + (size_t)m * 2 * a.nz * a.ldn;
@@ -199,12 +234,16 @@ constexpr int STAGE = A_SZ + B_SZ;
 constexpr int SMEM = STAGES * STAGE * 8;
 }  // namespace sy
 
-__global__ void __launch_bounds__(256) leg_synthesis_kernel(LegArgs a) {
+template <bool GROUP>
+__global__ void __launch_bounds__(256) leg_synthesis_kernel(LegArgs a0, LegGroup grp) {
   using namespace sy;
   extern __shared__ __align__(16) double sm[];
-  const LegTile tile = a.tiles[blockIdx.x];
+  LegArgs a;
+  int bx, by;
+  leg_cta<GROUP>(a0, grp, a, bx, by);
+  const LegTile tile = a.tiles[bx];
   const int m = tile.m, i0 = tile.r0;
-  const int kz0 = blockIdx.y * KZ;
+  const int kz0 = by * KZ;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
   const int par = warp >> 2, mh = (warp >> 1) & 1, nh = warp & 1;
   const size_t base_lm = (size_t)a.mbase[m] - m;
@@ -531,11 +570,11 @@ int launch_leg_analysis(const sph_plan* p, int gfield, double2* spec, cudaStream
   a.gfield = gfield;
   a.out = spec;
   a.tiles = p->tilesA;
-  static bool once = set_smem(leg_analysis_kernel, an::SMEM);
+  static bool once = set_smem(leg_analysis_kernel<false>, an::SMEM);
   if (!once) return SPH_ECUDA;
   dim3 grid(p->ntilesA, (a.nkz + an::KZ - 1) / an::KZ);
   TimedLaunch tl(p, T_LEG_ANA, st);
-  leg_analysis_kernel<<<grid, 128, an::SMEM, st>>>(a);
+  leg_analysis_kernel<false><<<grid, 128, an::SMEM, st>>>(a, LegGroup{});
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
@@ -545,11 +584,11 @@ int launch_leg_synthesis(const sph_plan* p, const double2* spec, int gfield, cud
   a.gfield = gfield;
   a.spec = spec;
   a.tiles = p->tilesS;
-  static bool once = set_smem(leg_synthesis_kernel, sy::SMEM);
+  static bool once = set_smem(leg_synthesis_kernel<false>, sy::SMEM);
   if (!once) return SPH_ECUDA;
   dim3 grid(p->ntilesS, (a.nkz + sy::KZ - 1) / sy::KZ);
   TimedLaunch tl(p, T_LEG_SYN, st);
-  leg_synthesis_kernel<<<grid, 256, sy::SMEM, st>>>(a);
+  leg_synthesis_kernel<false><<<grid, 256, sy::SMEM, st>>>(a, LegGroup{});
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
@@ -580,4 +619,66 @@ int launch_vec_synthesis(const sph_plan* p, const double2* s, const double2* t, 
   vec_synthesis_kernel<<<grid, 256, vs::SMEM, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;
+}
+
+// ---------------------------------------------------------------- grouped launches
+int leg_group_prepare(bool analysis, const std::vector<GroupJob>& jobs, GroupLaunch* g) {
+  std::vector<LegArgs> args;
+  std::vector<int> prefix;
+  long long total = 0;
+  for (const GroupJob& j : jobs) {
+    if (j.p->precision != SPH_FP64 || j.field < 0 || j.field >= SPH_MAX_FIELDS) return SPH_EINVAL;
+    LegArgs a = base_args(j.p);
+    a.gfield = j.field;
+    if (analysis) {
+      a.out = j.spec;
+      a.tiles = j.p->tilesA;
+      a.ntiles = j.p->ntilesA;
+    } else {
+      a.spec = j.spec;
+      a.tiles = j.p->tilesS;
+      a.ntiles = j.p->ntilesS;
+    }
+    const int kz = analysis ? an::KZ : sy::KZ;
+    prefix.push_back((int)total);
+    total += (long long)a.ntiles * ((a.nkz + kz - 1) / kz);
+    args.push_back(a);
+  }
+  if (total > (1ll << 30)) return SPH_EINVAL;
+  g->analysis = analysis;
+  g->njobs = (int)jobs.size();
+  g->total = (int)total;
+  g->grid = (int)total;
+  if (jobs.empty()) return SPH_OK;
+  if (cudaMalloc(&g->jobs, args.size() * sizeof(LegArgs)) != cudaSuccess ||
+      cudaMalloc((void**)&g->prefix, prefix.size() * sizeof(int)) != cudaSuccess)
+    return SPH_ENOMEM;
+  if (cudaMemcpy(g->jobs, args.data(), args.size() * sizeof(LegArgs), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(g->prefix, prefix.data(), prefix.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+    return SPH_ECUDA;
+  return SPH_OK;
+}
+
+int leg_group_launch(const GroupLaunch& g, cudaStream_t st) {
+  if (g.total == 0) return SPH_OK;
+  const LegGroup grp{static_cast<const LegArgs*>(g.jobs), g.prefix, g.njobs};
+  if (g.analysis) {
+    static bool once = set_smem(leg_analysis_kernel<true>, an::SMEM);
+    if (!once) return SPH_ECUDA;
+    leg_analysis_kernel<true><<<g.grid, 128, an::SMEM, st>>>(LegArgs{}, grp);
+  } else {
+    static bool once = set_smem(leg_synthesis_kernel<true>, sy::SMEM);
+    if (!once) return SPH_ECUDA;
+    leg_synthesis_kernel<true><<<g.grid, 256, sy::SMEM, st>>>(LegArgs{}, grp);
+  }
+  SPH_LAUNCH_OK();
+  return SPH_OK;
+}
+
+void group_free(GroupLaunch* g) {
+  if (g->jobs) cudaFree(g->jobs);
+  if (g->prefix) cudaFree(g->prefix);
+  g->jobs = nullptr;
+  g->prefix = nullptr;
+  g->njobs = g->total = g->grid = 0;
 }

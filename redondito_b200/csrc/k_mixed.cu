@@ -153,34 +153,81 @@ __device__ __forceinline__ const __nv_bfloat16* a_tile(const TcArgs& a, const Tc
   return a.tiles + (size_t)field * a.tfield + syn_tile(a.toff, a.lmax, it.m, par, cb, kk) * TILE_HALVES;
 }
 
+// A launch of the tensor-core kernel: one work set (`one`), or a group of
+// work sets from several plans (`jobs`, job j owning the global units
+// prefix[j] .. prefix[j+1]-1) walked by the same persistent CTAs.
+struct TcLaunch {
+  TcArgs one;
+  const TcArgs* jobs;   // grouped launches (nullptr: `one`)
+  const int* prefix;    // [njobs] first global unit of each job
+  int njobs, total;     // total work units
+  int* flag;            // status word of the launch
+};
+
+template <bool G>
+__device__ __forceinline__ int job_of(const TcLaunch& L, int u) {
+  if constexpr (!G) {
+    return 0;
+  } else {
+    int lo = 0, hi = L.njobs - 1;  // last job whose first unit is <= u
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(L.prefix + mid) <= u) lo = mid;
+      else hi = mid - 1;
+    }
+    return lo;
+  }
+}
+
+// The work unit u of a launch: its job's arguments, item and plane block.
+template <bool G>
+struct Unit {
+  TcArgs a;
+  TcItem it;
+  int cb;
+  __device__ __forceinline__ void load(const TcLaunch& L, int u) {
+    int lu = u;
+    if constexpr (G) {
+      const int j = job_of<G>(L, u);
+      a = L.jobs[j];
+      lu = u - __ldg(L.prefix + j);
+    } else {
+      a = L.one;
+    }
+    it = a.items[lu / a.ncb];
+    cb = lu % a.ncb;
+  }
+};
+
 // Walks the K steps of this CTA's work units in order (units with no K
 // steps are skipped).
+template <bool G>
 struct TileCur {
   int u, kt;
-  TcItem it;
-  __device__ void skip(const TcArgs& a) {
-    while (u < a.nunits && kt >= it.nk) {
+  Unit<G> w;
+  __device__ void skip(const TcLaunch& L) {
+    while (u < L.total && kt >= w.it.nk) {
       u += gridDim.x;
       kt = 0;
-      if (u < a.nunits) it = a.items[u / a.ncb];
+      if (u < L.total) w.load(L, u);
     }
   }
-  __device__ void init(const TcArgs& a) {
+  __device__ void init(const TcLaunch& L) {
     u = blockIdx.x;
     kt = 0;
-    if (u < a.nunits) it = a.items[u / a.ncb];
-    skip(a);
+    if (u < L.total) w.load(L, u);
+    skip(L);
   }
-  __device__ void next(const TcArgs& a) {
+  __device__ void next(const TcLaunch& L) {
     ++kt;
-    skip(a);
+    skip(L);
   }
-  __device__ bool valid(const TcArgs& a) const { return u < a.nunits; }
+  __device__ bool valid(const TcLaunch& L) const { return u < L.total; }
 };
 
 // ---------------------------------------------------------------- tensor-core kernel
-template <int MODE>
-__global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm(TcArgs a) {
+template <int MODE, bool G>
+__global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm(TcLaunch L) {
   extern __shared__ __align__(1024) unsigned char smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + OFF_BAR);
   uint64_t* full = bars;                 // [STAGES] data + table tiles landed
@@ -195,8 +242,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm(TcArgs a) {
   constexpr bool vector = (MODE == ANA_V || MODE == SYN_V);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-  // once any CTA of the plan has given up a wait, later launches do no work
-  if (tid == 0) *abort_flag = *(volatile int*)a.flag;
+  // once any CTA of the launch's owner has given up a wait, later launches do no work
+  if (tid == 0) *abort_flag = *(volatile int*)L.flag;
   __syncthreads();
   if (*abort_flag) return;
   __syncthreads();
@@ -219,28 +266,29 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm(TcArgs a) {
   tc05::fence_after();
   const uint32_t tbase = *tslot;
   auto fail = [&]() {
-    atomicExch(a.flag, 1);
+    atomicExch(L.flag, 1);
     *abort_flag = 1;
   };
 
   if (warp == 0) {
     // ------------------------------------------------------------ bulk copies
     if (lane == 0) {
-      TileCur cur;
-      cur.init(a);
+      TileCur<G> cur;
+      cur.init(L);
       int g = 0;
-      for (; cur.valid(a); ++g, cur.next(a)) {
+      for (; cur.valid(L); ++g, cur.next(L)) {
         const int s = g % STAGES, n = g / STAGES;
         if (n > 0 && (*abort_flag || !tc05::mbar_wait(&empty[s], (n - 1) & 1))) {
           fail();
           break;
         }
-        const __nv_bfloat16* At = a_tile<MODE>(a, cur.it, cur.u % a.ncb, cur.kt);
-        const uint32_t bbytes = (uint32_t)(NPIECE * cur.it.nr * TK * 2);
+        const TcItem& it = cur.w.it;
+        const __nv_bfloat16* At = a_tile<MODE>(cur.w.a, it, cur.w.cb, cur.kt);
+        const uint32_t bbytes = (uint32_t)(NPIECE * it.nr * TK * 2);
         unsigned char* st = smem + s * STAGE_BYTES;
         mbar_arrive_tx(&full[s], A_BYTES + bbytes);
         bulk_copy(st, At, A_BYTES, &full[s]);
-        bulk_copy(st + A_BYTES, a.blocks + cur.it.boff + (size_t)cur.kt * NPIECE * cur.it.nr * TK, bbytes,
+        bulk_copy(st + A_BYTES, cur.w.a.blocks + it.boff + (size_t)cur.kt * NPIECE * it.nr * TK, bbytes,
                   &full[s]);
       }
       // after a failure, copies may still be in flight: let them land
@@ -254,8 +302,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm(TcArgs a) {
     if (lane == 0) {
       int g = 0, uc = 0;
       bool ok = true;
-      for (int u = blockIdx.x; u < a.nunits && ok; u += gridDim.x, ++uc) {
-        const TcItem it = a.items[u / a.ncb];
+      for (int u = blockIdx.x; u < L.total && ok; u += gridDim.x, ++uc) {
+        Unit<G> w;
+        w.load(L, u);
+        const TcItem& it = w.it;
         const int buf = uc & 1;
         if (uc >= 2 && !tc05::mbar_wait(&accEmpty[buf], ((uc >> 1) - 1) & 1)) {
           ok = false;
@@ -316,8 +366,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm(TcArgs a) {
     double* stg = reinterpret_cast<double*>(smem + OFF_STG) + (warp - 2) * STG_WORDS;  // [32 lanes][17]
     const int j_out = lane & 15, ph = lane >> 4;  // store phase: row, plane half
     int uc = 0;
-    for (int u = blockIdx.x; u < a.nunits; u += gridDim.x, ++uc) {
-      const TcItem it = a.items[u / a.ncb];
+    for (int u = blockIdx.x; u < L.total; u += gridDim.x, ++uc) {
+      Unit<G> w;
+      w.load(L, u);
+      const TcArgs& a = w.a;
+      const TcItem& it = w.it;
       const int buf = uc & 1;
       bool ok = !*abort_flag && tc05::mbar_wait(&accFull[buf], (uc >> 1) & 1);
       ok = __all_sync(0xffffffffu, ok);
@@ -326,7 +379,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm(TcArgs a) {
         break;
       }
       tc05::fence_after();
-      const int kbase = (u % a.ncb) * PLANES + 16 * q;  // first plane of this warp
+      const int kbase = w.cb * PLANES + 16 * q;  // first plane of this warp
       const size_t base_lm = (size_t)a.mbase[it.m] - it.m;
       const uint32_t ta = tbase + (uint32_t)buf * 256 + ((uint32_t)(32 * q) << 16);
       const bool have0 = vector ? it.nk1 > 0 : it.nk > 0;
@@ -965,7 +1018,7 @@ int mixed_setup(sph_plan* p, const std::vector<double>& hP, const std::vector<do
     }
   p->Tsynfield = (size_t)nsyn * TILE_HALVES;
   const size_t nana = ana_tile(lmax, ncb, nkn, SPH_MAX_FIELDS, 0, 0, 0, 0) * TILE_HALVES;
-  const size_t bytes_ana = nana * 2, bytes_syn = 2 * p->Tsynfield * 2;
+  const size_t bytes_ana = nana * 2, bytes_syn = (size_t)SPH_MAX_FIELDS * p->Tsynfield * 2;
   if (rc == SPH_OK && cudaMalloc((void**)&p->Tana, bytes_ana) != cudaSuccess) rc = SPH_ENOMEM;
   if (rc == SPH_OK && cudaMemset(p->Tana, 0, bytes_ana) != cudaSuccess) rc = SPH_ECUDA;
   if (rc == SPH_OK && cudaMalloc((void**)&p->Tsyn, std::max<size_t>(16, bytes_syn)) != cudaSuccess) rc = SPH_ENOMEM;
@@ -1029,19 +1082,28 @@ TcArgs tc_args(const sph_plan* p) {
   return a;
 }
 
+template <int MODE, bool G>
+bool tc_attr() {
+  static const bool ok =
+      cudaFuncSetAttribute(tc_gemm<MODE, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM) == cudaSuccess;
+  return ok;
+}
+
 template <int MODE>
 int run_tc(const sph_plan* p, const TcSet& set, TcArgs a, cudaStream_t st) {
-  static const bool attr_ok =
-      cudaFuncSetAttribute(tc_gemm<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM) == cudaSuccess;
-  if (!attr_ok) return SPH_ECUDA;
+  if (!tc_attr<MODE, false>()) return SPH_ECUDA;
   const long long nunits = (long long)set.nitems * a.ncb;
   if (nunits == 0) return SPH_OK;
   if (nunits > (1ll << 30)) return SPH_EINVAL;
   a.items = set.items;
   a.blocks = reinterpret_cast<const __nv_bfloat16*>(set.blocks);
   a.nunits = (int)nunits;
+  TcLaunch L = {};
+  L.one = a;
+  L.total = (int)nunits;
+  L.flag = p->dflag;
   const int grid = (int)std::min<long long>(nunits, std::max(1, p->nsm));
-  tc_gemm<MODE><<<grid, TC_THREADS, TC_SMEM, st>>>(a);
+  tc_gemm<MODE, false><<<grid, TC_THREADS, TC_SMEM, st>>>(L);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
@@ -1198,4 +1260,72 @@ int launch_tc_synthesis(const sph_plan* p, int vector, const double2* in, const 
   }
   TimedLaunch tl(p, vector ? T_VEC_SYN : T_LEG_SYN, st);
   return vector ? run_tc<SYN_V>(p, p->tcSV, a, st) : run_tc<SYN_S>(p, p->tcSS, a, st);
+}
+
+// ---------------------------------------------------------------- grouped launches
+int tc_group_prepare(bool analysis, const std::vector<GroupJob>& jobs, int nsm, GroupLaunch* g) {
+  std::vector<TcArgs> args;
+  std::vector<int> prefix;
+  long long total = 0;
+  for (const GroupJob& j : jobs) {
+    const sph_plan* p = j.p;
+    if (p->precision != SPH_MIXED || j.field < 0 || j.field >= SPH_MAX_FIELDS) return SPH_EINVAL;
+    TcArgs a = tc_args(p);
+    const TcSet& set = analysis ? p->tcAS : p->tcSS;
+    a.items = set.items;
+    a.blocks = reinterpret_cast<const __nv_bfloat16*>(set.blocks);
+    if (analysis) {
+      const size_t per = ana_tile(p->lmax, a.ncb, a.nkn, 1, 0, 0, 0, 0) * TILE_HALVES;
+      a.tiles = reinterpret_cast<const __nv_bfloat16*>(p->Tana) + (size_t)j.field * per;
+      a.out = j.spec;
+    } else {
+      a.tiles = reinterpret_cast<const __nv_bfloat16*>(p->Tsyn) + (size_t)j.field * p->Tsynfield;
+      a.G32w = reinterpret_cast<float2*>(p->G) + (size_t)j.field * p->G32field;
+    }
+    a.nunits = set.nitems * a.ncb;
+    prefix.push_back((int)total);
+    total += a.nunits;
+    args.push_back(a);
+  }
+  if (total > (1ll << 30)) return SPH_EINVAL;
+  g->analysis = analysis;
+  g->njobs = (int)jobs.size();
+  g->total = (int)total;
+  g->grid = (int)std::min<long long>(total, std::max(1, nsm));
+  if (jobs.empty()) return SPH_OK;
+  if (cudaMalloc(&g->jobs, args.size() * sizeof(TcArgs)) != cudaSuccess ||
+      cudaMalloc((void**)&g->prefix, prefix.size() * sizeof(int)) != cudaSuccess)
+    return SPH_ENOMEM;
+  if (cudaMemcpy(g->jobs, args.data(), args.size() * sizeof(TcArgs), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(g->prefix, prefix.data(), prefix.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+    return SPH_ECUDA;
+  return SPH_OK;
+}
+
+int tc_group_launch(const GroupLaunch& g, int* flag, cudaStream_t st) {
+  if (g.total == 0) return SPH_OK;
+  TcLaunch L = {};
+  L.jobs = static_cast<const TcArgs*>(g.jobs);
+  L.prefix = g.prefix;
+  L.njobs = g.njobs;
+  L.total = g.total;
+  L.flag = flag;
+  if (g.analysis) {
+    if (!tc_attr<ANA_S, true>()) return SPH_ECUDA;
+    tc_gemm<ANA_S, true><<<g.grid, TC_THREADS, TC_SMEM, st>>>(L);
+  } else {
+    if (!tc_attr<SYN_S, true>()) return SPH_ECUDA;
+    tc_gemm<SYN_S, true><<<g.grid, TC_THREADS, TC_SMEM, st>>>(L);
+  }
+  SPH_LAUNCH_OK();
+  return SPH_OK;
+}
+
+int launch_spec_to_tiles_field(const sph_plan* p, const double2* in, int field, cudaStream_t st) {
+  if (p->precision != SPH_MIXED || field < 0 || field >= SPH_MAX_FIELDS) return SPH_EINVAL;
+  spec_to_tiles<<<dim3(p->lmax + 1, p->nz, 1), 32, 0, st>>>(
+      in, nullptr, reinterpret_cast<__nv_bfloat16*>(p->Tsyn) + (size_t)field * p->Tsynfield, p->Tsynfield,
+      p->d_toff, p->d_mbase, p->lmax, p->nlm);
+  SPH_LAUNCH_OK();
+  return SPH_OK;
 }

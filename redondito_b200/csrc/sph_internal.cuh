@@ -225,6 +225,27 @@ int launch_tc_synthesis(const sph_plan* p, int vector, const double2* in, const 
 int mixed_status(const sph_plan* p);
 bool mixed_nphi_ok(int nphi);  // phi lengths the fp32 phi kernels are built for
 
+// grouped launches over several plans' work sets (batches): one job per
+// (plan, field); the spectra are the synthesis input or the analysis output
+struct GroupJob {
+  const sph_plan* p;
+  int field;
+  double2* spec;
+};
+struct GroupLaunch {
+  void* jobs = nullptr;   // device array of the kernel's per-job arguments
+  int* prefix = nullptr;  // device [njobs]: first CTA (FP64) or work unit (mixed) of each job
+  int njobs = 0, total = 0, grid = 0;
+  bool analysis = false;
+};
+int leg_group_prepare(bool analysis, const std::vector<GroupJob>& jobs, GroupLaunch* g);
+int leg_group_launch(const GroupLaunch& g, cudaStream_t st);
+int tc_group_prepare(bool analysis, const std::vector<GroupJob>& jobs, int nsm, GroupLaunch* g);
+int tc_group_launch(const GroupLaunch& g, int* flag, cudaStream_t st);
+void group_free(GroupLaunch* g);
+// spectra -> synthesis data tiles of field slot `field` (mixed plans)
+int launch_spec_to_tiles_field(const sph_plan* p, const double2* in, int field, cudaStream_t st);
+
 #define SPH_CUDA_OK(call)                     \
   do {                                        \
     cudaError_t e_ = (call);                  \

@@ -46,6 +46,7 @@ SYMBOLS = (
     "sph_nl_rhs", "sph_rk3_step",
     "sph_timer_enable", "sph_timer_reset", "sph_timer_read",
     "sph_derivr_noalloc", "sph_plan_status", "sph_fftp3d_vec_to_qst", "sph_fftp3d_qst_to_vec",
+    "sph_batch_create", "sph_batch_run", "sph_batch_status", "sph_batch_destroy",
 )
 TIMER_CLASSES = ("phi_fwd", "phi_inv", "leg_analysis", "leg_synthesis", "vec_analysis",
                  "vec_synthesis", "zfft", "ops")
@@ -109,6 +110,11 @@ def lib(build_if_missing=True):
             "sph_plan_status": [P],
             "sph_fftp3d_vec_to_qst": [P] + [Vp] * 6 + [Vp],
             "sph_fftp3d_qst_to_vec": [P] + [Vp] * 6 + [Vp],
+            "sph_batch_create": [ctypes.POINTER(P), I, ctypes.POINTER(P), pI, ctypes.POINTER(P),
+                                 ctypes.POINTER(P), ctypes.POINTER(P)],
+            "sph_batch_run": [P, Vp],
+            "sph_batch_status": [P],
+            "sph_batch_destroy": [P],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -385,3 +391,47 @@ def timer_read(plan):
     n = (ctypes.c_int * len(TIMER_CLASSES))()
     _call("sph_timer_read", plan.h, ms, n)
     return {c: (ms[i], n[i]) for i, c in enumerate(TIMER_CLASSES)}
+
+
+# ---------------------------------------------------------------- batches
+class Batch:
+    """Independent problems run together (sph_batch_*): for every field of
+    every plan, the inverse 3D transform of `spec` into `grid` (z inverse in
+    place), `dspec` = derivr(spec, 1, 'r'), and the forward 3D transform of
+    `grid` back into `spec`; one CUDA graph, grouped Legendre launches."""
+
+    def __init__(self, plans, nfields):
+        self.plans = list(plans)
+        self.nfields = [int(n) for n in nfields]
+        self.spec, self.grid, self.dspec = [], [], []
+        for P, n in zip(self.plans, self.nfields):
+            self.spec.append([P.new_spec() for _ in range(n)])
+            self.grid.append([P.new_grid() for _ in range(n)])
+            self.dspec.append([P.new_spec() for _ in range(n)])
+        flat = [lambda xs=xs: [t for ts in xs for t in ts] for xs in (self.spec, self.grid, self.dspec)]
+        arrays = [f() for f in flat]
+        ptrs = [(ctypes.c_void_p * len(xs))(*[t.data_ptr() for t in xs]) for xs in arrays]
+        ph = (ctypes.c_void_p * len(self.plans))(*[P.h.value for P in self.plans])
+        nf = (ctypes.c_int * len(self.nfields))(*self.nfields)
+        self._keep = (ph, nf, *ptrs)
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.plans[0].device):
+            _call("sph_batch_create", ctypes.byref(h), len(self.plans), ph, nf, *ptrs)
+        self.h = h
+
+    def run(self, stream=None):
+        _call("sph_batch_run", self.h, _stream(stream))
+
+    def status(self):
+        _call("sph_batch_status", self.h)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().sph_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,94 @@
+"""Batches of independent problems (sph_batch_*): one CUDA graph with the
+Legendre contractions of every problem in one grouped launch per direction.
+Every output must equal, bit for bit, the same work done by the single-plan
+entry points (the grouped launches run the same arithmetic per work unit),
+and the FP64 batch must match the CPU oracle like the single-plan path."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests._helpers import rel_l2, random_spec
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+TOL_CONT = 1e-11
+# the derivative of a z-inverted input passes through two FC-Gram continued
+# transforms, each amplifying round-off by the continuation operator
+TOL_DERIV = 1e-10
+
+# (lmax, nz, nfields): the C4 ensemble's shapes at small sizes (nlat = 3(lmax+1)/2, nphi = 2 nlat)
+PROBLEMS = [(15, 32, 1), (31, 64, 3), (31, 32, 2), (63, 96, 1), (15, 64, 2), (63, 32, 3)]
+
+
+def dev(x):
+    return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+def _problem_inputs(lmax, nz, nf, seed):
+    nlat = 3 * (lmax + 1) // 2
+    P = O.Plan(lmax, nz, nlat=nlat, nphi=2 * nlat, C=25, d=5)
+    rng = np.random.default_rng(seed)
+    return P, [P.z_forward(random_spec(P, rng)) for _ in range(nf)]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_equals_single_plan_calls(precision):
+    from redondito_b200 import sphp as S
+    prec = S.SPH_FP64 if precision == "fp64" else S.SPH_MIXED
+    plans, inputs, orcs = [], [], []
+    for i, (lmax, nz, nf) in enumerate(PROBLEMS):
+        P, xs = _problem_inputs(lmax, nz, nf, 40 + i)
+        orcs.append(P)
+        plans.append(S.Plan(lmax, nz, nlat=P.nlat, nphi=P.nphi, Cz=25, oz=5, precision=prec))
+        inputs.append(xs)
+    B = S.Batch(plans, [len(x) for x in inputs])
+    for p, xs in enumerate(inputs):
+        for f, x in enumerate(xs):
+            B.spec[p][f].copy_(dev(x))
+    torch.cuda.synchronize()
+    B.run()
+    B.status()
+    for p, (G, xs) in enumerate(zip(plans, inputs)):
+        for f, x in enumerate(xs):
+            s = dev(x)
+            d = G.new_spec()
+            g = G.new_grid()
+            S.fftp1d_complex_to_real_z(G, s)
+            S.derivr(G, s, d, 1, "r")
+            S.fftp2d_complex_to_real_xy(G, s, g)
+            out = G.new_spec()
+            S.fftp3d_real_to_complex(G, g, out)
+            torch.cuda.synchronize()
+            assert torch.equal(B.grid[p][f], g), (p, f)
+            assert torch.equal(B.dspec[p][f], d), (p, f)
+            assert torch.equal(B.spec[p][f], out), (p, f)
+            if precision == "fp64":
+                P = orcs[p]
+                sr = P.z_inverse(x)
+                assert rel_l2(host(g), P.sh_synthesis(sr)) < TOL_CONT
+                assert rel_l2(host(d), P.derivr(sr, 1)) < TOL_DERIV
+                assert rel_l2(host(out), P.forward_3d(P.sh_synthesis(sr))) < TOL_CONT
+
+
+def test_batch_replays():
+    """A second run of the same graph on new inputs gives the new answers."""
+    from redondito_b200 import sphp as S
+    P, xs = _problem_inputs(31, 64, 2, 7)
+    G = S.Plan(31, 64, nlat=P.nlat, nphi=P.nphi, Cz=25, oz=5, precision=S.SPH_MIXED)
+    B = S.Batch([G], [2])
+    for rep in range(2):
+        ys = [x * (rep + 1.5) for x in xs]
+        for f, y in enumerate(ys):
+            B.spec[0][f].copy_(dev(y))
+        torch.cuda.synchronize()
+        B.run()
+        B.status()
+        for f, y in enumerate(ys):
+            ref = P.sh_synthesis(P.z_inverse(y))
+            assert rel_l2(host(B.grid[0][f]), ref) < 1e-6
