@@ -232,6 +232,16 @@ int sph_timer_enable(sph_plan* plan, int on);
 int sph_timer_reset(sph_plan* plan);
 int sph_timer_read(sph_plan* plan, double* ms, int* launches);
 
+/* Tile shapes of a plan (no reference counterpart; chosen per problem size
+ * by redondito_b200/autotune.py).  rows: MMA rows per scalar Legendre work
+ * item of an SPH_MIXED plan (32, 64 or 128; rebuilds its tensor-core tables,
+ * ignored by FP64 plans); ring_pairs: Gauss ring pairs per CTA of the phi
+ * transforms (1, 2, 4, 8, dividing nlat/2, ring_pairs*nphi <= 8192);
+ * z_cols: lm columns per CTA of the z transforms (a power of two <= 64,
+ * z_cols*nz <= 4096).  0 selects the built-in choice.  Results do not
+ * depend on the tile shapes beyond round-off.  Synchronises the device. */
+int sph_plan_set_tiles(sph_plan* plan, int rows, int ring_pairs, int z_cols);
+
 /* Device status of a plan (no reference counterpart: the reference's
  * kernels have no bounded waits).  The tensor-core kernels of an SPH_MIXED
  * plan bound every wait on a shared-memory barrier; one that gives up

@@ -1,0 +1,121 @@
+"""Tile-shape autotuner.
+
+For a problem size (lmax, nz, nlat, nphi, precision) the tuner times the
+candidate tile shapes of sph_plan_set_tiles -- MMA rows per scalar Legendre
+work item (mixed plans), Gauss ring pairs per phi-transform CTA and lm
+columns per z-transform CTA -- on the device, one batch run (3D pair plus
+radial derivative of one field, the C4 work of a problem) per repetition,
+and keeps the fastest.  Results are cached in a JSON table keyed by the
+problem size; the table measured on B200 ships as tiles_b200.json beside
+this module and is what batches use by default.
+
+    python -m redondito_b200.autotune --out redondito_b200/tiles_b200.json
+"""
+import argparse
+import itertools
+import json
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_TABLE = os.path.join(HERE, "tiles_b200.json")
+
+ROWS = (64, 128)
+RING_PAIRS = (2, 4, 8)
+Z_COLS = (16, 32, 64)
+
+# the C4 ensemble: lmax in {63, 127, 255}, nz in {32, 64, 96, 128}, nlat = 3(lmax+1)/2, nphi = 2 nlat
+C4_LMAX = (63, 127, 255)
+C4_NZ = (32, 64, 96, 128)
+
+
+def key(lmax, nz, nlat, nphi, precision):
+    return f"{'mixed' if precision else 'fp64'}/lmax{lmax}/nz{nz}/{nlat}x{nphi}"
+
+
+def load_table(path=DEFAULT_TABLE):
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def save_table(table, path):
+    tmp = path + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(table, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def candidates(lmax, nz, nlat, nphi, precision):
+    """Tile shapes that sph_plan_set_tiles accepts for this size."""
+    rows = ROWS if precision else (0,)
+    pairs = [r for r in RING_PAIRS if (nlat // 2) % r == 0 and r * nphi <= 8192]
+    cols = [c for c in Z_COLS if c * nz <= 4096]
+    return [dict(rows=r, ring_pairs=p, z_cols=c) for r, p, c in itertools.product(rows, pairs, cols)]
+
+
+def best(times):
+    """The candidate with the smallest time: times is a list of (ms, tiles)."""
+    return min(times, key=lambda t: t[0])[1] if times else None
+
+
+def tiles_for(lmax, nz, nlat, nphi, precision, table=None):
+    table = load_table() if table is None else table
+    return table.get(key(lmax, nz, nlat, nphi, precision))
+
+
+def apply(plan, tiles):
+    from redondito_b200 import sphp as S
+    if tiles:
+        S.set_tiles(plan, tiles["rows"], tiles["ring_pairs"], tiles["z_cols"])
+
+
+def time_candidate(S, torch, P, tiles, reps=5):
+    """Device ms of one batch run (3D pair + radial derivative of one field)."""
+    apply(P, tiles)
+    B = S.Batch([P], [1])
+    gen = torch.Generator(device=P.device)
+    gen.manual_seed(1)
+    x = torch.randn((P.nz, P.nlm), generator=gen, device=P.device, dtype=torch.float64)
+    B.spec[0][0].copy_(torch.complex(x, torch.zeros_like(x)))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    B.run()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        B.run()
+    e1.record()
+    torch.cuda.synchronize()
+    B.status()
+    B.close()
+    return e0.elapsed_time(e1) / reps
+
+
+def tune(lmax, nz, nlat, nphi, precision, reps=5):
+    import torch
+    from redondito_b200 import sphp as S
+    P = S.Plan(lmax, nz, nlat=nlat, nphi=nphi, Cz=25, oz=5,
+               precision=S.SPH_MIXED if precision else S.SPH_FP64)
+    times = [(time_candidate(S, torch, P, c, reps), c) for c in candidates(lmax, nz, nlat, nphi, precision)]
+    P.close()
+    t = best(times)
+    return dict(t, ms=min(ms for ms, _ in times)), times
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--out", default=DEFAULT_TABLE)
+    ap.add_argument("--reps", type=int, default=5)
+    a = ap.parse_args()
+    table = load_table(a.out)
+    for precision, lmax, nz in itertools.product((0, 1), C4_LMAX, C4_NZ):
+        nlat = 3 * (lmax + 1) // 2
+        t, times = tune(lmax, nz, nlat, 2 * nlat, precision, a.reps)
+        table[key(lmax, nz, nlat, 2 * nlat, precision)] = t
+        print(key(lmax, nz, nlat, 2 * nlat, precision), t, flush=True)
+    save_table(table, a.out)
+
+
+if __name__ == "__main__":
+    main()

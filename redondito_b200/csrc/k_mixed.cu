@@ -912,22 +912,18 @@ bool mixed_nphi_ok(int nphi) {
   return false;
 }
 
-int mixed_setup(sph_plan* p, const std::vector<double>& hP, const std::vector<double>& hdP,
-                const std::vector<double>& hmPs) {
-  const int lmax = p->lmax, ldn = p->ldn, n2 = p->nlat2;
-  p->ldn8 = (n2 + 7) & ~7;
-  p->G32field = (size_t)(lmax + 1) * 2 * p->nz * p->ldn8;
-  if (p->G32field * sizeof(float2) > p->Gfield * sizeof(double2)) return SPH_EINVAL;
-  const int nkn = (n2 + TK - 1) / TK;  // K tiles over the nodes
-  const int ncb = (p->nz + PLANES - 1) / PLANES;
-  p->nkn = nkn;
+// The tensor-core work sets (items and table blocks) of a mixed plan from
+// its host Legendre tables [nlm][ldn]; scalar and/or vector sets.
+static int build_sets(sph_plan* p, const std::vector<double>& hP, const std::vector<double>& hdP,
+                      const std::vector<double>& hmPs, bool scalar, bool vector) {
+  const int lmax = p->lmax, ldn = p->ldn, n2 = p->nlat2, nkn = p->nkn;
   auto lm = [&](int l, int m) { return (size_t)p->mbase[m] + (l - m); };
   auto rows = [&](int m, int par) { return rows_of(lmax, m, par); };
 
   // analysis: rows = l of one parity, K = nodes (vector: [dP . fold 1-p | mPs . fold p])
   auto ana_items = [&](bool vec) {
     return [&, vec](std::vector<TcItem>& v) {
-      const int NR = vec ? NR_V : NR_S;
+      const int NR = vec ? NR_V : (p->tile_nr ? p->tile_nr : NR_S);
       for (int m = 0; m <= lmax; ++m)
         for (int par = 0; par < 2; ++par) {
           const int L = rows(m, par);
@@ -962,7 +958,7 @@ int mixed_setup(sph_plan* p, const std::vector<double>& hP, const std::vector<do
   // synthesis: rows = nodes, K = l of one parity (vector: [dP . l of 1-q | mPs . l of q])
   auto syn_items = [&](bool vec) {
     return [&, vec](std::vector<TcItem>& v) {
-      const int NR = vec ? NR_V : NR_S;
+      const int NR = vec ? NR_V : (p->tile_nr ? p->tile_nr : NR_S);
       for (int m = 0; m <= lmax; ++m)
         for (int q = 0; q < 2; ++q) {
           for (int i0 = 0; i0 < n2; i0 += NR) {
@@ -1004,10 +1000,24 @@ int mixed_setup(sph_plan* p, const std::vector<double>& hP, const std::vector<do
     };
   };
 
-  int rc = build_set(p->tcAS, ana_items(false), ana_val(false));
-  if (rc == SPH_OK) rc = build_set(p->tcAV, ana_items(true), ana_val(true));
-  if (rc == SPH_OK) rc = build_set(p->tcSS, syn_items(false), syn_val(false));
-  if (rc == SPH_OK) rc = build_set(p->tcSV, syn_items(true), syn_val(true));
+  int rc = SPH_OK;
+  if (scalar) rc = build_set(p->tcAS, ana_items(false), ana_val(false));
+  if (rc == SPH_OK && vector) rc = build_set(p->tcAV, ana_items(true), ana_val(true));
+  if (rc == SPH_OK && scalar) rc = build_set(p->tcSS, syn_items(false), syn_val(false));
+  if (rc == SPH_OK && vector) rc = build_set(p->tcSV, syn_items(true), syn_val(true));
+  return rc;
+}
+
+int mixed_setup(sph_plan* p, const std::vector<double>& hP, const std::vector<double>& hdP,
+                const std::vector<double>& hmPs) {
+  const int lmax = p->lmax, n2 = p->nlat2;
+  p->ldn8 = (n2 + 7) & ~7;
+  p->G32field = (size_t)(lmax + 1) * 2 * p->nz * p->ldn8;
+  if (p->G32field * sizeof(float2) > p->Gfield * sizeof(double2)) return SPH_EINVAL;
+  const int nkn = (n2 + TK - 1) / TK;  // K tiles over the nodes
+  const int ncb = (p->nz + PLANES - 1) / PLANES;
+  p->nkn = nkn;
+  int rc = build_sets(p, hP, hdP, hmPs, true, true);
   // data tiles: analysis [3 fields][m][fold][cb][nkn]; synthesis 2 fields of [m][par][cb][ntiles]
   std::vector<long long> off(2 * (lmax + 1));
   long long nsyn = 0;
@@ -1038,6 +1048,22 @@ int mixed_setup(sph_plan* p, const std::vector<double>& hP, const std::vector<do
                        cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess))
     rc = SPH_ECUDA;
   return rc;
+}
+
+// Rebuilds the scalar work sets with p->tile_nr rows per item, from the
+// Legendre tables read back from the device.
+int mixed_retile(sph_plan* p) {
+  const size_t n = (size_t)p->nlm * p->ldn;
+  std::vector<double> hP(n);
+  SPH_CUDA_OK(cudaDeviceSynchronize());
+  SPH_CUDA_OK(cudaMemcpy(hP.data(), p->P, n * sizeof(double), cudaMemcpyDeviceToHost));
+  for (TcSet* s : {&p->tcAS, &p->tcSS}) {
+    if (s->items) cudaFree(s->items);
+    if (s->blocks) cudaFree(s->blocks);
+    *s = TcSet();
+  }
+  const std::vector<double> none;
+  return build_sets(p, hP, none, none, true, false);
 }
 
 void mixed_free(sph_plan* p) {
@@ -1109,6 +1135,7 @@ int run_tc(const sph_plan* p, const TcSet& set, TcArgs a, cudaStream_t st) {
 }
 
 int phi_pairs(const sph_plan* p) {
+  if (p->tile_np) return p->tile_np;
   for (int np = 8; np > 1; np >>= 1)
     if (p->nlat2 % np == 0 && np * p->nphi <= PMAXC) return np;
   return 1;

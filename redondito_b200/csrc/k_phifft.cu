@@ -246,6 +246,7 @@ __global__ void __launch_bounds__(PTHREADS, 2) phi_inv_kernel(PhiArgs a) {
 // ring pairs per CTA: the largest of 8, 4, 2, 1 that divides nlat/2 and
 // keeps NP*nphi <= PMAXC
 int pairs_per_cta(const sph_plan* p) {
+  if (p->tile_np) return p->tile_np;
   for (int np = 8; np > 1; np >>= 1)
     if (p->nlat2 % np == 0 && np * p->nphi <= PMAXC) return np;
   return 1;

@@ -200,6 +200,7 @@ int launch_zfft(const sph_plan* p, int mode, const double2* in, double2* out, in
   // columns per CTA: a power of two with LB*nz <= ZMAXCOL, at most 64
   int LB = 64;
   while (LB > 1 && LB * p->nz > ZMAXCOL) LB >>= 1;
+  if (p->tile_lb) LB = p->tile_lb;
   if (LB * p->nz > ZMAXCOL) return SPH_EINVAL;
   a.LB = LB;
   int nblocks = (p->nlm + LB - 1) / LB;

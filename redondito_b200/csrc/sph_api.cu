@@ -466,6 +466,23 @@ void timer_stop(const sph_plan* cp, int slot, cudaStream_t st) {
   cudaEventRecord(p->ev_pool[2 * slot + 1], st);
 }
 
+extern "C" int sph_plan_set_tiles(sph_plan* p, int rows, int ring_pairs, int z_cols) {
+  if (!p) return SPH_EINVAL;
+  if (rows != 0 && rows != 32 && rows != 64 && rows != 128) return SPH_EINVAL;
+  if (ring_pairs != 0 && (ring_pairs != 1 && ring_pairs != 2 && ring_pairs != 4 && ring_pairs != 8))
+    return SPH_EINVAL;
+  if (ring_pairs && (p->nlat2 % ring_pairs != 0 || (size_t)ring_pairs * p->nphi > 8192)) return SPH_EINVAL;
+  if (z_cols != 0 && (z_cols < 1 || z_cols > 64 || (z_cols & (z_cols - 1)) || z_cols * p->nz > 4096))
+    return SPH_EINVAL;
+  p->tile_np = ring_pairs;
+  p->tile_lb = z_cols;
+  if (p->precision == SPH_MIXED && rows != p->tile_nr) {
+    p->tile_nr = rows;
+    return mixed_retile(p);
+  }
+  return SPH_OK;
+}
+
 extern "C" int sph_plan_status(sph_plan* p) {
   if (!p) return SPH_EINVAL;
   SPH_CUDA_OK(cudaDeviceSynchronize());

@@ -137,6 +137,10 @@ struct sph_plan {
   mutable const int* sel_kz = nullptr;
   mutable int sel_n = 0;
   mutable int bpass = 0;         // mixed 2D transforms recompute d_bplanes in FP64
+  // tile shapes (0: the built-in choice; sph_plan_set_tiles)
+  int tile_nr = 0;               // mixed scalar items: MMA rows (32, 64, 128)
+  int tile_np = 0;               // phi transforms: ring pairs per CTA (1, 2, 4, 8)
+  int tile_lb = 0;               // z transforms: lm columns per CTA (1..64, power of two)
   double* contg = nullptr;       // [3][Cz][nphi][nlat] physically continued planes (mixed)
   // stage timers (sph_timer_*): event pairs recorded around each launch
   int timing = 0;
@@ -223,6 +227,7 @@ int launch_tc_analysis(const sph_plan* p, int vector, double2* out, double2* out
 int launch_tc_synthesis(const sph_plan* p, int vector, const double2* in, const double2* in2,
                         cudaStream_t st);
 int mixed_status(const sph_plan* p);
+int mixed_retile(sph_plan* p);  // rebuild the scalar work sets for tile_nr
 bool mixed_nphi_ok(int nphi);  // phi lengths the fp32 phi kernels are built for
 
 // grouped launches over several plans' work sets (batches): one job per

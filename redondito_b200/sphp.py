@@ -47,6 +47,7 @@ SYMBOLS = (
     "sph_timer_enable", "sph_timer_reset", "sph_timer_read",
     "sph_derivr_noalloc", "sph_plan_status", "sph_fftp3d_vec_to_qst", "sph_fftp3d_qst_to_vec",
     "sph_batch_create", "sph_batch_run", "sph_batch_status", "sph_batch_destroy",
+    "sph_plan_set_tiles",
 )
 TIMER_CLASSES = ("phi_fwd", "phi_inv", "leg_analysis", "leg_synthesis", "vec_analysis",
                  "vec_synthesis", "zfft", "ops")
@@ -115,6 +116,7 @@ def lib(build_if_missing=True):
             "sph_batch_run": [P, Vp],
             "sph_batch_status": [P],
             "sph_batch_destroy": [P],
+            "sph_plan_set_tiles": [P, I, I, I],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -379,6 +381,12 @@ def timer_reset(plan):
     _call("sph_timer_reset", plan.h)
 
 
+def set_tiles(plan, rows=0, ring_pairs=0, z_cols=0):
+    """Tile shapes of the plan's kernels (0: built-in choice); see sph_plan_set_tiles."""
+    _call("sph_plan_set_tiles", plan.h, int(rows), int(ring_pairs), int(z_cols))
+    plan.tiles = {"rows": int(rows), "ring_pairs": int(ring_pairs), "z_cols": int(z_cols)}
+
+
 def plan_status(plan):
     """Raises SphError(SPH_ETIMEDOUT) if a bounded device wait of the plan's
     tensor-core kernels gave up since the last check."""
@@ -400,8 +408,14 @@ class Batch:
     place), `dspec` = derivr(spec, 1, 'r'), and the forward 3D transform of
     `grid` back into `spec`; one CUDA graph, grouped Legendre launches."""
 
-    def __init__(self, plans, nfields):
+    def __init__(self, plans, nfields, tuned=True):
         self.plans = list(plans)
+        if tuned:  # tile shapes from the autotuner's table, where it has the size
+            from redondito_b200 import autotune
+            table = autotune.load_table()
+            for P in self.plans:
+                autotune.apply(P, autotune.tiles_for(P.lmax, P.nz, P.nlat, P.nphi,
+                                                     P.precision == SPH_MIXED, table))
         self.nfields = [int(n) for n in nfields]
         self.spec, self.grid, self.dspec = [], [], []
         for P, n in zip(self.plans, self.nfields):

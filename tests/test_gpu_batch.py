@@ -92,3 +92,33 @@ def test_batch_replays():
         for f, y in enumerate(ys):
             ref = P.sh_synthesis(P.z_inverse(y))
             assert rel_l2(host(B.grid[0][f]), ref) < 1e-6
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_tile_shapes_do_not_change_results(precision):
+    from redondito_b200 import sphp as S
+    prec = S.SPH_FP64 if precision == "fp64" else S.SPH_MIXED
+    P, xs = _problem_inputs(63, 96, 1, 11)
+    G = S.Plan(63, 96, nlat=P.nlat, nphi=P.nphi, Cz=25, oz=5, precision=prec)
+
+    def run():
+        s = dev(xs[0])
+        g = G.new_grid()
+        out = G.new_spec()
+        S.fftp3d_complex_to_real(G, s, g)
+        S.fftp3d_real_to_complex(G, g, out)
+        return host(g), host(out)
+
+    g0, o0 = run()
+    S.set_tiles(G, 64 if prec else 0, 2, 16)
+    g1, o1 = run()
+    S.set_tiles(G, 32 if prec else 0, 4, 32)
+    g2, o2 = run()
+    tol = 1e-13 if precision == "fp64" else 1e-9
+    for g, o in ((g1, o1), (g2, o2)):
+        assert rel_l2(g, g0) < tol
+        assert rel_l2(o, o0) < tol
+    with pytest.raises(S.SphError):
+        S.set_tiles(G, 48, 0, 0)
+    with pytest.raises(S.SphError):
+        S.set_tiles(G, 0, 3, 0)
