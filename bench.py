@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="mixed only: skip the FP64 comparison")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-c4", action="store_true", help="skip the 64-problem batched ensemble")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop measurement")
     ap.add_argument("--case", default="c3", choices=sorted(CASES),
                     help="c3: the benchmark workload; small, angular: profiling cases for ncu")
     a = ap.parse_args()
@@ -249,6 +251,84 @@ def algorithmic_work(P, mixed):
     }
 
 
+def c4_ensemble(seed=20261203 + 4, nprob=64):
+    """64 independent problems: lmax ~ U{63,127,255}, nz ~ U{32,64,96,128},
+    nlat = 3(lmax+1)/2, nphi = 2 nlat, 1-3 fields, FC-Gram C=25 d=5, r in [0.35, 1]."""
+    rng = np.random.default_rng(seed)
+    return [(int(rng.choice((63, 127, 255))), int(rng.choice((32, 64, 96, 128))), int(rng.integers(1, 4)))
+            for _ in range(nprob)]
+
+
+def batched_c4(S, torch, steps, warmup):
+    """The C4 ensemble as one batch (3D pair + radial derivative per field, one
+    CUDA graph, grouped Legendre launches, autotuned tiles), FP64 and mixed."""
+    ens = c4_ensemble()
+    nfield = sum(nf for _, _, nf in ens)
+    out = {"problems": len(ens), "fields": nfield,
+           "work": "per field: 3D inverse + radial derivative + 3D forward (one batch run)"}
+    for name, prec in (("fp64", S.SPH_FP64), ("mixed", S.SPH_MIXED)):
+        plans = [S.Plan(l, nz, nlat=3 * (l + 1) // 2, nphi=3 * (l + 1), Cz=25, oz=5, rint=0.35, rext=1.0,
+                        precision=prec) for l, nz, _ in ens]
+        B = S.Batch(plans, [nf for _, _, nf in ens])
+        gen = torch.Generator(device=plans[0].device)
+        gen.manual_seed(20261203 + 4)
+        states = []
+        for P, xs in zip(plans, B.spec):
+            amp = (P.ell.to(P.device).double() + 1.0) ** -2.0
+            for x in xs:
+                re = torch.randn((P.nz, P.nlm), generator=gen, device=P.device, dtype=torch.float64)
+                im = torch.randn((P.nz, P.nlm), generator=gen, device=P.device, dtype=torch.float64)
+                v = torch.complex(re * amp, im * amp)
+                v[:, P.emm.to(P.device) == 0] = v[:, P.emm.to(P.device) == 0].real.to(torch.complex128)
+                x.copy_(v)
+                S.fftp1d_real_to_complex_z(P, x)
+                states.append(x.clone())
+        for _ in range(warmup):
+            B.run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            B.run()
+        e1.record()
+        torch.cuda.synchronize()
+        B.status()
+        ms = e0.elapsed_time(e1) / steps
+        rt = max(float((torch.linalg.vector_norm(x - r) / torch.linalg.vector_norm(r)).item())
+                 for x, r in zip((x for xs in B.spec for x in xs), states))
+        out[name] = {"ms_per_run": ms, "field_pairs_per_s": nfield / (ms * 1e-3),
+                     "max_roundtrip_rel_l2": rt}
+        B.close()
+        for P in plans:
+            P.close()
+        del states
+        torch.cuda.empty_cache()
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["ms_per_run"] / out["mixed"]["ms_per_run"]
+    return out
+
+
+def serving_c5(S, torch, nreq=200, rate=500.0):
+    """C5: Poisson arrivals (mean 500/s, seeded), sizes lmax 31/63/127/255/511
+    weighted 8:4:2:1:1, half transform pairs, half k ~ U[1,10] RK3 steps;
+    continuous admission into pre-created slots; latency p50/p99 and jobs/s,
+    mixed and FP64."""
+    from redondito_b200 import serve
+    slots = {31: 4, 63: 4, 127: 2, 255: 2, 511: 1}
+    out = {"requests": nreq, "arrival_rate_per_s": rate, "slots": {str(k): v for k, v in slots.items()},
+           "sizes": {str(l): list(serve.size_of(l)[1:]) for l in slots}}
+    for name, prec in (("mixed", S.SPH_MIXED), ("fp64", S.SPH_FP64)):
+        srv = serve.Server(S, torch, prec, slots, hbm_budget=120e9)
+        warm = [serve.Request(i, 0.0, l, k, 1) for i, (l, k) in
+                enumerate((l, k) for l in slots for k in ("pair", "rk3"))]
+        srv.serve(warm)
+        reqs = serve.poisson_mix(nreq, rate, seed=20261203 + 5)
+        srv.serve(reqs)
+        out[name] = dict(serve.latency_stats(reqs), hbm_gb=srv.bytes / 1e9)
+        srv.close()
+        torch.cuda.empty_cache()
+    return out
+
+
 def time_pairs(S, P, st, grids, steps, stream, torch, dist, world):
     """Device time of `steps` pairs (barrier + sync on both sides, max over ranks)."""
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -429,6 +509,18 @@ def main():
     shares = {c: round(stage[c][0] / max(ms, 1e-9), 4) for c in stage if stage[c][1]}
     launches = sum(v[1] for v in stage.values())
 
+    c4 = None
+    if not args.no_c4 and args.case == "c3":
+        del grids
+        torch.cuda.empty_cache()
+        c4 = batched_c4(S, torch, args.steps, args.warmup)
+
+    c5 = None
+    if not args.no_serve and args.case == "c3":
+        P.close()
+        torch.cuda.empty_cache()
+        c5 = serving_c5(S, torch)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, cores, sample = cpu_pairs_per_s()
@@ -456,6 +548,9 @@ def main():
         "fp64": fp64,
         "speedup_vs_fp64": (value / fp64["value"]) if fp64 else None,
         "accuracy": errors,
+        "batched_c4": c4,
+        "serve_c5": c5,
+        "serve_p99_ms": c5["mixed"]["p99_ms"] if c5 else None,
         "roundtrip_rel_l2": {"scalar": rt[0], "Q": rt[1], "S": rt[2], "T": rt[3]},
         "clocks": clocks,
         "cpu_baseline": cpu,
