@@ -259,21 +259,34 @@ def c4_ensemble(seed=20261203 + 4, nprob=64):
             for _ in range(nprob)]
 
 
-def batched_c4(S, torch, steps, warmup):
-    """The C4 ensemble as one batch (3D pair + radial derivative per field, one
-    CUDA graph, grouped Legendre launches, autotuned tiles), FP64 and mixed."""
+def _max_over_ranks(torch, dist, world, x):
+    if world > 1:
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        x = float(t.item())
+    return x
+
+
+def batched_c4(S, torch, steps, warmup, rank=0, world=1, dist=None):
+    """The C4 ensemble as one batch per GPU (3D pair + radial derivative per
+    field, one CUDA graph, grouped Legendre launches, autotuned tiles), FP64
+    and mixed.  With several ranks each runs the problems the greedy-by-flops
+    partition gives it; the run time is the max over ranks."""
+    from redondito_b200 import shard
     ens = c4_ensemble()
+    mine = shard.ensemble_share(ens, rank, world)
     nfield = sum(nf for _, _, nf in ens)
     out = {"problems": len(ens), "fields": nfield,
-           "work": "per field: 3D inverse + radial derivative + 3D forward (one batch run)"}
+           "work": "per field: 3D inverse + radial derivative + 3D forward (one batch run)",
+           "partition": "greedy by flops" if world > 1 else "one GPU"}
     for name, prec in (("fp64", S.SPH_FP64), ("mixed", S.SPH_MIXED)):
-        plans = [S.Plan(l, nz, nlat=3 * (l + 1) // 2, nphi=3 * (l + 1), Cz=25, oz=5, rint=0.35, rext=1.0,
-                        precision=prec) for l, nz, _ in ens]
-        B = S.Batch(plans, [nf for _, _, nf in ens])
-        gen = torch.Generator(device=plans[0].device)
-        gen.manual_seed(20261203 + 4)
+        plans = [S.Plan(ens[i][0], ens[i][1], nlat=3 * (ens[i][0] + 1) // 2, nphi=3 * (ens[i][0] + 1), Cz=25,
+                        oz=5, rint=0.35, rext=1.0, precision=prec) for i in mine]
+        B = S.Batch(plans, [ens[i][2] for i in mine]) if plans else None
         states = []
-        for P, xs in zip(plans, B.spec):
+        for i, P, xs in zip(mine, plans, B.spec if B else []):
+            gen = torch.Generator(device=P.device)
+            gen.manual_seed(20261203 + 4 + 7919 * i)
             amp = (P.ell.to(P.device).double() + 1.0) ** -2.0
             for x in xs:
                 re = torch.randn((P.nz, P.nlm), generator=gen, device=P.device, dtype=torch.float64)
@@ -283,22 +296,28 @@ def batched_c4(S, torch, steps, warmup):
                 x.copy_(v)
                 S.fftp1d_real_to_complex_z(P, x)
                 states.append(x.clone())
-        for _ in range(warmup):
+        for _ in range(warmup if B else 0):
             B.run()
         torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(steps):
+        for _ in range(steps if B else 0):
             B.run()
         e1.record()
         torch.cuda.synchronize()
-        B.status()
         ms = e0.elapsed_time(e1) / steps
-        rt = max(float((torch.linalg.vector_norm(x - r) / torch.linalg.vector_norm(r)).item())
-                 for x, r in zip((x for xs in B.spec for x in xs), states))
+        rt = 0.0
+        if B:
+            B.status()
+            rt = max(float((torch.linalg.vector_norm(x - r) / torch.linalg.vector_norm(r)).item())
+                     for x, r in zip((x for xs in B.spec for x in xs), states))
+            B.close()
+        ms = _max_over_ranks(torch, dist, world, ms)
+        rt = _max_over_ranks(torch, dist, world, rt)
         out[name] = {"ms_per_run": ms, "field_pairs_per_s": nfield / (ms * 1e-3),
                      "max_roundtrip_rel_l2": rt}
-        B.close()
         for P in plans:
             P.close()
         del states
@@ -307,23 +326,37 @@ def batched_c4(S, torch, steps, warmup):
     return out
 
 
-def serving_c5(S, torch, nreq=200, rate=500.0):
+def serving_c5(S, torch, nreq=200, rate=500.0, rank=0, world=1, dist=None):
     """C5: Poisson arrivals (mean 500/s, seeded), sizes lmax 31/63/127/255/511
     weighted 8:4:2:1:1, half transform pairs, half k ~ U[1,10] RK3 steps;
     continuous admission into pre-created slots; latency p50/p99 and jobs/s,
-    mixed and FP64."""
-    from redondito_b200 import serve
+    mixed and FP64.  With several ranks the stream is dispatched online to
+    the least-loaded rank (by flops) and each rank runs its own server;
+    latencies are pooled and the span is the longest over ranks."""
+    from redondito_b200 import serve, shard
     slots = {31: 4, 63: 4, 127: 2, 255: 2, 511: 1}
     out = {"requests": nreq, "arrival_rate_per_s": rate, "slots": {str(k): v for k, v in slots.items()},
-           "sizes": {str(l): list(serve.size_of(l)[1:]) for l in slots}}
+           "sizes": {str(l): list(serve.size_of(l)[1:]) for l in slots},
+           "dispatch": "online least-loaded by flops" if world > 1 else "one GPU"}
     for name, prec in (("mixed", S.SPH_MIXED), ("fp64", S.SPH_FP64)):
         srv = serve.Server(S, torch, prec, slots, hbm_budget=120e9)
         warm = [serve.Request(i, 0.0, l, k, 1) for i, (l, k) in
                 enumerate((l, k) for l in slots for k in ("pair", "rk3"))]
         srv.serve(warm)
         reqs = serve.poisson_mix(nreq, rate, seed=20261203 + 5)
-        srv.serve(reqs)
-        out[name] = dict(serve.latency_stats(reqs), hbm_gb=srv.bytes / 1e9)
+        share = shard.stream_share(reqs, rank, world, serve.size_of)
+        if world > 1:
+            dist.barrier()
+        srv.serve(share)
+        lat = [(r.arrival, r.t_done) for r in share]
+        if world > 1:
+            allr = [None] * world
+            dist.all_gather_object(allr, lat)
+            lat = [x for r in allr for x in r]
+        pooled = [serve.Request(i, a, 0, "pair") for i, (a, _) in enumerate(lat)]
+        for r, (_, d) in zip(pooled, lat):
+            r.t_done = d
+        out[name] = dict(serve.latency_stats(pooled), hbm_gb_per_gpu=srv.bytes / 1e9)
         srv.close()
         torch.cuda.empty_cache()
     return out
@@ -513,13 +546,13 @@ def main():
     if not args.no_c4 and args.case == "c3":
         del grids
         torch.cuda.empty_cache()
-        c4 = batched_c4(S, torch, args.steps, args.warmup)
+        c4 = batched_c4(S, torch, args.steps, args.warmup, rank, world, dist)
 
     c5 = None
     if not args.no_serve and args.case == "c3":
         P.close()
         torch.cuda.empty_cache()
-        c5 = serving_c5(S, torch)
+        c5 = serving_c5(S, torch, rank=rank, world=world, dist=dist)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
