@@ -27,13 +27,16 @@
 // Warp roles of the tensor-core kernel: 0 bulk copies (one lane), 1 TMEM
 // allocation and MMA issue (one lane), 2-5 epilogue (TMEM lane quarters
 // 2, 3, 0, 1).
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <thread>
 
+#include "fft3.cuh"
 #include "fft_ct.cuh"
 #include "tc05.cuh"
 
@@ -480,6 +483,7 @@ struct Phi32Args {
   const float2* tw1;  // four-step kernels: pass twiddles of length N1 and N2,
   const float2* tw2;  // and W_N^e = exp(-2 pi i e / N)
   const float2* twN;
+  int* flag;  // set when a bounded wait gives up (three-step forward)
 };
 
 // Four-step phi FFT geometry (N = N1 N2, NP ring pairs per CTA).  Shared
@@ -749,6 +753,456 @@ __global__ void __launch_bounds__(PTHREADS, 2) phi_inv32(Phi32Args a) {
   for (int j = j0; j < N; j += JSTEP) plane[(size_t)j * nlat + ring] = (double)smf[2 * g.addr(b, j) + half];
 }
 
+// ---------------------------------------------------------------- three-step phi FFTs
+// Persistent kernels over tiles of NP ring pairs of one (plane, field).  The
+// input of the tile after the current one is copied into shared memory while
+// the current one is transformed -- TMA boxes of the grid for the forward
+// transform (2 N / BR requests of NP x BR values instead of N NP / 2 16-byte
+// copies, which the load path cannot keep in flight), cp.async for the
+// inverse's folded coefficients -- so no registers are held by loads in flight.
+//
+// N = A M, M = B C (A = 16, B the power-of-two part of M up to 16, C the
+// rest).  Forward: (A) A-point DFTs of the stride-M subsequences
+// x[nm + M n1], the twiddle W_N^(nm ka), stored as row ka, column nm;
+// (B) B-point DFTs of each row over its stride-C subsequences c + C nb,
+// the twiddle W_M^(c kb), stored back at c + C kb; (C) C-point DFTs of the
+// runs C kb .. C kb + C-1, stored back in place.  Frequency ka + A (kb + B kc)
+// then sits in row ka, column C kb + kc.  The inverse runs the same steps
+// backwards with conjugate twiddles.  The row pitch PR is odd and the
+// ring-pair stride SB = 16/NP (mod 16), so the lanes of every half warp
+// (NP ring pairs x 16/NP rows or columns) hit distinct banks in each step.
+template <int N, int NP>
+struct P3 {
+  static constexpr int A = 16, M = N / A, B = ct::pow2_part_cap16(M), C = M / B;
+  static constexpr int ITEMS_A = NP * M, ITEMS_B = NP * A * C, ITEMS_C = NP * A * B;
+  static constexpr int THREADS = ITEMS_A <= 64 ? 64 : (ITEMS_A + 31) / 32 * 32;
+  static constexpr int PR = M | 1;
+  static constexpr int SB = up_mod16(A * PR, 16 / NP);
+  static constexpr size_t XBYTES = (size_t)NP * SB * sizeof(float2);      // transform area
+  static constexpr size_t STAGE_F = (size_t)N * 2 * NP * sizeof(double);  // one forward tile, fp64
+  static constexpr size_t SMEM_F = 2 * STAGE_F + (size_t)N * sizeof(float2) + 2 * sizeof(uint64_t);
+  // two CTAs per SM where two forward tiles fit (registers bounded to match)
+  static constexpr int MINB = SMEM_F <= 110 * 1024 && THREADS <= 512 ? 2 : 1;
+  static_assert(N % A == 0 && NP >= 2 && NP <= 16 && XBYTES % 16 == 0, "three-step geometry");
+  // single-pass kernels: the transform area overlays one staged tile, one step-A item per thread
+  static constexpr bool ONE_PASS = XBYTES <= STAGE_F && ITEMS_A <= THREADS && THREADS <= 1024;
+  // inverse: transform area, twiddles, two staged coefficient tiles of (lmax + 1) x 2 x NP float2
+  __host__ __device__ static size_t smem_inv(int lmax) { return XBYTES + (size_t)N * sizeof(float2) + 2 * stage_inv(lmax) * sizeof(float2); }
+  __host__ __device__ static int stage_inv(int lmax) { return (lmax + 1) * 2 * NP; }
+};
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// staged rows of 2 NP values (rings | mirrors, or parity 0 | parity 1) swap
+// their halves every 8/NP rows, so that 16/NP consecutive rows read by a
+// half warp fall in distinct banks
+template <int NP>
+__device__ __forceinline__ int stage_swz(int row) {
+  return ((row * NP) >> 3) & 1;
+}
+
+__device__ __forceinline__ float2 conj2(float2 z) { return make_float2(z.x, -z.y); }
+
+// TMA views of the forward input: per field, the planes below ksplit (lo)
+// and the continued planes from ksplit on (hi), each a 2D fp64 array of
+// nlat columns (rings) and N x planes rows (phi samples); box NP x BR.
+struct Phi3Maps {
+  CUtensorMap lo[SPH_MAX_FIELDS], hi[SPH_MAX_FIELDS];
+};
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+      "[%4];\n" ::"r"(tc05::smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(tc05::smem_u32(mbar))
+      : "memory");
+}
+
+template <int N>
+__host__ __device__ constexpr int phi3_box_rows() {
+  return N <= 256 ? N : (N % 256 == 0 ? 256 : 192);
+}
+
+template <int N, int NP>
+__global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB)
+    phi3_fwd32(Phi32Args a, int ntiles, const __grid_constant__ Phi3Maps maps) {
+  using G = P3<N, NP>;
+  constexpr int A = G::A, M = G::M, B = G::B, C = G::C, T = G::THREADS, BR = phi3_box_rows<N>();
+  static_assert(N % BR == 0 && G::ONE_PASS, "box rows, single-pass geometry");
+  // [stage 0 | stage 1 | twiddles | 2 mbarriers]; a stage is [ring rows | mirror rows], rows of NP values
+  extern __shared__ __align__(1024) unsigned char sm3[];
+  float2* tw = reinterpret_cast<float2*>(sm3 + 2 * G::STAGE_F);
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm3 + 2 * G::STAGE_F + (size_t)N * sizeof(float2));
+  const int t = threadIdx.x;
+  const int nlat = a.nlat, ngroups = nlat / 2 / NP;
+  for (int i = t; i < N; i += T) tw[i] = __ldg(a.twN + i);
+  if (t == 0) {
+    tc05::mbar_init(&full[0], 1);
+    tc05::mbar_init(&full[1], 1);
+    tc05::mbar_fence_init();
+  }
+  __syncthreads();
+  auto stage = [&](int which) { return reinterpret_cast<double*>(sm3 + which * G::STAGE_F); };
+  // one thread: the 2 N / BR boxes of a tile (its NP rings and their NP mirrors, all N samples)
+  auto issue = [&](int tile, int which) {
+    const int g = tile % ngroups, r = tile / ngroups, k = r % a.nz, f = r / a.nz;
+    const bool lo = k < a.ksplit;
+    const CUtensorMap* map = lo ? &maps.lo[f] : &maps.hi[f];
+    const int y0 = (lo ? k : k - a.ksplit) * N;
+    double* st = stage(which);
+    mbar_arrive_tx(&full[which], (uint32_t)(2 * N * NP * sizeof(double)));
+#pragma unroll 1
+    for (int i = 0; i < N / BR; ++i) {
+      tma_load_2d(st + (size_t)i * BR * NP, map, g * NP, y0 + i * BR, &full[which]);
+      tma_load_2d(st + (size_t)(N + i * BR) * NP, map, nlat - g * NP - NP, y0 + i * BR, &full[which]);
+    }
+  };
+  if (t == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+  int s = 0;
+  uint32_t phase = 0;  // bit s: parity of the next completion of stage s
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, s ^= 1) {
+    const bool ok = tc05::mbar_wait(&full[s], (phase >> s) & 1);
+    if (__syncthreads_or(!ok)) {  // the tile never arrived: report, let the copies land, stop
+      if (t == 0) {
+        atomicExch(a.flag, 1);
+        tc05::mbar_wait(&full[s], (phase >> s) & 1);
+      }
+      return;
+    }
+    phase ^= 1u << s;
+    if (t == 0 && tile + (int)gridDim.x < ntiles) {
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      issue(tile + gridDim.x, s ^ 1);
+    }
+    const int g = tile % ngroups, r = tile / ngroups, k = r % a.nz, f = r / a.nz, p0 = g * NP;
+    const double* ring = stage(s);
+    const double* mir = ring + (size_t)N * NP;
+    float2* X = reinterpret_cast<float2*>(stage(s));
+    // (A) the samples x[nm + M n1] of ring pair bA (ring: real part, mirror: imaginary part)
+    const bool act = t < G::ITEMS_A;
+    const int bA = t % NP, nm = t / NP;
+    float2 v[A];
+    if (act) {
+#pragma unroll
+      for (int n1 = 0; n1 < A; ++n1) {
+        const int j = nm + M * n1;
+        v[n1] = make_float2((float)ring[j * NP + bA], (float)mir[j * NP + (NP - 1 - bA)]);
+      }
+    }
+    __syncthreads();  // the transform area overlays the staged samples
+    if (act) {
+      ct::RD<float2, A, -1>::run(v);
+      float2* xo = X + bA * G::SB + nm;
+#pragma unroll
+      for (int ka = 0; ka < A; ++ka) xo[ka * G::PR] = ka ? ct::mul(v[ka], tw[nm * ka]) : v[ka];
+    }
+    __syncthreads();
+    if constexpr (B > 1) {  // (B)
+      for (int it = t; it < G::ITEMS_B; it += T) {
+        const int ka = it % A, rr = it / A, c = rr % C, b = rr / C;
+        float2* row = X + b * G::SB + ka * G::PR + c;
+        float2 w[B];
+#pragma unroll
+        for (int nb = 0; nb < B; ++nb) w[nb] = row[C * nb];
+        ct::RD<float2, B, -1>::run(w);
+#pragma unroll
+        for (int kb = 0; kb < B; ++kb) row[C * kb] = (kb && c) ? ct::mul(w[kb], tw[A * c * kb]) : w[kb];
+      }
+      __syncthreads();
+    }
+    if constexpr (C > 1) {  // (C)
+      for (int it = t; it < G::ITEMS_C; it += T) {
+        const int ka = it % A, rr = it / A, kb = rr % B, b = rr / B;
+        float2* row = X + b * G::SB + ka * G::PR + C * kb;
+        float2 u[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) u[c] = row[c];
+        ct::RD<float2, C, -1>::run(u);
+#pragma unroll
+        for (int kc = 0; kc < C; ++kc) row[kc] = u[kc];
+      }
+      __syncthreads();
+    }
+    // fold both parities of the NP ring pairs from Z(m), Z(-m), weight, split, write tile rows
+    float W[NP];
+#pragma unroll
+    for (int b = 0; b < NP; ++b) W[b] = (float)__ldg(a.wfold + p0 + b);
+    const int cb = k / PLANES, row = 2 * (k % PLANES), kt = p0 / TK, kk0 = p0 % TK;
+    auto zpos = [&](int m) {
+      const int q = m / A;
+      return (m % A) * G::PR + C * (q % B) + q / B;
+    };
+    for (int m = t; m <= a.lmax; m += T) {
+      const int pz = zpos(m), pc = zpos(m == 0 ? 0 : N - m);
+      float er[NP], ei[NP], orr[NP], oi[NP];
+#pragma unroll
+      for (int b = 0; b < NP; ++b) {
+        const float2 Z = X[b * G::SB + pz], Zc = X[b * G::SB + pc];
+        // F(ring) = (Z + conj Z(-m))/2, F(mirror) = -i (Z - conj Z(-m))/2
+        const float fir = 0.5f * (Z.x + Zc.x), fii = 0.5f * (Z.y - Zc.y);
+        const float fmr = 0.5f * (Z.y + Zc.y), fmi = -0.5f * (Z.x - Zc.x);
+        er[b] = (fir + fmr) * W[b];
+        ei[b] = (fii + fmi) * W[b];
+        orr[b] = (fir - fmr) * W[b];
+        oi[b] = (fii - fmi) * W[b];
+      }
+      __nv_bfloat16* t0 = a.tiles + ana_tile(a.lmax, a.ncb, a.nkn, f, m, 0, cb, kt) * TILE_HALVES;
+      __nv_bfloat16* t1 = a.tiles + ana_tile(a.lmax, a.ncb, a.nkn, f, m, 1, cb, kt) * TILE_HALVES;
+      store_tile_row<NP>(t0, row, kk0, er);
+      store_tile_row<NP>(t0, row + 1, kk0, ei);
+      store_tile_row<NP>(t1, row, kk0, orr);
+      store_tile_row<NP>(t1, row + 1, kk0, oi);
+    }
+    // this stage is refilled by TMA (async proxy) after the next barrier
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  }
+}
+
+template <int N, int NP>
+__global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB) phi3_inv32(Phi32Args a, int ntiles) {
+  using G = P3<N, NP>;
+  constexpr int A = G::A, M = G::M, B = G::B, C = G::C, T = G::THREADS;
+  static_assert(G::ONE_PASS, "single-pass geometry");
+  extern __shared__ __align__(1024) unsigned char sm3i[];
+  float2* X = reinterpret_cast<float2*>(sm3i);
+  float2* tw = reinterpret_cast<float2*>(sm3i + G::XBYTES);
+  const int lmax = a.lmax, nlat = a.nlat, ngroups = nlat / 2 / NP;
+  const int sf2 = G::stage_inv(lmax);
+  float2* stg = tw + N;
+  const int t = threadIdx.x;
+  for (int i = t; i < N; i += T) tw[i] = __ldg(a.twN + i);
+  const size_t pstride = (size_t)a.nz * a.ldn8;  // parity stride of the folded coefficients
+  auto issue = [&](int tile, float2* st) {
+    const int g = tile % ngroups, r = tile / ngroups, k = r % a.nz, f = r / a.nz;
+    const float2* gs = a.G32c + (size_t)f * a.G32field + (size_t)k * a.ldn8 + g * NP;
+    constexpr int GR = NP / 2;
+    const int total = (lmax + 1) * 2 * GR;
+    for (int q = t; q < total; q += T) {
+      const int gg = q % GR, rr = q / GR, par = rr & 1, mm = rr >> 1;
+      cp_async16(st + mm * 2 * NP + (par ^ stage_swz<NP>(mm)) * NP + 2 * gg, gs + (size_t)rr * pstride + 2 * gg);
+    }
+    cp_async_commit();
+  };
+  if ((int)blockIdx.x < ntiles) issue(blockIdx.x, stg);
+  int s = 0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, s ^= 1) {
+    cp_async_wait_all();
+    __syncthreads();
+    if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x, stg + (s ^ 1) * sf2);
+    const int g = tile % ngroups, r = tile / ngroups, k = r % a.nz, f = r / a.nz, p0 = g * NP;
+    const float2* st = stg + s * sf2;
+    // Z(m) of ring pair b (x = ring + i mirror) from the folded coefficients of both parities
+    auto zin = [&](int m, int b) {
+      const bool lo = m <= lmax, hi = N - m <= lmax;
+      if (!lo && !hi) return make_float2(0.f, 0.f);
+      const int mm = lo ? m : N - m;
+      const int sw = stage_swz<NP>(mm);
+      const float2 se = st[mm * 2 * NP + sw * NP + b], so = st[mm * 2 * NP + (1 - sw) * NP + b];
+      const float2 Fi = make_float2(se.x + so.x, se.y + so.y), Fm = make_float2(se.x - so.x, se.y - so.y);
+      if (m == 0) return make_float2(Fi.x, Fm.x);
+      if (lo) return make_float2(Fi.x - Fm.y, Fi.y + Fm.x);
+      return make_float2(Fi.x + Fm.y, -Fi.y + Fm.x);
+    };
+    // (C') C-point inverse DFTs over kc of Z(ka + A (kb + B kc)), the twiddle W_M^-(c kb)
+    for (int it = t; it < G::ITEMS_C; it += T) {
+      const int b = it % NP, rr = it / NP, ka = rr % A, kb = rr / A;
+      float2 u[C];
+#pragma unroll
+      for (int kc = 0; kc < C; ++kc) u[kc] = zin(ka + A * (kb + B * kc), b);
+      ct::RD<float2, C, 1>::run(u);
+      float2* row = X + b * G::SB + ka * G::PR + C * kb;
+#pragma unroll
+      for (int c = 0; c < C; ++c) row[c] = (c && kb) ? ct::mul(u[c], conj2(tw[A * c * kb])) : u[c];
+    }
+    __syncthreads();
+    if constexpr (B > 1) {  // (B') B-point inverse DFTs over kb, stored at column c + C nb
+      for (int it = t; it < G::ITEMS_B; it += T) {
+        const int ka = it % A, rr = it / A, c = rr % C, b = rr / C;
+        float2* row = X + b * G::SB + ka * G::PR + c;
+        float2 w[B];
+#pragma unroll
+        for (int kb = 0; kb < B; ++kb) w[kb] = row[C * kb];
+        ct::RD<float2, B, 1>::run(w);
+#pragma unroll
+        for (int nb = 0; nb < B; ++nb) row[C * nb] = w[nb];
+      }
+      __syncthreads();
+    }
+    // (A') the twiddle W_N^-(nm ka), A-point inverse DFTs over ka, grid stores
+    if (t < G::ITEMS_A) {
+      const int b = t % NP, nm = t / NP;
+      float2 v[A];
+      const float2* xi = X + b * G::SB + nm;
+#pragma unroll
+      for (int ka = 0; ka < A; ++ka) v[ka] = ka ? ct::mul(xi[ka * G::PR], conj2(tw[nm * ka])) : xi[0];
+      ct::RD<float2, A, 1>::run(v);
+      double* plane = a.gout[f] + (size_t)k * N * nlat;
+      double* pr = plane + p0 + b;
+      double* pm = plane + (nlat - 1 - p0 - b);
+#pragma unroll
+      for (int n1 = 0; n1 < A; ++n1) {
+        const size_t j = (size_t)(nm + M * n1) * nlat;
+        pr[j] = (double)v[n1].x;
+        pm[j] = (double)v[n1].y;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- two-pass forward phi FFT
+// For lengths whose tile of 8 ring pairs does not fit shared memory twice,
+// the forward transform runs in two passes, so that every HBM request is a
+// full line: pass 1 reads whole grid rows (PB consecutive ring pairs per
+// warp: 128-byte runs of rings and of mirrors) and does step (A) of the
+// three-step transform for all ring pairs; it writes, through shared memory,
+// each tile's transform area exactly as the single-pass kernel lays it out
+// in shared memory ([b][ka][nm], pitches PR and SB), one contiguous image per
+// (plane, tile).  Pass 2 bulk-copies an image into shared memory (double
+// buffered) and finishes steps (B), (C), the fold and the tile rows.
+constexpr int PHI2_PB = 16, PHI2_NMC = 16, PHI2_NP = 8, PHI2_BATCH = 64;
+
+template <int N>
+__global__ void __launch_bounds__(PHI2_PB* PHI2_NMC, 2) phi2a_fwd32(Phi32Args a, float2* img, int q0) {
+  using G = P3<N, PHI2_NP>;
+  constexpr int A = G::A, M = G::M, PB = PHI2_PB, NMC = PHI2_NMC, SPB = A * NMC + 1;
+  static_assert(M % NMC == 0, "nm chunks");
+  __shared__ float2 S[PB * SPB];
+  const int t = threadIdx.x, b = t % PB, nmi = t / PB;
+  const int nlat = a.nlat, pair = blockIdx.x * PB + b, nm0 = blockIdx.y * NMC, nm = nm0 + nmi;
+  const int q = q0 + blockIdx.z, k = q % a.nz, f = q / a.nz;
+  const double* pl =
+      k < a.ksplit ? a.gin[f] + (size_t)k * N * nlat : a.gin_hi[f] + (size_t)(k - a.ksplit) * N * nlat;
+  float2 v[A];
+#pragma unroll
+  for (int n1 = 0; n1 < A; ++n1) {
+    const double* row = pl + (size_t)(nm + M * n1) * nlat;
+    v[n1] = make_float2((float)__ldg(row + pair), (float)__ldg(row + (nlat - 1 - pair)));
+  }
+  ct::RD<float2, A, -1>::run(v);
+#pragma unroll
+  for (int ka = 0; ka < A; ++ka) S[b * SPB + ka * NMC + nmi] = ka ? ct::mul(v[ka], __ldg(a.twN + nm * ka)) : v[ka];
+  __syncthreads();
+  // rows (b, ka) of NMC consecutive columns into the tile images
+  const int ntile = a.nlat / 2 / PHI2_NP;
+  for (int e = t; e < PB * A * NMC; e += PB * NMC) {
+    const int r = e / NMC, i = e % NMC, bb = r / A, ka = r % A;
+    const int pr = blockIdx.x * PB + bb, tile = pr / PHI2_NP, b8 = pr % PHI2_NP;
+    float2* dst = img + ((size_t)blockIdx.z * ntile + tile) * (PHI2_NP * G::SB);
+    dst[b8 * G::SB + ka * G::PR + nm0 + i] = S[bb * SPB + ka * NMC + i];
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(P3<N, PHI2_NP>::ITEMS_C < 384 ? 256 : 384, 1)
+    phi2b_fwd32(Phi32Args a, const float2* img, int q0, int ntiles) {
+  using G = P3<N, PHI2_NP>;
+  constexpr int NP = PHI2_NP, A = G::A, B = G::B, C = G::C;
+  constexpr int T = G::ITEMS_C < 384 ? 256 : 384;
+  constexpr int XF = NP * G::SB;  // float2 per tile image
+  // [image 0 | image 1 | twiddles | 2 mbarriers]
+  extern __shared__ __align__(1024) unsigned char sm2[];
+  float2* tw = reinterpret_cast<float2*>(sm2 + 2 * G::XBYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm2 + 2 * G::XBYTES + (size_t)N * sizeof(float2));
+  const int t = threadIdx.x;
+  const int ngroups = a.nlat / 2 / NP;
+  for (int i = t; i < N; i += T) tw[i] = __ldg(a.twN + i);
+  if (t == 0) {
+    tc05::mbar_init(&full[0], 1);
+    tc05::mbar_init(&full[1], 1);
+    tc05::mbar_fence_init();
+  }
+  __syncthreads();
+  auto image = [&](int which) { return reinterpret_cast<float2*>(sm2 + which * G::XBYTES); };
+  auto issue = [&](int tile, int which) {
+    const float2* src = img + (size_t)tile * XF;
+    float2* dst = image(which);
+    mbar_arrive_tx(&full[which], (uint32_t)G::XBYTES);
+    constexpr uint32_t PIECE = 32768;
+    for (uint32_t o = 0; o < (uint32_t)G::XBYTES; o += PIECE) {
+      const uint32_t n = (uint32_t)G::XBYTES - o < PIECE ? (uint32_t)G::XBYTES - o : PIECE;
+      bulk_copy(reinterpret_cast<char*>(dst) + o, reinterpret_cast<const char*>(src) + o, n, &full[which]);
+    }
+  };
+  if (t == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+  int s = 0;
+  uint32_t phase = 0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, s ^= 1) {
+    const bool ok = tc05::mbar_wait(&full[s], (phase >> s) & 1);
+    if (__syncthreads_or(!ok)) {
+      if (t == 0) {
+        atomicExch(a.flag, 1);
+        tc05::mbar_wait(&full[s], (phase >> s) & 1);
+      }
+      return;
+    }
+    phase ^= 1u << s;
+    if (t == 0 && tile + (int)gridDim.x < ntiles) {
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      issue(tile + gridDim.x, s ^ 1);
+    }
+    const int g = tile % ngroups, q = q0 + tile / ngroups, k = q % a.nz, f = q / a.nz, p0 = g * NP;
+    float2* X = image(s);
+    if constexpr (B > 1) {  // (B)
+      for (int it = t; it < G::ITEMS_B; it += T) {
+        const int ka = it % A, rr = it / A, c = rr % C, b = rr / C;
+        float2* row = X + b * G::SB + ka * G::PR + c;
+        float2 w[B];
+#pragma unroll
+        for (int nb = 0; nb < B; ++nb) w[nb] = row[C * nb];
+        ct::RD<float2, B, -1>::run(w);
+#pragma unroll
+        for (int kb = 0; kb < B; ++kb) row[C * kb] = (kb && c) ? ct::mul(w[kb], tw[A * c * kb]) : w[kb];
+      }
+      __syncthreads();
+    }
+    if constexpr (C > 1) {  // (C)
+      for (int it = t; it < G::ITEMS_C; it += T) {
+        const int ka = it % A, rr = it / A, kb = rr % B, b = rr / B;
+        float2* row = X + b * G::SB + ka * G::PR + C * kb;
+        float2 u[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) u[c] = row[c];
+        ct::RD<float2, C, -1>::run(u);
+#pragma unroll
+        for (int kc = 0; kc < C; ++kc) row[kc] = u[kc];
+      }
+      __syncthreads();
+    }
+    // fold: lanes 2i and 2i+1 take degree m's real (even and odd parity) and
+    // imaginary rows, so each store instruction fills whole 32-byte sectors
+    const int cb = k / PLANES, row = 2 * (k % PLANES), kt = p0 / TK, kk0 = p0 % TK;
+    const int im = t & 1;
+    float W[NP];
+#pragma unroll
+    for (int b = 0; b < NP; ++b) W[b] = (float)__ldg(a.wfold + p0 + b);
+    auto zpos = [&](int m) {
+      const int qq = m / A;
+      return (m % A) * G::PR + C * (qq % B) + qq / B;
+    };
+    for (int m = t >> 1; m <= a.lmax; m += T / 2) {
+      const int pz = zpos(m), pc = zpos(m == 0 ? 0 : N - m);
+      float ev[NP], od[NP];
+#pragma unroll
+      for (int b = 0; b < NP; ++b) {
+        const float2 Z = X[b * G::SB + pz], Zc = X[b * G::SB + pc];
+        // F(ring) = (Z + conj Z(-m))/2, F(mirror) = -i (Z - conj Z(-m))/2
+        const float fr = im ? 0.5f * (Z.y - Zc.y) : 0.5f * (Z.x + Zc.x);
+        const float fm = im ? -0.5f * (Z.x - Zc.x) : 0.5f * (Z.y + Zc.y);
+        ev[b] = (fr + fm) * W[b];
+        od[b] = (fr - fm) * W[b];
+      }
+      store_tile_row<NP>(a.tiles + ana_tile(a.lmax, a.ncb, a.nkn, f, m, 0, cb, kt) * TILE_HALVES, row + im, kk0, ev);
+      store_tile_row<NP>(a.tiles + ana_tile(a.lmax, a.ncb, a.nkn, f, m, 1, cb, kt) * TILE_HALVES, row + im, kk0, od);
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  }
+}
+
 // FC-Gram continuation of physical planes (FP64), one grid point per
 // thread: out(ii) = sum_jj dir(ii,jj) f(N-d+jj) + dir(C-1-ii,jj) f(d-1-jj),
 // the same operator the z transform applies to spectral planes
@@ -1008,6 +1462,10 @@ static int build_sets(sph_plan* p, const std::vector<double>& hP, const std::vec
   return rc;
 }
 
+namespace {
+size_t phi2_plane_floats(int nphi, int nlat2);
+}  // namespace
+
 int mixed_setup(sph_plan* p, const std::vector<double>& hP, const std::vector<double>& hdP,
                 const std::vector<double>& hmPs) {
   const int lmax = p->lmax, n2 = p->nlat2;
@@ -1041,6 +1499,13 @@ int mixed_setup(sph_plan* p, const std::vector<double>& hP, const std::vector<do
       cudaMalloc((void**)&p->contg, (size_t)SPH_MAX_FIELDS * p->C * p->nphi * p->nlat * sizeof(double)) !=
           cudaSuccess)
     rc = SPH_ENOMEM;
+  if (rc == SPH_OK) {
+    const size_t per = phi2_plane_floats(p->nphi, p->nlat2);
+    if (per) {
+      p->phi2_planes = std::min(PHI2_BATCH, p->nz * SPH_MAX_FIELDS);
+      if (cudaMalloc((void**)&p->phi2, per * p->phi2_planes * sizeof(float2)) != cudaSuccess) rc = SPH_ENOMEM;
+    }
+  }
   if (rc == SPH_OK && cudaMalloc((void**)&p->dflag, sizeof(int)) != cudaSuccess) rc = SPH_ENOMEM;
   if (rc == SPH_OK && cudaMemset(p->dflag, 0, sizeof(int)) != cudaSuccess) rc = SPH_ECUDA;
   int dev = 0;
@@ -1073,9 +1538,11 @@ void mixed_free(sph_plan* p) {
     s->items = nullptr;
     s->blocks = nullptr;
   }
-  void* ptrs[] = {p->dflag, p->Tana, p->Tsyn, p->d_toff, p->contg};
+  void* ptrs[] = {p->dflag, p->Tana, p->Tsyn, p->d_toff, p->contg, p->phi2};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  p->phi2 = nullptr;
+  p->phi2_planes = 0;
   p->contg = nullptr;
   p->dflag = nullptr;
   p->Tana = nullptr;
@@ -1208,6 +1675,185 @@ int phi32_dispatch(const sph_plan* p, const Phi32Args& a, dim3 grid, size_t smem
   return SPH_EINVAL;
 }
 
+constexpr int PHI3_UNSUPPORTED = 1000;
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  return fn;
+}
+
+// 2D fp64 view [rows][nlat] of a grid array, box NP x box_rows
+#ifndef PHI3_L2_PROMOTION
+#define PHI3_L2_PROMOTION CU_TENSOR_MAP_L2_PROMOTION_L2_256B
+#endif
+int phi3_map(CUtensorMap* map, const double* base, int nlat, int rows, int np, int box_rows) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || !base || rows < 1 || reinterpret_cast<uintptr_t>(base) % 16 || nlat % 2) return PHI3_UNSUPPORTED;
+  const cuuint64_t dims[2] = {(cuuint64_t)nlat, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)nlat * sizeof(double)};
+  const cuuint32_t box[2] = {(cuuint32_t)np, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims, strides, box,
+                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         PHI3_L2_PROMOTION, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? SPH_OK : PHI3_UNSUPPORTED;
+}
+
+// three-step kernels: which (N, NP) fit (one step-A item per thread, both
+// staged forward tiles and the twiddles in shared memory)
+constexpr size_t PHI3_SMEM_MAX = 220 * 1024;
+template <int N, int NP>
+constexpr bool phi3_ok() {
+  return N % 16 == 0 && N >= 48 && NP * (N / 16) <= 1024 &&
+         (size_t)2 * N * 2 * NP * sizeof(double) + (size_t)N * sizeof(float2) <= PHI3_SMEM_MAX;
+}
+
+template <int N, int NP, bool FWD>
+int phi3_run(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st) {
+  if constexpr (!phi3_ok<N, NP>()) {
+    return PHI3_UNSUPPORTED;
+  } else {
+    using G = P3<N, NP>;
+    const size_t smem = FWD ? G::SMEM_F : G::smem_inv(p->lmax);
+    if (smem > PHI3_SMEM_MAX) return PHI3_UNSUPPORTED;
+    const long long ntiles = (long long)(p->nlat2 / NP) * p->nz * nfields;
+    if (ntiles == 0) return SPH_OK;
+    if (ntiles > (1ll << 30)) return PHI3_UNSUPPORTED;
+    int occ = 0;
+    if constexpr (FWD) {
+      Phi3Maps maps;
+      if (!a.flag) return PHI3_UNSUPPORTED;
+      for (int f = 0; f < nfields; ++f) {
+        const int rc = phi3_map(&maps.lo[f], a.gin[f], p->nlat, N * a.ksplit, NP, phi3_box_rows<N>());
+        if (rc != SPH_OK) return rc;
+        const bool hi = a.ksplit < p->nz;
+        const int rc2 = phi3_map(&maps.hi[f], hi ? a.gin_hi[f] : a.gin[f], p->nlat,
+                                 N * (hi ? p->nz - a.ksplit : a.ksplit), NP, phi3_box_rows<N>());
+        if (rc2 != SPH_OK) return rc2;
+      }
+      for (int f = nfields; f < SPH_MAX_FIELDS; ++f) maps.lo[f] = maps.hi[f] = maps.lo[0];
+      auto kern = phi3_fwd32<N, NP>;
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, G::THREADS, smem) != cudaSuccess)
+        return SPH_ECUDA;
+      const int grid = (int)std::min<long long>(ntiles, (long long)std::max(1, occ) * std::max(1, p->nsm));
+      kern<<<grid, G::THREADS, smem, st>>>(a, (int)ntiles, maps);
+    } else {
+      auto kern = phi3_inv32<N, NP>;
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, G::THREADS, smem) != cudaSuccess)
+        return SPH_ECUDA;
+      const int grid = (int)std::min<long long>(ntiles, (long long)std::max(1, occ) * std::max(1, p->nsm));
+      kern<<<grid, G::THREADS, smem, st>>>(a, (int)ntiles);
+    }
+    SPH_LAUNCH_OK();
+    return SPH_OK;
+  }
+}
+
+// two-pass forward: lengths whose 8-ring-pair tile fits shared memory only once
+template <int N>
+constexpr bool phi2_ok() {
+  if constexpr (N % 256 != 0 || N < 768 || phi3_ok<N, 8>()) {
+    return false;
+  } else {
+    return 2 * P3<N, PHI2_NP>::XBYTES + (size_t)N * sizeof(float2) + 16 <= PHI3_SMEM_MAX;
+  }
+}
+
+template <int N>
+int phi2_run(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st) {
+  if constexpr (!phi2_ok<N>()) {
+    return PHI3_UNSUPPORTED;
+  } else {
+    using G = P3<N, PHI2_NP>;
+    if (!p->phi2 || p->phi2_planes < 1 || p->nlat2 % PHI2_PB || !a.flag) return PHI3_UNSUPPORTED;
+    constexpr int T = G::ITEMS_C < 384 ? 256 : 384;
+    const size_t smem = 2 * G::XBYTES + (size_t)N * sizeof(float2) + 2 * sizeof(uint64_t);
+    auto kb = phi2b_fwd32<N>;
+    int occ = 0;
+    if (cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kb, T, smem) != cudaSuccess)
+      return SPH_ECUDA;
+    const int nq = p->nz * nfields, ngroups = p->nlat2 / PHI2_NP;
+    for (int q0 = 0; q0 < nq; q0 += p->phi2_planes) {
+      const int nb = std::min(p->phi2_planes, nq - q0);
+      phi2a_fwd32<N><<<dim3(p->nlat2 / PHI2_PB, G::M / PHI2_NMC, nb), PHI2_PB * PHI2_NMC, 0, st>>>(a, p->phi2, q0);
+      SPH_LAUNCH_OK();
+      const int ntiles = nb * ngroups;
+      const int grid = std::min(ntiles, std::max(1, occ) * std::max(1, p->nsm));
+      kb<<<grid, T, smem, st>>>(a, p->phi2, q0, ntiles);
+      SPH_LAUNCH_OK();
+    }
+    return SPH_OK;
+  }
+}
+
+int phi2_dispatch(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st) {
+  switch (p->nphi) {
+#define CASE(n) \
+  case n: return phi2_run<n>(p, a, nfields, st);
+    PHI32_SIZES(CASE)
+#undef CASE
+  }
+  return PHI3_UNSUPPORTED;
+}
+
+template <int N>
+size_t phi2_plane_floats_n(int nlat2) {
+  if constexpr (phi2_ok<N>())
+    return (size_t)(nlat2 / PHI2_NP) * PHI2_NP * P3<N, PHI2_NP>::SB;
+  else
+    return 0;
+}
+
+// float2 values of one plane's tile images (0: the two-pass form does not apply)
+size_t phi2_plane_floats(int nphi, int nlat2) {
+  if (nlat2 % PHI2_PB) return 0;
+  switch (nphi) {
+#define CASE(n) \
+  case n: return phi2_plane_floats_n<n>(nlat2);
+    PHI32_SIZES(CASE)
+#undef CASE
+  }
+  return 0;
+}
+
+// ring pairs per tile: the most that fit, at most the tuned ring_pairs
+template <int N>
+int phi3_pairs(const sph_plan* p) {
+  const int cap = p->tile_np ? p->tile_np : 8;
+  if (phi3_ok<N, 8>() && cap >= 8 && p->nlat2 % 8 == 0) return 8;
+  if (phi3_ok<N, 4>() && cap >= 4 && p->nlat2 % 4 == 0) return 4;
+  if (phi3_ok<N, 2>() && cap >= 2 && p->nlat2 % 2 == 0) return 2;
+  return 0;
+}
+
+template <bool FWD>
+int phi3_dispatch(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st) {
+  switch (p->nphi) {
+#define CASE(n)                                                  \
+  case n:                                                        \
+    switch (phi3_pairs<n>(p)) {                                  \
+      case 8: return phi3_run<n, 8, FWD>(p, a, nfields, st);     \
+      case 4: return phi3_run<n, 4, FWD>(p, a, nfields, st);     \
+      case 2: return phi3_run<n, 2, FWD>(p, a, nfields, st);     \
+    }                                                            \
+    return PHI3_UNSUPPORTED;
+    PHI32_SIZES(CASE)
+#undef CASE
+  }
+  return PHI3_UNSUPPORTED;
+}
+
 Phi32Args phi32_args(const sph_plan* p) {
   Phi32Args a = {};
   a.tiles = reinterpret_cast<__nv_bfloat16*>(p->Tana);
@@ -1226,6 +1872,7 @@ Phi32Args phi32_args(const sph_plan* p) {
   a.tw1 = p->tw4f;
   a.tw2 = p->tw4f ? p->tw4f + p->tw4off : nullptr;
   a.twN = p->twphif;
+  a.flag = p->dflag;
   return a;
 }
 
@@ -1252,18 +1899,32 @@ int launch_phi_fwd32(const sph_plan* p, const double* const* grids, int nfields,
     a.ksplit = p->N;
     for (int f = 0; f < nfields; ++f) a.gin_hi[f] = grids_hi[f];
   }
+  TimedLaunch tl(p, T_PHI_FWD, st);
+  bool aligned = p->nlat % 2 == 0;
+  for (int f = 0; f < nfields; ++f)
+    aligned = aligned && reinterpret_cast<uintptr_t>(a.gin[f]) % 16 == 0 &&
+              (!grids_hi || reinterpret_cast<uintptr_t>(a.gin_hi[f]) % 16 == 0);
+  {
+    const int rc = phi2_dispatch(p, a, nfields, st);
+    if (rc != PHI3_UNSUPPORTED) return rc;
+  }
+  if (aligned) {
+    const int rc = phi3_dispatch<true>(p, a, nfields, st);
+    if (rc != PHI3_UNSUPPORTED) return rc;
+  }
   dim3 grid(p->nlat2 / a.NP, p->nz, nfields);
   const size_t smem = (size_t)a.NP * seq_stride(p->nphi) * sizeof(float2);
-  TimedLaunch tl(p, T_PHI_FWD, st);
   return phi32_dispatch<true>(p, a, grid, smem, st);
 }
 
 int launch_phi_inv32(const sph_plan* p, double* const* grids, int nfields, cudaStream_t st) {
   Phi32Args a = phi32_args(p);
   for (int f = 0; f < nfields; ++f) a.gout[f] = grids[f];
+  TimedLaunch tl(p, T_PHI_INV, st);
+  const int rc = phi3_dispatch<false>(p, a, nfields, st);
+  if (rc != PHI3_UNSUPPORTED) return rc;
   dim3 grid(p->nlat2 / a.NP, p->nz, nfields);
   const size_t smem = (size_t)a.NP * seq_stride(p->nphi) * sizeof(float2);
-  TimedLaunch tl(p, T_PHI_INV, st);
   return phi32_dispatch<false>(p, a, grid, smem, st);
 }
 

@@ -142,6 +142,9 @@ struct sph_plan {
   int tile_np = 0;               // phi transforms: ring pairs per CTA (1, 2, 4, 8)
   int tile_lb = 0;               // z transforms: lm columns per CTA (1..64, power of two)
   double* contg = nullptr;       // [3][Cz][nphi][nlat] physically continued planes (mixed)
+  // two-pass forward phi transform (mixed): tile images of phi2_planes plane-fields
+  float2* phi2 = nullptr;
+  int phi2_planes = 0;
   // stage timers (sph_timer_*): event pairs recorded around each launch
   int timing = 0;
   std::vector<cudaEvent_t> ev_pool;
