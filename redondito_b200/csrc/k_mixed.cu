@@ -113,8 +113,23 @@ template <int NV>
 __device__ __forceinline__ void store_tile_row(__nv_bfloat16* tile, int row, int kk0, const float* v) {
   static_assert(NV == 1 || NV == 2 || NV == 4 || NV == 8, "row chunk");
   __align__(16) __nv_bfloat16 p[NPIECE][NV];
+  if constexpr (NV == 1) {
+    split3(v[0], p[0][0], p[1][0], p[2][0]);
+  } else {
+    // the same three roundings as split3, two values per conversion
 #pragma unroll
-  for (int j = 0; j < NV; ++j) split3(v[j], p[0][j], p[1][j], p[2][j]);
+    for (int j = 0; j < NV; j += 2) {
+      const __nv_bfloat162 h = __floats2bfloat162_rn(v[j], v[j + 1]);
+      const float2 hf = __bfloat1622float2(h);
+      const float r0 = v[j] - hf.x, r1 = v[j + 1] - hf.y;
+      const __nv_bfloat162 m = __floats2bfloat162_rn(r0, r1);
+      const float2 mf = __bfloat1622float2(m);
+      const __nv_bfloat162 l = __floats2bfloat162_rn(r0 - mf.x, r1 - mf.y);
+      *reinterpret_cast<__nv_bfloat162*>(&p[0][j]) = h;
+      *reinterpret_cast<__nv_bfloat162*>(&p[1][j]) = m;
+      *reinterpret_cast<__nv_bfloat162*>(&p[2][j]) = l;
+    }
+  }
   const uint32_t off = tc05::kmaj_off(row, kk0, MCOLS) / 2;
 #pragma unroll
   for (int s = 0; s < NPIECE; ++s) {
@@ -1097,56 +1112,55 @@ __global__ void __launch_bounds__(PHI2_PB* PHI2_NMC, 2) phi2a_fwd32(Phi32Args a,
   }
 }
 
+constexpr int PHI2_T = 384;  // pass-2 threads: two CTAs per SM, one tile image each
 template <int N>
-__global__ void __launch_bounds__(P3<N, PHI2_NP>::ITEMS_C < 384 ? 256 : 384, 1)
-    phi2b_fwd32(Phi32Args a, const float2* img, int q0, int ntiles) {
+__host__ __device__ constexpr size_t phi2_smem() {
+  return P3<N, PHI2_NP>::XBYTES + (size_t)P3<N, PHI2_NP>::M * sizeof(float2) + sizeof(uint64_t);
+}
+
+template <int N>
+__global__ void __launch_bounds__(PHI2_T, 2) phi2b_fwd32(Phi32Args a, const float2* img, int q0, int nq, int ntiles) {
   using G = P3<N, PHI2_NP>;
-  constexpr int NP = PHI2_NP, A = G::A, B = G::B, C = G::C;
-  constexpr int T = G::ITEMS_C < 384 ? 256 : 384;
+  constexpr int NP = PHI2_NP, A = G::A, M = G::M, B = G::B, C = G::C, T = PHI2_T;
   constexpr int XF = NP * G::SB;  // float2 per tile image
-  // [image 0 | image 1 | twiddles | 2 mbarriers]
+  // [tile image | twiddles W_M^e | mbarrier]; the other CTA on the SM computes while this one loads
   extern __shared__ __align__(1024) unsigned char sm2[];
-  float2* tw = reinterpret_cast<float2*>(sm2 + 2 * G::XBYTES);
-  uint64_t* full = reinterpret_cast<uint64_t*>(sm2 + 2 * G::XBYTES + (size_t)N * sizeof(float2));
+  float2* X = reinterpret_cast<float2*>(sm2);
+  float2* tw = reinterpret_cast<float2*>(sm2 + G::XBYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm2 + G::XBYTES + (size_t)M * sizeof(float2));
   const int t = threadIdx.x;
   const int ngroups = a.nlat / 2 / NP;
-  for (int i = t; i < N; i += T) tw[i] = __ldg(a.twN + i);
+  for (int i = t; i < M; i += T) tw[i] = __ldg(a.twN + A * i);
   if (t == 0) {
-    tc05::mbar_init(&full[0], 1);
-    tc05::mbar_init(&full[1], 1);
+    tc05::mbar_init(full, 1);
     tc05::mbar_fence_init();
   }
   __syncthreads();
-  auto image = [&](int which) { return reinterpret_cast<float2*>(sm2 + which * G::XBYTES); };
-  auto issue = [&](int tile, int which) {
-    const float2* src = img + (size_t)tile * XF;
-    float2* dst = image(which);
-    mbar_arrive_tx(&full[which], (uint32_t)G::XBYTES);
-    constexpr uint32_t PIECE = 32768;
-    for (uint32_t o = 0; o < (uint32_t)G::XBYTES; o += PIECE) {
-      const uint32_t n = (uint32_t)G::XBYTES - o < PIECE ? (uint32_t)G::XBYTES - o : PIECE;
-      bulk_copy(reinterpret_cast<char*>(dst) + o, reinterpret_cast<const char*>(src) + o, n, &full[which]);
-    }
-  };
-  if (t == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
-  int s = 0;
   uint32_t phase = 0;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, s ^= 1) {
-    const bool ok = tc05::mbar_wait(&full[s], (phase >> s) & 1);
-    if (__syncthreads_or(!ok)) {
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, phase ^= 1) {
+    // planes fastest: the CTAs in flight write the tiles of one or two node
+    // tiles (kt), a set that stays in L2 until every row of it is written
+    const int g = tile / nq, ql = tile % nq, q = q0 + ql, k = q % a.nz, f = q / a.nz, p0 = g * NP;
+    if (t == 0) {
+      const float2* src = img + ((size_t)ql * ngroups + g) * XF;
+      mbar_arrive_tx(full, (uint32_t)G::XBYTES);
+      constexpr uint32_t PIECE = 32768;
+      for (uint32_t o = 0; o < (uint32_t)G::XBYTES; o += PIECE) {
+        const uint32_t n = (uint32_t)G::XBYTES - o < PIECE ? (uint32_t)G::XBYTES - o : PIECE;
+        bulk_copy(reinterpret_cast<char*>(X) + o, reinterpret_cast<const char*>(src) + o, n, full);
+      }
+    }
+    float W[NP];  // quadrature weights, loaded while the image arrives
+#pragma unroll
+    for (int b = 0; b < NP; ++b) W[b] = (float)__ldg(a.wfold + p0 + b);
+    const bool ok = tc05::mbar_wait(full, phase);
+    if (__syncthreads_or(!ok)) {  // the image never arrived: report, let the copy land, stop
       if (t == 0) {
         atomicExch(a.flag, 1);
-        tc05::mbar_wait(&full[s], (phase >> s) & 1);
+        tc05::mbar_wait(full, phase);
       }
       return;
     }
-    phase ^= 1u << s;
-    if (t == 0 && tile + (int)gridDim.x < ntiles) {
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      issue(tile + gridDim.x, s ^ 1);
-    }
-    const int g = tile % ngroups, q = q0 + tile / ngroups, k = q % a.nz, f = q / a.nz, p0 = g * NP;
-    float2* X = image(s);
     if constexpr (B > 1) {  // (B)
       for (int it = t; it < G::ITEMS_B; it += T) {
         const int ka = it % A, rr = it / A, c = rr % C, b = rr / C;
@@ -1156,7 +1170,7 @@ __global__ void __launch_bounds__(P3<N, PHI2_NP>::ITEMS_C < 384 ? 256 : 384, 1)
         for (int nb = 0; nb < B; ++nb) w[nb] = row[C * nb];
         ct::RD<float2, B, -1>::run(w);
 #pragma unroll
-        for (int kb = 0; kb < B; ++kb) row[C * kb] = (kb && c) ? ct::mul(w[kb], tw[A * c * kb]) : w[kb];
+        for (int kb = 0; kb < B; ++kb) row[C * kb] = (kb && c) ? ct::mul(w[kb], tw[c * kb]) : w[kb];
       }
       __syncthreads();
     }
@@ -1177,9 +1191,6 @@ __global__ void __launch_bounds__(P3<N, PHI2_NP>::ITEMS_C < 384 ? 256 : 384, 1)
     // imaginary rows, so each store instruction fills whole 32-byte sectors
     const int cb = k / PLANES, row = 2 * (k % PLANES), kt = p0 / TK, kk0 = p0 % TK;
     const int im = t & 1;
-    float W[NP];
-#pragma unroll
-    for (int b = 0; b < NP; ++b) W[b] = (float)__ldg(a.wfold + p0 + b);
     auto zpos = [&](int m) {
       const int qq = m / A;
       return (m % A) * G::PR + C * (qq % B) + qq / B;
@@ -1199,7 +1210,9 @@ __global__ void __launch_bounds__(P3<N, PHI2_NP>::ITEMS_C < 384 ? 256 : 384, 1)
       store_tile_row<NP>(a.tiles + ana_tile(a.lmax, a.ncb, a.nkn, f, m, 0, cb, kt) * TILE_HALVES, row + im, kk0, ev);
       store_tile_row<NP>(a.tiles + ana_tile(a.lmax, a.ncb, a.nkn, f, m, 1, cb, kt) * TILE_HALVES, row + im, kk0, od);
     }
+    // the image is refilled by the bulk copy (async proxy) after this barrier
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
   }
 }
 
@@ -1742,6 +1755,7 @@ int phi3_run(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st
       for (int f = nfields; f < SPH_MAX_FIELDS; ++f) maps.lo[f] = maps.hi[f] = maps.lo[0];
       auto kern = phi3_fwd32<N, NP>;
       if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+          cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess ||
           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, G::THREADS, smem) != cudaSuccess)
         return SPH_ECUDA;
       const int grid = (int)std::min<long long>(ntiles, (long long)std::max(1, occ) * std::max(1, p->nsm));
@@ -1749,6 +1763,7 @@ int phi3_run(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st
     } else {
       auto kern = phi3_inv32<N, NP>;
       if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+          cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess ||
           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, G::THREADS, smem) != cudaSuccess)
         return SPH_ECUDA;
       const int grid = (int)std::min<long long>(ntiles, (long long)std::max(1, occ) * std::max(1, p->nsm));
@@ -1765,7 +1780,7 @@ constexpr bool phi2_ok() {
   if constexpr (N % 256 != 0 || N < 768 || phi3_ok<N, 8>()) {
     return false;
   } else {
-    return 2 * P3<N, PHI2_NP>::XBYTES + (size_t)N * sizeof(float2) + 16 <= PHI3_SMEM_MAX;
+    return phi2_smem<N>() <= PHI3_SMEM_MAX;
   }
 }
 
@@ -1776,11 +1791,12 @@ int phi2_run(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st
   } else {
     using G = P3<N, PHI2_NP>;
     if (!p->phi2 || p->phi2_planes < 1 || p->nlat2 % PHI2_PB || !a.flag) return PHI3_UNSUPPORTED;
-    constexpr int T = G::ITEMS_C < 384 ? 256 : 384;
-    const size_t smem = 2 * G::XBYTES + (size_t)N * sizeof(float2) + 2 * sizeof(uint64_t);
+    constexpr int T = PHI2_T;
+    const size_t smem = phi2_smem<N>();
     auto kb = phi2b_fwd32<N>;
     int occ = 0;
     if (cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(kb, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kb, T, smem) != cudaSuccess)
       return SPH_ECUDA;
     const int nq = p->nz * nfields, ngroups = p->nlat2 / PHI2_NP;
@@ -1790,7 +1806,7 @@ int phi2_run(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st
       SPH_LAUNCH_OK();
       const int ntiles = nb * ngroups;
       const int grid = std::min(ntiles, std::max(1, occ) * std::max(1, p->nsm));
-      kb<<<grid, T, smem, st>>>(a, p->phi2, q0, ntiles);
+      kb<<<grid, T, smem, st>>>(a, p->phi2, q0, nb, ntiles);
       SPH_LAUNCH_OK();
     }
     return SPH_OK;
