@@ -1243,25 +1243,72 @@ __global__ void cont_phys_kernel(const double* __restrict__ f0, const double* __
   }
 }
 
-// Spectra (lm order) -> synthesis data tiles.  Thread c of block (m, k, field)
-// takes l = m + 16c .. m + 16c + 15, i.e. 8 values of each parity (q = 8c ..
+// The same continuation with the order d fixed at compile time: the matrix
+// in shared memory (read as a broadcast), the 2 d input values of each point
+// in registers, two points per thread (each matrix entry read once for both);
+// every output is summed in the same order as above.
+template <int D>
+__global__ void __launch_bounds__(256) cont_phys_d(const double* __restrict__ f0, const double* __restrict__ f1,
+                                                   const double* __restrict__ f2, double* out,
+                                                   const double* __restrict__ dir, int C, int N, size_t npts) {
+  extern __shared__ double sdir[];  // dir(ii, jj) at ii + C jj
+  for (int i = threadIdx.x; i < C * D; i += blockDim.x) sdir[i] = __ldg(dir + i);
+  __syncthreads();
+  const int f = blockIdx.y;
+  const double* in = f == 0 ? f0 : (f == 1 ? f1 : f2);
+  double* o = out + (size_t)f * C * npts;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < npts; x += 2 * stride) {
+    const size_t x2 = x + stride;
+    const bool two = x2 < npts;
+    double hi0[D], lo0[D], hi1[D], lo1[D];
+#pragma unroll
+    for (int jj = 0; jj < D; ++jj) {
+      hi0[jj] = __ldg(in + (size_t)(N - D + jj) * npts + x);
+      lo0[jj] = __ldg(in + (size_t)(D - 1 - jj) * npts + x);
+      hi1[jj] = two ? __ldg(in + (size_t)(N - D + jj) * npts + x2) : 0.0;
+      lo1[jj] = two ? __ldg(in + (size_t)(D - 1 - jj) * npts + x2) : 0.0;
+    }
+    for (int ii = 0; ii < C; ++ii) {
+      double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+      for (int jj = 0; jj < D; ++jj) {
+        const double w1 = sdir[ii + C * jj], w2 = sdir[(C - 1 - ii) + C * jj];
+        a0 = (a0 + w1 * hi0[jj]) + w2 * lo0[jj];
+        a1 = (a1 + w1 * hi1[jj]) + w2 * lo1[jj];
+      }
+      o[(size_t)ii * npts + x] = a0;
+      if (two) o[(size_t)ii * npts + x2] = a1;
+    }
+  }
+}
+
+// Spectra (lm order) -> synthesis data tiles.  The warp of block (m, k,
+// field) first reads the block's degrees l = m .. into shared memory with
+// consecutive lanes on consecutive l (one padding slot every 16 values, so
+// the chunk reads below fall in distinct banks); then thread c takes
+// l = m + 16c .. m + 16c + 15, i.e. 8 values of each parity (q = 8c ..
 // 8c + 7), and writes one row chunk per parity and component; values past
 // lmax are written as zeros.
+__host__ __device__ inline int spec_tile_values(int lmax) { return ntiles_of(lmax, 0, 0) * (TK / 8) * 16; }
 __global__ void spec_to_tiles(const double2* __restrict__ in, const double2* __restrict__ in2,
                               __nv_bfloat16* tiles, size_t tfield, const long long* __restrict__ toff,
                               const int* __restrict__ mbase, int lmax, int nlm) {
+  extern __shared__ double2 sv[];
   const int m = blockIdx.x, k = blockIdx.y, f = blockIdx.z;
   const double2* src = (f ? in2 : in) + (size_t)k * nlm + mbase[m] - m;
   __nv_bfloat16* T = tiles + (size_t)f * tfield;
   const int cb = k / PLANES, row = 2 * (k % PLANES);
   const int nc = ntiles_of(lmax, m, 0) * (TK / 8);  // chunks of 8 q (parity 0 has the most rows)
+  for (int i = threadIdx.x; i < nc * 16; i += blockDim.x) {
+    const int l = m + i;
+    sv[i + (i >> 4)] = l <= lmax ? __ldg(src + l) : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
   for (int c = threadIdx.x; c < nc; c += blockDim.x) {
     double2 v[16];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const int l = m + 16 * c + j;
-      v[j] = l <= lmax ? __ldg(src + l) : make_double2(0.0, 0.0);
-    }
+    for (int j = 0; j < 16; ++j) v[j] = sv[17 * c + j];
     const int kt = c / (TK / 8), kk0 = (c % (TK / 8)) * 8;
 #pragma unroll
     for (int par = 0; par < 2; ++par) {
@@ -1870,6 +1917,11 @@ int phi3_dispatch(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream
   return PHI3_UNSUPPORTED;
 }
 
+size_t spec_smem(int lmax) {
+  const int nv = spec_tile_values(lmax);
+  return (size_t)(nv + nv / 16) * sizeof(double2);
+}
+
 Phi32Args phi32_args(const sph_plan* p) {
   Phi32Args a = {};
   a.tiles = reinterpret_cast<__nv_bfloat16*>(p->Tana);
@@ -1900,8 +1952,19 @@ int launch_cont_phys(const sph_plan* p, const double* const* grids, int nfields,
   const double* f[SPH_MAX_FIELDS] = {grids[0], nfields > 1 ? grids[1] : grids[0], nfields > 2 ? grids[2] : grids[0]};
   TimedLaunch tl(p, T_OPS, st);
   const int blocks = (int)std::min<size_t>((npts + 255) / 256, 148 * 8);
-  cont_phys_kernel<<<dim3(blocks, nfields), 256, 0, st>>>(f[0], f[1], f[2], p->contg, p->d_dir, p->C, p->d, p->N,
-                                                        npts);
+  const size_t smem = (size_t)p->C * p->d * sizeof(double);
+  switch (p->d) {
+#define CASE(D)                                                                                                  \
+  case D:                                                                                                        \
+    cont_phys_d<D><<<dim3(blocks, nfields), 256, smem, st>>>(f[0], f[1], f[2], p->contg, p->d_dir, p->C, p->N, \
+                                                              npts);                                             \
+    break;
+    CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
+#undef CASE
+    default:
+      cont_phys_kernel<<<dim3(blocks, nfields), 256, 0, st>>>(f[0], f[1], f[2], p->contg, p->d_dir, p->C, p->d,
+                                                            p->N, npts);
+  }
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
@@ -1958,7 +2021,7 @@ int launch_tc_synthesis(const sph_plan* p, int vector, const double2* in, const 
   a.tiles = reinterpret_cast<const __nv_bfloat16*>(p->Tsyn);
   {
     TimedLaunch tl(p, T_OPS, st);
-    spec_to_tiles<<<dim3(p->lmax + 1, p->nz, vector ? 2 : 1), 32, 0, st>>>(
+    spec_to_tiles<<<dim3(p->lmax + 1, p->nz, vector ? 2 : 1), 32, spec_smem(p->lmax), st>>>(
         in, in2, reinterpret_cast<__nv_bfloat16*>(p->Tsyn), p->Tsynfield, p->d_toff, p->d_mbase, p->lmax, p->nlm);
     SPH_LAUNCH_OK();
   }
@@ -2027,7 +2090,7 @@ int tc_group_launch(const GroupLaunch& g, int* flag, cudaStream_t st) {
 
 int launch_spec_to_tiles_field(const sph_plan* p, const double2* in, int field, cudaStream_t st) {
   if (p->precision != SPH_MIXED || field < 0 || field >= SPH_MAX_FIELDS) return SPH_EINVAL;
-  spec_to_tiles<<<dim3(p->lmax + 1, p->nz, 1), 32, 0, st>>>(
+  spec_to_tiles<<<dim3(p->lmax + 1, p->nz, 1), 32, spec_smem(p->lmax), st>>>(
       in, nullptr, reinterpret_cast<__nv_bfloat16*>(p->Tsyn) + (size_t)field * p->Tsynfield, p->Tsynfield,
       p->d_toff, p->d_mbase, p->lmax, p->nlm);
   SPH_LAUNCH_OK();
