@@ -53,6 +53,13 @@ struct ZGeo<0> {
   }
 };
 
+// 16-byte global -> shared copy that lands asynchronously; src_bytes 0
+// writes zeros (src is then not read but must be a valid address)
+__device__ __forceinline__ void cp_async16z(void* dst, const void* src, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+
 template <int MODE, int CTN>
 __global__ void __launch_bounds__(ZTHREADS) zfft_kernel(ZArgs a) {
   extern __shared__ double2 sm[];
@@ -64,20 +71,26 @@ __global__ void __launch_bounds__(ZTHREADS) zfft_kernel(ZArgs a) {
   double2* orig = sm + (size_t)LB * nz;  // D_l keeps the input column for the l(l+1)/r^2 term
 
   const int* __restrict__ rev = a.fd.rev;
+  // every copy of the slab is in flight at once (no registers held); columns
+  // past nlm are zero-filled
   for (int idx = tid; idx < nload * LB; idx += ZTHREADS) {
     int r = idx / LB, c = idx - r * LB;
     int lm = lm0 + c;
-    double2 v = lm < nlm ? a.in[(size_t)r * nlm + lm] : make_double2(0.0, 0.0);
+    const bool in = lm < nlm;
     // the inverse transform takes its input in digit-reversed order
-    sm[(MODE == Z_INV ? __ldg(rev + r) : r) * LB + c] = v;
+    cp_async16z(sm + (MODE == Z_INV ? __ldg(rev + r) : r) * LB + c, in ? a.in + (size_t)r * nlm + lm : a.in,
+                in ? 16 : 0);
   }
   if (MODE == Z_DLR) {
     for (int idx = tid; idx < nz * LB; idx += ZTHREADS) {
       int r = idx / LB, c = idx - r * LB;
       int lm = lm0 + c;
-      orig[idx] = lm < nlm ? a.in[(size_t)r * nlm + lm] : make_double2(0.0, 0.0);
+      const bool in = lm < nlm;
+      cp_async16z(orig + idx, in ? a.in + (size_t)r * nlm + lm : a.in, in ? 16 : 0);
     }
   }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncthreads();
 
   if (cont) {
