@@ -801,8 +801,10 @@ struct P3 {
   static_assert(N % A == 0 && NP >= 2 && NP <= 16 && XBYTES % 16 == 0, "three-step geometry");
   // single-pass kernels: the transform area overlays one staged tile, one step-A item per thread
   static constexpr bool ONE_PASS = XBYTES <= STAGE_F && ITEMS_A <= THREADS && THREADS <= 1024;
-  // inverse: transform area, twiddles, two staged coefficient tiles of (lmax + 1) x 2 x NP float2
-  __host__ __device__ static size_t smem_inv(int lmax) { return XBYTES + (size_t)N * sizeof(float2) + 2 * stage_inv(lmax) * sizeof(float2); }
+  // inverse: transform area, twiddles, one staged coefficient tile of (lmax + 1) x 2 x NP float2;
+  // two CTAs per SM where that fits for every lmax < N/2 (one loads while the other computes)
+  __host__ __device__ static size_t smem_inv(int lmax) { return XBYTES + (size_t)N * sizeof(float2) + stage_inv(lmax) * sizeof(float2); }
+  static constexpr int MINB_INV = XBYTES + (size_t)N * sizeof(float2) + (size_t)N * NP * sizeof(float2) <= 113 * 1024 && THREADS <= 512 ? 2 : 1;
   __host__ __device__ static int stage_inv(int lmax) { return (lmax + 1) * 2 * NP; }
 };
 
@@ -979,7 +981,7 @@ __global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB)
 }
 
 template <int N, int NP>
-__global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB) phi3_inv32(Phi32Args a, int ntiles) {
+__global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB_INV) phi3_inv32(Phi32Args a, int ntiles) {
   using G = P3<N, NP>;
   constexpr int A = G::A, M = G::M, B = G::B, C = G::C, T = G::THREADS;
   static_assert(G::ONE_PASS, "single-pass geometry");
@@ -987,7 +989,6 @@ __global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB) phi3_inv3
   float2* X = reinterpret_cast<float2*>(sm3i);
   float2* tw = reinterpret_cast<float2*>(sm3i + G::XBYTES);
   const int lmax = a.lmax, nlat = a.nlat, ngroups = nlat / 2 / NP;
-  const int sf2 = G::stage_inv(lmax);
   float2* stg = tw + N;
   const int t = threadIdx.x;
   for (int i = t; i < N; i += T) tw[i] = __ldg(a.twN + i);
@@ -1003,14 +1004,14 @@ __global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB) phi3_inv3
     }
     cp_async_commit();
   };
-  if ((int)blockIdx.x < ntiles) issue(blockIdx.x, stg);
-  int s = 0;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, s ^= 1) {
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    // the staged tile of the previous iteration was last read before the
+    // barrier that follows step (C'), so it can be refilled here
+    issue(tile, stg);
     cp_async_wait_all();
     __syncthreads();
-    if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x, stg + (s ^ 1) * sf2);
     const int g = tile % ngroups, r = tile / ngroups, k = r % a.nz, f = r / a.nz, p0 = g * NP;
-    const float2* st = stg + s * sf2;
+    const float2* st = stg;
     // Z(m) of ring pair b (x = ring + i mirror) from the folded coefficients of both parities
     auto zin = [&](int m, int b) {
       const bool lo = m <= lmax, hi = N - m <= lmax;
@@ -1283,32 +1284,25 @@ __global__ void __launch_bounds__(256) cont_phys_d(const double* __restrict__ f0
   }
 }
 
-// Spectra (lm order) -> synthesis data tiles.  The warp of block (m, k,
-// field) first reads the block's degrees l = m .. into shared memory with
-// consecutive lanes on consecutive l (one padding slot every 16 values, so
-// the chunk reads below fall in distinct banks); then thread c takes
-// l = m + 16c .. m + 16c + 15, i.e. 8 values of each parity (q = 8c ..
+// Spectra (lm order) -> synthesis data tiles.  Thread c of block (m, k, field)
+// takes l = m + 16c .. m + 16c + 15, i.e. 8 values of each parity (q = 8c ..
 // 8c + 7), and writes one row chunk per parity and component; values past
 // lmax are written as zeros.
-__host__ __device__ inline int spec_tile_values(int lmax) { return ntiles_of(lmax, 0, 0) * (TK / 8) * 16; }
 __global__ void spec_to_tiles(const double2* __restrict__ in, const double2* __restrict__ in2,
                               __nv_bfloat16* tiles, size_t tfield, const long long* __restrict__ toff,
                               const int* __restrict__ mbase, int lmax, int nlm) {
-  extern __shared__ double2 sv[];
   const int m = blockIdx.x, k = blockIdx.y, f = blockIdx.z;
   const double2* src = (f ? in2 : in) + (size_t)k * nlm + mbase[m] - m;
   __nv_bfloat16* T = tiles + (size_t)f * tfield;
   const int cb = k / PLANES, row = 2 * (k % PLANES);
   const int nc = ntiles_of(lmax, m, 0) * (TK / 8);  // chunks of 8 q (parity 0 has the most rows)
-  for (int i = threadIdx.x; i < nc * 16; i += blockDim.x) {
-    const int l = m + i;
-    sv[i + (i >> 4)] = l <= lmax ? __ldg(src + l) : make_double2(0.0, 0.0);
-  }
-  __syncthreads();
   for (int c = threadIdx.x; c < nc; c += blockDim.x) {
     double2 v[16];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) v[j] = sv[17 * c + j];
+    for (int j = 0; j < 16; ++j) {
+      const int l = m + 16 * c + j;
+      v[j] = l <= lmax ? __ldg(src + l) : make_double2(0.0, 0.0);
+    }
     const int kt = c / (TK / 8), kk0 = (c % (TK / 8)) * 8;
 #pragma unroll
     for (int par = 0; par < 2; ++par) {
@@ -1917,11 +1911,6 @@ int phi3_dispatch(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream
   return PHI3_UNSUPPORTED;
 }
 
-size_t spec_smem(int lmax) {
-  const int nv = spec_tile_values(lmax);
-  return (size_t)(nv + nv / 16) * sizeof(double2);
-}
-
 Phi32Args phi32_args(const sph_plan* p) {
   Phi32Args a = {};
   a.tiles = reinterpret_cast<__nv_bfloat16*>(p->Tana);
@@ -2021,7 +2010,7 @@ int launch_tc_synthesis(const sph_plan* p, int vector, const double2* in, const 
   a.tiles = reinterpret_cast<const __nv_bfloat16*>(p->Tsyn);
   {
     TimedLaunch tl(p, T_OPS, st);
-    spec_to_tiles<<<dim3(p->lmax + 1, p->nz, vector ? 2 : 1), 32, spec_smem(p->lmax), st>>>(
+    spec_to_tiles<<<dim3(p->lmax + 1, p->nz, vector ? 2 : 1), 32, 0, st>>>(
         in, in2, reinterpret_cast<__nv_bfloat16*>(p->Tsyn), p->Tsynfield, p->d_toff, p->d_mbase, p->lmax, p->nlm);
     SPH_LAUNCH_OK();
   }
@@ -2090,7 +2079,7 @@ int tc_group_launch(const GroupLaunch& g, int* flag, cudaStream_t st) {
 
 int launch_spec_to_tiles_field(const sph_plan* p, const double2* in, int field, cudaStream_t st) {
   if (p->precision != SPH_MIXED || field < 0 || field >= SPH_MAX_FIELDS) return SPH_EINVAL;
-  spec_to_tiles<<<dim3(p->lmax + 1, p->nz, 1), 32, spec_smem(p->lmax), st>>>(
+  spec_to_tiles<<<dim3(p->lmax + 1, p->nz, 1), 32, 0, st>>>(
       in, nullptr, reinterpret_cast<__nv_bfloat16*>(p->Tsyn) + (size_t)field * p->Tsynfield, p->Tsynfield,
       p->d_toff, p->d_mbase, p->lmax, p->nlm);
   SPH_LAUNCH_OK();
