@@ -210,9 +210,10 @@ int launch_zfft(const sph_plan* p, int mode, const double2* in, double2* out, in
   a.zinv2 = p->zinv2;
   a.ell = p->d_ell;
   a.fd = p->fz;
-  // columns per CTA: a power of two with LB*nz <= ZMAXCOL, at most 64
+  // columns per CTA: a power of two with LB*nz <= ZMAXCOL/2, at most 64
+  // (32 KB slabs: 4 CTAs per SM, still full 128-byte lines per row at nz = 256)
   int LB = 64;
-  while (LB > 1 && LB * p->nz > ZMAXCOL) LB >>= 1;
+  while (LB > 1 && LB * p->nz > ZMAXCOL / 2) LB >>= 1;
   if (p->tile_lb) LB = p->tile_lb;
   if (LB * p->nz > ZMAXCOL) return SPH_EINVAL;
   a.LB = LB;
