@@ -538,7 +538,10 @@ def main():
                 "launches": nl, "ms_per_launch": tms / max(nl, 1),
                 "peak_source": ("fp64 DMMA probe run live (redondito_b200/peak/fp64_peak.cu)"
                                 if bound == "tensor" and args.precision == "fp64"
-                                else "MEASURED_PEAKS.json")}
+                                else "measured (MEASURED_PEAKS.json)"
+                                if ("hbm_gbs" if bound == "hbm" else "bf16_tflops") in peaks
+                                else "fallback: this pool's earlier measurement, 6.65 TB/s and 1.59 PFLOP/s "
+                                     "(MEASURED_PEAKS.json absent)")}
     shares = {c: round(stage[c][0] / max(ms, 1e-9), 4) for c in stage if stage[c][1]}
     launches = sum(v[1] for v in stage.values())
 
