@@ -3,9 +3,12 @@
 For a problem size (lmax, nz, nlat, nphi, precision) the tuner times the
 candidate tile shapes of sph_plan_set_tiles -- MMA rows per scalar Legendre
 work item (mixed plans), Gauss ring pairs per phi-transform CTA and lm
-columns per z-transform CTA -- on the device, one batch run (3D pair plus
-radial derivative of one field, the C4 work of a problem) per repetition,
-and keeps the fastest.  Results are cached in a JSON table keyed by the
+columns per z-transform CTA -- on the device and keeps the fastest.  A
+timing is one batch run (3D pair plus radial derivative of one field, the
+C4 work of a problem) of CONCURRENT copies of the problem, each on its own
+plan, so that a shape is judged under the load of an ensemble rather than
+alone (alone, shapes that split a small problem into more CTAs win, and
+they lose when 64 problems share the device).  Results are cached in a JSON table keyed by the
 problem size; the table measured on B200 ships as tiles_b200.json beside
 this module and is what batches use by default.
 
@@ -21,7 +24,8 @@ DEFAULT_TABLE = os.path.join(HERE, "tiles_b200.json")
 
 ROWS = (64, 128)
 RING_PAIRS = (2, 4, 8)
-Z_COLS = (16, 32, 64)
+Z_COLS = (8, 16, 32, 64)
+CONCURRENT = 8  # problems per timed batch
 
 # the C4 ensemble: lmax in {63, 127, 255}, nz in {32, 64, 96, 128}, nlat = 3(lmax+1)/2, nphi = 2 nlat
 C4_LMAX = (63, 127, 255)
@@ -65,20 +69,31 @@ def tiles_for(lmax, nz, nlat, nphi, precision, table=None):
     return table.get(key(lmax, nz, nlat, nphi, precision))
 
 
-def apply(plan, tiles):
-    from redondito_b200 import sphp as S
+def apply(plan, tiles, S=None):
+    if S is None:
+        from redondito_b200 import sphp as S
     if tiles:
         S.set_tiles(plan, tiles["rows"], tiles["ring_pairs"], tiles["z_cols"])
 
 
-def time_candidate(S, torch, P, tiles, reps=5):
-    """Device ms of one batch run (3D pair + radial derivative of one field)."""
-    apply(P, tiles)
-    B = S.Batch([P], [1])
+def candidate_batch(S, plans, tiles):
+    """The batch a candidate is timed on: the candidate's shape on every plan,
+    and the shipped table NOT applied on top of it."""
+    for P in plans:
+        apply(P, tiles, S)
+    return S.Batch(plans, [1] * len(plans), tuned=False)
+
+
+def time_candidate(S, torch, plans, tiles, reps=5):
+    """Device ms of one batch run (3D pair + radial derivative of one field
+    per plan) with the candidate's tile shape."""
+    B = candidate_batch(S, plans, tiles)
+    P = plans[0]
     gen = torch.Generator(device=P.device)
     gen.manual_seed(1)
-    x = torch.randn((P.nz, P.nlm), generator=gen, device=P.device, dtype=torch.float64)
-    B.spec[0][0].copy_(torch.complex(x, torch.zeros_like(x)))
+    for xs in B.spec:
+        x = torch.randn((P.nz, P.nlm), generator=gen, device=P.device, dtype=torch.float64)
+        xs[0].copy_(torch.complex(x, torch.zeros_like(x)))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     B.run()
     torch.cuda.synchronize()
@@ -92,13 +107,14 @@ def time_candidate(S, torch, P, tiles, reps=5):
     return e0.elapsed_time(e1) / reps
 
 
-def tune(lmax, nz, nlat, nphi, precision, reps=5):
+def tune(lmax, nz, nlat, nphi, precision, reps=5, concurrent=CONCURRENT):
     import torch
     from redondito_b200 import sphp as S
-    P = S.Plan(lmax, nz, nlat=nlat, nphi=nphi, Cz=25, oz=5,
-               precision=S.SPH_MIXED if precision else S.SPH_FP64)
-    times = [(time_candidate(S, torch, P, c, reps), c) for c in candidates(lmax, nz, nlat, nphi, precision)]
-    P.close()
+    plans = [S.Plan(lmax, nz, nlat=nlat, nphi=nphi, Cz=25, oz=5,
+                    precision=S.SPH_MIXED if precision else S.SPH_FP64) for _ in range(concurrent)]
+    times = [(time_candidate(S, torch, plans, c, reps), c) for c in candidates(lmax, nz, nlat, nphi, precision)]
+    for P in plans:
+        P.close()
     t = best(times)
     return dict(t, ms=min(ms for ms, _ in times)), times
 

@@ -39,3 +39,23 @@ def test_shipped_table_covers_the_ensemble_if_present():
                 assert t is not None
                 shape = {k: t[k] for k in ("rows", "ring_pairs", "z_cols")}
                 assert shape in A.candidates(lmax, nz, nlat, 2 * nlat, prec)
+
+
+def test_candidates_are_timed_without_the_table():
+    """Each plan of the timed batch gets the candidate's shape, and the batch
+    is built with tuned=False, so the shipped table cannot replace it."""
+    calls = []
+
+    class FakeS:
+        @staticmethod
+        def set_tiles(plan, rows, ring_pairs, z_cols):
+            calls.append((plan, rows, ring_pairs, z_cols))
+
+        class Batch:
+            def __init__(self, plans, nfields, tuned=True):
+                self.plans, self.nfields, self.tuned = plans, nfields, tuned
+
+    tiles = {"rows": 64, "ring_pairs": 4, "z_cols": 8}
+    B = A.candidate_batch(FakeS, ["p0", "p1", "p2"], tiles)
+    assert B.tuned is False and B.nfields == [1, 1, 1]
+    assert calls == [(p, 64, 4, 8) for p in ("p0", "p1", "p2")]
