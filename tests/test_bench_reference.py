@@ -1,0 +1,25 @@
+"""bench.py's reference arm on the host (no GPU): one JSON line carrying the
+metric, unit and config of the GPU arm, with the CPU timing described in
+cpu_baseline and an e2e block that moves no bytes."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_reference_arm_prints_one_contract_line():
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "0"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    assert d["metric"] == "3D transform pairs/s at lmax=511 nr=256" and d["unit"] == "pairs/s"
+    assert d["value"] > 0 and d["higher_is_better"] is True
+    assert d["config"]["lmax"] == 511 and d["config"]["nz"] == 256 and d["config"]["fields"] == 4
+    cb = d["cpu_baseline"]
+    assert cb["value"] == d["value"] and cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
