@@ -228,6 +228,14 @@ def fp64_peak():
         return None
 
 
+# DRAM bytes per plane of one field of the two-pass forward phi transform
+# (nphi 1536, lmax 511), from one ncu capture over 32 planes of the angular
+# case: pass 1 read 307.4 MB and wrote 119.8 MB, pass 2 read 152.8 MB and
+# wrote 105.8 MB.  The traffic grows in proportion to the planes, so a
+# launch's traffic is this figure times the plane-fields it transforms.
+PHI2_TRAFFIC_PER_PLANE = (307.4 + 119.8 + 152.8 + 105.8) / 32 * 1e6
+
+
 def algorithmic_work(P, mixed):
     """Bytes (HBM kernels) or flops (Legendre) per step for each kernel class:
     compulsory reads + writes at their storage precision (grid FP64; folded
@@ -566,7 +574,11 @@ def main():
         peak = peak_fp64 if (peak_fp64 and args.precision == "fp64") else peaks.get("bf16_tflops", 1590.0)
         unit = "TFLOP/s"
     roofline = {"kernel": dom, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
-                "frac": achieved / peak if peak else None, "traffic": None,
+                "frac": achieved / peak if peak else None,
+                "traffic": (PHI2_TRAFFIC_PER_PLANE * 4 * W["nz"] * args.steps / max(nl, 1)
+                            if dom == "phi_fwd" and prec == S.SPH_MIXED and W["nphi"] == 1536 and W["lmax"] == 511
+                            else None),
+                "traffic_unit": "bytes per launch (ncu capture at 32 planes, scaled by plane-fields)",
                 "launches": nl, "ms_per_launch": tms / max(nl, 1),
                 "peak_source": ("fp64 DMMA probe run live (redondito_b200/peak/fp64_peak.cu)"
                                 if bound == "tensor" and args.precision == "fp64"
