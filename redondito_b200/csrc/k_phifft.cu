@@ -14,6 +14,7 @@
 // (synthesised even/odd sums) and writes both rings of the grid.
 // Lengths 2^a 3^b use the compile-time FFT of fft_ct.cuh; others the
 // runtime engine of fft_engine.cuh.
+#include "fft3.cuh"
 #include "fft_ct.cuh"
 
 namespace {
@@ -243,6 +244,180 @@ __global__ void __launch_bounds__(PTHREADS, 2) phi_inv_kernel(PhiArgs a) {
   }
 }
 
+// ---------------------------------------------------------------- three-step inverse (FP64)
+// Persistent kernel over tiles of NP ring pairs of one (plane, field): the
+// folded coefficients of the tile (lmax + 1 degrees x 2 parities x NP nodes,
+// double2) arrive by cp.async, are assembled into Z(m) of each ring pair
+// (x = ring + i mirror, zero past lmax), and go through the three-step
+// inverse DFT N = A M, M = B C (A = 16): (C') C-point DFTs over kc of
+// Z(ka + A (kb + B kc)), the twiddle W_M^-(c kb); (B') B-point DFTs over kb;
+// (A') the twiddle W_N^-(nm ka) and A-point DFTs over ka, written to the
+// grid rows x[nm + M n1].  One staged tile per CTA; two CTAs per SM where
+// shared memory allows, so that one loads while the other computes.  Shared
+// memory accesses are 16 bytes wide, so a quarter warp must hit distinct
+// 16-byte slots mod 8: the row pitch PR is odd, the ring-pair stride SB is
+// 8/NP (mod 8), and staged rows swap their parity halves every 4/NP rows.
+constexpr int up_mod16(int x, int r) { return x + (((r - x) % 16) + 16) % 16; }
+
+template <int N, int NP>
+struct P3d {
+  static constexpr int A = 16, M = N / A, B = ct::pow2_part_cap16(M), C = M / B;
+  static constexpr int ITEMS_A = NP * M, ITEMS_B = NP * A * C, ITEMS_C = NP * A * B;
+  static constexpr int THREADS = ITEMS_A <= 64 ? 64 : (ITEMS_A + 31) / 32 * 32;
+  static constexpr int PR = M | 1;
+  static constexpr int SB = up_mod16(A * PR, 8 / NP);
+  static constexpr size_t XBYTES = (size_t)NP * SB * sizeof(double2);
+  // transform area, twiddles W_N^e, one staged tile for the largest lmax (N/2 - 1)
+  static constexpr size_t SMEM_MAX = XBYTES + (size_t)N * sizeof(double2) + (size_t)N * NP * sizeof(double2);
+  static constexpr int MINB = SMEM_MAX <= 113 * 1024 && THREADS <= 512 ? 2 : 1;
+  static size_t smem(int lmax) {
+    return XBYTES + (size_t)N * sizeof(double2) + (size_t)(lmax + 1) * 2 * NP * sizeof(double2);
+  }
+  static_assert(N % A == 0 && NP >= 2 && NP <= 8 && XBYTES % 16 == 0, "three-step geometry");
+};
+
+template <int NP>
+__device__ __forceinline__ int stage_swz64(int row) {
+  return ((row * NP) >> 2) & 1;
+}
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+template <int N, int NP>
+__global__ void __launch_bounds__(P3d<N, NP>::THREADS, P3d<N, NP>::MINB) phi3_inv64(PhiArgs a, int ntiles) {
+  using G = P3d<N, NP>;
+  constexpr int A = G::A, M = G::M, B = G::B, C = G::C, T = G::THREADS;
+  extern __shared__ __align__(1024) unsigned char sm3d[];
+  double2* X = reinterpret_cast<double2*>(sm3d);
+  double2* tw = reinterpret_cast<double2*>(sm3d + G::XBYTES);
+  double2* st = tw + N;
+  const int lmax = a.lmax, nlat = a.nlat, ngroups = nlat / 2 / NP;
+  const int t = threadIdx.x;
+  for (int i = t; i < N; i += T) tw[i] = __ldg(a.fd.tw + i);
+  const size_t pstride = (size_t)a.nz * a.ldn;  // parity stride of the folded coefficients
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int g = tile % ngroups, r = tile / ngroups, k = r % a.nz, f = r / a.nz, p0 = g * NP;
+    // the staged tile of the previous iteration was last read before the
+    // barrier that follows step (C'), so it can be refilled here
+    {
+      const double2* gs = a.Gc + (size_t)f * a.Gfield + (size_t)k * a.ldn + p0;
+      const int total = (lmax + 1) * 2 * NP;
+      for (int q = t; q < total; q += T) {
+        const int b = q % NP, rr = q / NP, par = rr & 1, mm = rr >> 1;
+        cp_async16(st + mm * 2 * NP + (par ^ stage_swz64<NP>(mm)) * NP + b, gs + (size_t)rr * pstride + b);
+      }
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
+    __syncthreads();
+    auto zin = [&](int m, int b) {
+      const bool lo = m <= lmax, hi = N - m <= lmax;
+      if (!lo && !hi) return make_double2(0.0, 0.0);
+      const int mm = lo ? m : N - m;
+      const int sw = stage_swz64<NP>(mm);
+      const double2 se = st[mm * 2 * NP + sw * NP + b], so = st[mm * 2 * NP + (1 - sw) * NP + b];
+      const double2 Fi = make_double2(se.x + so.x, se.y + so.y), Fm = make_double2(se.x - so.x, se.y - so.y);
+      if (m == 0) return make_double2(Fi.x, Fm.x);
+      // z = x + i y with x, y the real fields of ring i and its mirror
+      if (lo) return make_double2(Fi.x - Fm.y, Fi.y + Fm.x);
+      return make_double2(Fi.x + Fm.y, -Fi.y + Fm.x);
+    };
+    auto conj = [](double2 z) { return make_double2(z.x, -z.y); };
+    // (C')
+    for (int it = t; it < G::ITEMS_C; it += T) {
+      const int b = it % NP, rr = it / NP, ka = rr % A, kb = rr / A;
+      double2 u[C];
+#pragma unroll
+      for (int kc = 0; kc < C; ++kc) u[kc] = zin(ka + A * (kb + B * kc), b);
+      ct::RD<double2, C, 1>::run(u);
+      double2* row = X + b * G::SB + ka * G::PR + C * kb;
+#pragma unroll
+      for (int c = 0; c < C; ++c) row[c] = (c && kb) ? ct::mul(u[c], conj(tw[A * c * kb])) : u[c];
+    }
+    __syncthreads();
+    if constexpr (B > 1) {  // (B'): stored at column c + C nb
+      for (int it = t; it < G::ITEMS_B; it += T) {
+        const int ka = it % A, rr = it / A, c = rr % C, b = rr / C;
+        double2* row = X + b * G::SB + ka * G::PR + c;
+        double2 w[B];
+#pragma unroll
+        for (int kb = 0; kb < B; ++kb) w[kb] = row[C * kb];
+        ct::RD<double2, B, 1>::run(w);
+#pragma unroll
+        for (int nb = 0; nb < B; ++nb) row[C * nb] = w[nb];
+      }
+      __syncthreads();
+    }
+    // (A')
+    if (t < G::ITEMS_A) {
+      const int b = t % NP, nm = t / NP;
+      double2 v[A];
+      const double2* xi = X + b * G::SB + nm;
+#pragma unroll
+      for (int ka = 0; ka < A; ++ka) v[ka] = ka ? ct::mul(xi[ka * G::PR], conj(tw[nm * ka])) : xi[0];
+      ct::RD<double2, A, 1>::run(v);
+      double* plane = a.gout[f] + (size_t)k * N * nlat;
+      double* pr = plane + p0 + b;
+      double* pm = plane + (nlat - 1 - p0 - b);
+#pragma unroll
+      for (int n1 = 0; n1 < A; ++n1) {
+        const size_t j = (size_t)(nm + M * n1) * nlat;
+        pr[j] = v[n1].x;
+        pm[j] = v[n1].y;
+      }
+    }
+  }
+}
+
+constexpr int PHI3D_UNSUPPORTED = 1000;
+
+template <int N, int NP>
+constexpr bool phi3d_ok() {
+  if constexpr (N % 16 != 0 || N < 48 || NP * (N / 16) > 1024) {
+    return false;
+  } else {
+    return P3d<N, NP>::SMEM_MAX <= 220 * 1024;
+  }
+}
+
+template <int N, int NP>
+int phi3d_run(const sph_plan* p, const PhiArgs& a, int nfields, cudaStream_t st) {
+  if constexpr (!phi3d_ok<N, NP>()) {
+    return PHI3D_UNSUPPORTED;
+  } else {
+    using G = P3d<N, NP>;
+    const size_t smem = G::smem(p->lmax);
+    const long long ntiles = (long long)(p->nlat2 / NP) * p->nz * nfields;
+    if (ntiles == 0) return SPH_OK;
+    if (ntiles > (1ll << 30)) return PHI3D_UNSUPPORTED;
+    auto kern = phi3_inv64<N, NP>;
+    int occ = 0, dev = 0, nsm = 0;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, G::THREADS, smem) != cudaSuccess ||
+        cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      return SPH_ECUDA;
+    const int grid = (int)std::min<long long>(ntiles, (long long)std::max(1, occ) * std::max(1, nsm));
+    kern<<<grid, G::THREADS, smem, st>>>(a, (int)ntiles);
+    SPH_LAUNCH_OK();
+    return SPH_OK;
+  }
+}
+
+// ring pairs per tile: the most that fit, at most the tuned ring_pairs
+template <int N>
+int phi3d_dispatch_n(const sph_plan* p, const PhiArgs& a, int nfields, cudaStream_t st) {
+  const int cap = p->tile_np ? p->tile_np : 8;
+  if (phi3d_ok<N, 8>() && cap >= 8 && p->nlat2 % 8 == 0) return phi3d_run<N, 8>(p, a, nfields, st);
+  if (phi3d_ok<N, 4>() && cap >= 4 && p->nlat2 % 4 == 0) return phi3d_run<N, 4>(p, a, nfields, st);
+  if (phi3d_ok<N, 2>() && cap >= 2 && p->nlat2 % 2 == 0) return phi3d_run<N, 2>(p, a, nfields, st);
+  return PHI3D_UNSUPPORTED;
+}
+
 // ring pairs per CTA: the largest of 8, 4, 2, 1 that divides nlat/2 and
 // keeps NP*nphi <= PMAXC
 int pairs_per_cta(const sph_plan* p) {
@@ -339,6 +514,16 @@ int launch_phi_inv(const sph_plan* p, double* const* grids, int nfields, cudaStr
   dim3 grid(p->nlat2 / a.NP, p->sel_kz ? p->sel_n : p->nz, nfields);
   size_t smem = (size_t)a.NP * seq_stride(p->nphi) * sizeof(double2);
   TimedLaunch tl(p, T_PHI_INV, st);
+  if (!p->sel_kz) {  // the three-step kernel walks every plane
+    int rc = PHI3D_UNSUPPORTED;
+    switch (p->nphi) {
+#define CASE(n) \
+  case n: rc = phi3d_dispatch_n<n>(p, a, nfields, st); break;
+      PHI_SIZES(CASE)
+#undef CASE
+    }
+    if (rc != PHI3D_UNSUPPORTED) return rc;
+  }
   switch (p->nphi) {
 #define CASE(n) \
   case n: return launch_inv_n<n>(a, grid, smem, st);
