@@ -378,8 +378,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm(TcLaunch L) {
     // Per chunk of 16 rows: TMEM -> registers (this lane's component), the
     // vector forms, then through a per-warp staging area so that the global
     // stores of a half-warp cover 16 consecutive rows of one plane.
-    const int q = warp & 3;       // TMEM lane quarter of this warp
-    const int n = 32 * q + lane;  // data column: plane n/2 of the unit, component n&1
+    const int q = warp & 3;  // TMEM lane quarter of this warp
     const bool odd = lane & 1;
     double* stg = reinterpret_cast<double*>(smem + OFF_STG) + (warp - 2) * STG_WORDS;  // [32 lanes][17]
     const int j_out = lane & 15, ph = lane >> 4;  // store phase: row, plane half
@@ -501,10 +500,11 @@ struct Phi32Args {
   int* flag;  // set when a bounded wait gives up (three-step forward)
 };
 
-// Four-step phi FFT geometry (N = N1 N2, NP ring pairs per CTA).  Shared
-// memory: X[b][k1][n2] (forward) or X[b][n2][k1] (inverse) with row pitch
-// = 1 (mod 16) and sequence stride = 4 (mod 16) float2 slots, so that the
-// lanes of a warp (8 sequences x 4 rows) hit 32 distinct slots; the forward
+// Four-step forward phi FFT geometry (N = N1 N2, NP ring pairs per CTA),
+// the register-staged fallback for grids whose rows cannot be staged by TMA
+// or for an odd number of ring pairs.  Shared memory: X[b][k1][n2] with row
+// pitch = 1 (mod 16) and sequence stride = 4 (mod 16) float2 slots, so that
+// the lanes of a warp (8 sequences x 4 rows) hit 32 distinct slots; the
 // kernel overwrites each row k1 with its spectrum Z(k1 + N1 k2), k2 along
 // the row.
 constexpr int up_mod16(int x, int r) { return x + (((r - x) % 16) + 16) % 16; }
@@ -514,9 +514,7 @@ struct P4 {
   // about two work items per thread, so that two CTAs fit an SM's registers
   static constexpr int THREADS = ((NP * (N1 > N2 ? N1 : N2) + 1) / 2 + 31) / 32 * 32;
   static constexpr int PF = up_mod16(N2, 1), SF = up_mod16(N1 * PF, 4);
-  static constexpr int PI = up_mod16(N1, 1), SI = up_mod16(N2 * PI, 4);
   static constexpr size_t SMEM_FWD = (size_t)NP * SF * sizeof(float2);
-  static constexpr size_t SMEM_INV = (size_t)NP * SI * sizeof(float2);
 };
 
 // Forward, four-step: (1) thread (b, n2) loads x[n2 + N2 n1] of ring pair b
@@ -592,72 +590,6 @@ __global__ void __launch_bounds__(P4<N, NP>::THREADS, 2) phi4_fwd32(Phi32Args a)
     store_tile_row<NP>(t0, row + 1, kk0, ei);
     store_tile_row<NP>(t1, row, kk0, orr);
     store_tile_row<NP>(t1, row + 1, kk0, oi);
-  }
-}
-
-// Inverse, four-step: (1) thread (b, k1) assembles Z(k1 + N1 k2) of ring
-// pair b from the folded coefficients (zero past lmax), an N2-point DFT, the
-// twiddle W_N^(-n2 k1), one store to X; (2) thread (b, n2) an N1-point DFT
-// and the grid stores x[n2 + N2 n1] (real part: ring, imaginary: mirror).
-template <int N, int NP>
-__global__ void __launch_bounds__(P4<N, NP>::THREADS, 2) phi4_inv32(Phi32Args a) {
-  using C = P4<N, NP>;
-  constexpr int N1 = C::N1, N2 = C::N2;
-  extern __shared__ float2 sx[];
-  const int nlat = a.nlat, lmax = a.lmax;
-  const int p0 = blockIdx.x * NP, k = blockIdx.y, f = blockIdx.z;
-  const int t = threadIdx.x;
-  for (int it = t; it < NP * N1; it += C::THREADS) {
-    const int b = it % NP, k1 = it / NP;
-    const float2* G = a.G32c + (size_t)f * a.G32field + (size_t)k * a.ldn8 + p0 + b;
-    const size_t mstride = (size_t)2 * a.nz * a.ldn8, pstride = (size_t)a.nz * a.ldn8;
-    float2 w[N2];
-#pragma unroll
-    for (int k2 = 0; k2 < N2; ++k2) {
-      const int m = k1 + N1 * k2;
-      const bool lo = m <= lmax, hi = N - m <= lmax;
-      const int mm = lo ? m : N - m;
-      float2 z = make_float2(0.f, 0.f);
-      if (lo || hi) {
-        const float2 se = __ldg(G + mm * mstride), so = __ldg(G + mm * mstride + pstride);
-        const float2 Fi = make_float2(se.x + so.x, se.y + so.y), Fm = make_float2(se.x - so.x, se.y - so.y);
-        if (m == 0) z = make_float2(Fi.x, Fm.x);
-        else if (lo) z = make_float2(Fi.x - Fm.y, Fi.y + Fm.x);
-        else z = make_float2(Fi.x + Fm.y, -Fi.y + Fm.x);
-      }
-      w[k2] = z;
-    }
-    ct::reg_dif<float2, N2>(w, a.tw2, +1);
-    float2* X = sx + b * C::SI + k1;
-#pragma unroll
-    for (int n2 = 0; n2 < N2; ++n2) {
-      float2 z = w[ct::rev_pos<N2>(n2)];
-      if (n2) {
-        float2 tw = __ldg(a.twN + n2 * k1);
-        tw.y = -tw.y;
-        z = ct::mul(z, tw);
-      }
-      X[n2 * C::PI] = z;
-    }
-  }
-  __syncthreads();
-  for (int it = t; it < NP * N2; it += C::THREADS) {
-    const int b = it % NP, n2 = it / NP;
-    float2 v[N1];
-    const float2* X = sx + b * C::SI + n2 * C::PI;
-#pragma unroll
-    for (int k1 = 0; k1 < N1; ++k1) v[k1] = X[k1];
-    ct::reg_dif<float2, N1>(v, a.tw1, +1);
-    double* plane = a.gout[f] + (size_t)k * N * nlat;
-    double* pr = plane + p0 + b;
-    double* pm = plane + (nlat - 1 - p0 - b);
-#pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) {
-      const size_t j = (size_t)(n2 + N2 * n1) * nlat;
-      const float2 z = v[ct::rev_pos<N1>(n1)];
-      pr[j] = (double)z.x;
-      pm[j] = (double)z.y;
-    }
   }
 }
 
@@ -1684,9 +1616,9 @@ int run_phi4(K kernel, const Phi32Args& a, dim3 grid, int threads, size_t smem, 
 
 template <int N, int NP, bool FWD>
 int phi4_np(const Phi32Args& a, dim3 grid, cudaStream_t st) {
+  static_assert(FWD, "the four-step form is forward only");
   using C = P4<N, NP>;
-  if constexpr (FWD) return run_phi4(phi4_fwd32<N, NP>, a, grid, C::THREADS, C::SMEM_FWD, st);
-  else return run_phi4(phi4_inv32<N, NP>, a, grid, C::THREADS, C::SMEM_INV, st);
+  return run_phi4(phi4_fwd32<N, NP>, a, grid, C::THREADS, C::SMEM_FWD, st);
 }
 
 template <int N, bool FWD>

@@ -21,7 +21,6 @@ namespace {
 
 constexpr int PTHREADS = 512;
 constexpr int PMAXC = 8192;  // NP*nphi complex values per CTA
-constexpr int UNR = 8;       // independent global loads in flight per thread
 
 // sequence stride in shared memory: E(e) = e + e/8 skews short-span passes,
 // and an odd stride spreads the per-ring stores of the load phase over banks
