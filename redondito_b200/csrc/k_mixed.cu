@@ -19,10 +19,12 @@
 //   analysis tiles (K = Gauss nodes); spec_to_tiles writes the synthesis
 //   tiles (K = degrees l of one parity).  The Legendre tables are split on
 //   the host into the same layout.
-// * One persistent CTA per SM walks its work units (item x 64 planes); TMEM
-//   holds two accumulator sets, so the epilogue of a unit overlaps the main
-//   loop of the next.  Vector transforms keep the dP and mPs parts in
-//   separate accumulators and apply the +-i factors in the epilogue.
+// * One persistent CTA per SM walks its work units (item x 64 planes).  For
+//   scalar units TMEM holds two accumulator sets, so the epilogue of a unit
+//   overlaps the main loop of the next.  Vector transforms keep the dP and
+//   mPs parts in separate accumulators (128-column MMAs: the four
+//   accumulators fill TMEM, one set) and apply the +-i factors in the
+//   epilogue.
 //
 // Warp roles of the tensor-core kernel: 0 bulk copies (one lane), 1 TMEM
 // allocation and MMA issue (one lane), 2-5 epilogue (TMEM lane quarters
@@ -49,7 +51,7 @@ constexpr int NPIECE = 3;                           // bf16 pieces per value
 constexpr int PIECE_HALVES = MCOLS * TK;            // 4096 (8 KB)
 constexpr int TILE_HALVES = NPIECE * PIECE_HALVES;  // one data tile (24 KB)
 constexpr int NR_S = 128;                           // MMA N of scalar items
-constexpr int NR_V = 64;                            // MMA N of vector items (two parts)
+constexpr int NR_V = 128;                           // MMA N of vector items (two parts)
 constexpr int A_BYTES = TILE_HALVES * 2;
 constexpr int B_BYTES = NPIECE * NR_S * TK * 2;     // 24 KB
 constexpr int STAGES = 4;
@@ -258,6 +260,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm(TcLaunch L) {
 
   constexpr bool analysis = (MODE == ANA_S || MODE == ANA_V);
   constexpr bool vector = (MODE == ANA_V || MODE == SYN_V);
+  // TMEM columns of one accumulator set: scalar modes main @0 and cross @128
+  // (two sets, so the epilogue of one unit overlaps the MMAs of the next);
+  // vector modes (128-column MMAs, two parts) main/cross @0/128 and
+  // @256/384 -- all 512 columns, one set
+  constexpr int NACC = vector ? 1 : 2;
+  constexpr uint32_t PART = vector ? 256u : 128u, CROSS = 128u;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   // once any CTA of the launch's owner has given up a wait, later launches do no work
@@ -324,8 +332,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm(TcLaunch L) {
         Unit<G> w;
         w.load(L, u);
         const TcItem& it = w.it;
-        const int buf = uc & 1;
-        if (uc >= 2 && !tc05::mbar_wait(&accEmpty[buf], ((uc >> 1) - 1) & 1)) {
+        const int buf = uc % NACC, use = uc / NACC;
+        if (use >= 1 && !tc05::mbar_wait(&accEmpty[buf], (use - 1) & 1)) {
           ok = false;
           break;
         }
@@ -343,8 +351,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm(TcLaunch L) {
           tc05::fence_after();
           const int part = (vector && kt >= it.nk1) ? 1 : 0;
           const bool first = kt == (part ? it.nk1 : 0);
-          const uint32_t tmain = tacc + (uint32_t)part * 128;
-          const uint32_t tcross = tmain + (vector ? 64u : 128u);
+          const uint32_t tmain = tacc + (uint32_t)part * PART;
+          const uint32_t tcross = tmain + CROSS;
           unsigned char* At = smem + s * STAGE_BYTES;
           unsigned char* Bt = At + A_BYTES;
 #pragma unroll
@@ -388,8 +396,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm(TcLaunch L) {
       w.load(L, u);
       const TcArgs& a = w.a;
       const TcItem& it = w.it;
-      const int buf = uc & 1;
-      bool ok = !*abort_flag && tc05::mbar_wait(&accFull[buf], (uc >> 1) & 1);
+      const int buf = uc % NACC, use = uc / NACC;
+      bool ok = !*abort_flag && tc05::mbar_wait(&accFull[buf], use & 1);
       ok = __all_sync(0xffffffffu, ok);
       if (!ok) {
         fail();
@@ -405,11 +413,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm(TcLaunch L) {
         uint32_t v0[16], x0[16], v1[16], x1[16];
         if (have0) {
           tc05::tmem_ld16_nw(ta + c, v0);
-          tc05::tmem_ld16_nw(ta + (vector ? 64 : 128) + c, x0);
+          tc05::tmem_ld16_nw(ta + CROSS + c, x0);
         }
         if (have1) {
-          tc05::tmem_ld16_nw(ta + 128 + c, v1);
-          tc05::tmem_ld16_nw(ta + 192 + c, x1);
+          tc05::tmem_ld16_nw(ta + PART + c, v1);
+          tc05::tmem_ld16_nw(ta + PART + CROSS + c, x1);
         }
         tc05::tmem_wait_ld();
         tc05::tmem_regs(v0);
