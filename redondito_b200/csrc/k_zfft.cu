@@ -60,6 +60,16 @@ __device__ __forceinline__ void cp_async16z(void* dst, const void* src, int src_
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
 }
 
+// v / nz: a multiplication by the exact reciprocal when nz is a power of
+// two (the same result bit for bit, without the cost of a double division)
+__device__ __forceinline__ double2 div_nz(double2 v, int nz) {
+  if ((nz & (nz - 1)) == 0) {
+    const double r = 1.0 / (double)nz;
+    return make_double2(v.x * r, v.y * r);
+  }
+  return make_double2(v.x / (double)nz, v.y / (double)nz);
+}
+
 template <int MODE, int CTN>
 __global__ void __launch_bounds__(ZTHREADS) zfft_kernel(ZArgs a) {
   extern __shared__ double2 sm[];
@@ -126,13 +136,10 @@ __global__ void __launch_bounds__(ZTHREADS) zfft_kernel(ZArgs a) {
 
   if (MODE == Z_DERIV || MODE == Z_FILTER || MODE == Z_DLR) {
     // spectral multiply in place (frequency k sits at row rev[k]), then back
-    const double rn = (double)nz;
     for (int idx = tid; idx < nz * LB; idx += ZTHREADS) {
       int k = idx / LB, c = idx - k * LB;
       int o = __ldg(rev + k) * LB + c;
-      double2 v = sm[o];
-      v.x = v.x / rn;
-      v.y = v.y / rn;
+      double2 v = div_nz(sm[o], nz);
       if (MODE == Z_FILTER) v = cscale(v, a.filt[k]);
       else v = cmul(a.kfac[k], v);
       sm[o] = v;
@@ -148,9 +155,7 @@ __global__ void __launch_bounds__(ZTHREADS) zfft_kernel(ZArgs a) {
     if (lm >= nlm) continue;
     double2 v;
     if (MODE == Z_FWD) {
-      v = sm[__ldg(rev + r) * LB + c];
-      v.x = v.x / (double)nz;
-      v.y = v.y / (double)nz;
+      v = div_nz(sm[__ldg(rev + r) * LB + c], nz);
     } else {
       v = sm[idx];
     }
