@@ -27,8 +27,9 @@
 //   epilogue.
 //
 // Warp roles of the tensor-core kernel: 0 bulk copies (one lane), 1 TMEM
-// allocation and MMA issue (one lane), 2-5 epilogue (TMEM lane quarters
-// 2, 3, 0, 1).
+// allocation and MMA issue (one lane), 2-9 epilogue (TMEM lane quarters
+// 2, 3, 0, 1, twice; the two warps of a quarter take alternate 16-column
+// chunks).
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
@@ -58,11 +59,12 @@ constexpr int STAGES = 4;
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int STG_WORDS = 32 * 17;                  // epilogue staging per warp (doubles)
 constexpr int OFF_STG = STAGES * STAGE_BYTES;
-constexpr int OFF_BAR = OFF_STG + 4 * STG_WORDS * 8;
+constexpr int NEPI_WARPS = 8;                       // epilogue warps: two per TMEM lane quarter
+constexpr int OFF_BAR = OFF_STG + NEPI_WARPS * STG_WORDS * 8;
 constexpr int NBARS = 2 * STAGES + 2 + 2 + 1;
 constexpr int TC_SMEM = OFF_BAR + NBARS * 8 + 16;
-constexpr int TC_THREADS = 6 * 32;
-constexpr int NEPI = 128;                           // epilogue threads
+constexpr int TC_THREADS = (2 + NEPI_WARPS) * 32;
+constexpr int NEPI = NEPI_WARPS * 32;                // epilogue threads
 constexpr int TMEM_COLS = 512;                      // two accumulator sets of 256 columns
 
 enum { ANA_S = 0, ANA_V = 1, SYN_S = 2, SYN_V = 3 };
@@ -409,7 +411,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm(TcLaunch L) {
       const uint32_t ta = tbase + (uint32_t)buf * 256 + ((uint32_t)(32 * q) << 16);
       const bool have0 = vector ? it.nk1 > 0 : it.nk > 0;
       const bool have1 = vector && it.nk > it.nk1;
-      for (int c = 0; c < it.nr; c += 16) {
+      for (int c = 16 * ((warp - 2) / 4); c < it.nr; c += 32) {  // the quarter's two warps alternate chunks
         uint32_t v0[16], x0[16], v1[16], x1[16];
         if (have0) {
           tc05::tmem_ld16_nw(ta + c, v0);
