@@ -22,8 +22,12 @@ transform.  Every buffer is larger than L2 (126 MB), so no flush is needed.
   roofline: the kernel class with the largest share of the timed region,
             achieved = algorithmic bytes (or flops) / its measured time
   cpu_baseline: the CPU oracle (a C++ restatement of the reference's
-            arithmetic; the Fortran reference cannot be built here) on a
-            bounded sample, extrapolated to the full pair
+            arithmetic; the Fortran reference cannot be built here) timed
+            on half of the pair (8 of its 16 slices, see CpuPair)
+  fp64    : the FP64 form on the same state: pairs/s, per-kernel rooflines,
+            e2e
+  c1, c2  : configs 1 and 2 on the GPU and the CPU oracle (see config1,
+            config2)
 
 Multi-GPU: one process per GPU (torchrun); each rank runs its own replica
 of the workload (a single problem does not shard: the reference's only
@@ -65,6 +69,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-c4", action="store_true", help="skip the 64-problem batched ensemble")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop measurement")
+    ap.add_argument("--no-configs", action="store_true", help="skip the config 1 and config 2 blocks")
     ap.add_argument("--case", default="c3", choices=sorted(CASES),
                     help="c3: the benchmark workload; small, angular: profiling cases for ncu")
     a = ap.parse_args()
@@ -73,56 +78,94 @@ def parse():
 
 
 # ---------------------------------------------------------------- CPU side
-def cpu_pairs_per_s(threads=None):
-    """The oracle's pair time on a bounded sample: the angular transforms of
-    all four fields on 2 and on 4 planes (a + b*nz fit, extrapolated to 256
-    planes) plus the z transforms of one full field (x4)."""
-    from oracle import oracle as O
-    if threads:
-        O.set_threads(threads)
-    nthreads = O.lib().orc_get_threads()
-    rng = np.random.default_rng(SEED)
-    times = {}
-    for nzs in (2, 4):
-        P = O.Plan(W["lmax"], nzs, nlat=W["nlat"], nphi=W["nphi"])
-        a = (rng.normal(size=(nzs, P.nlm)) + 1j * rng.normal(size=(nzs, P.nlm))) * (P.ell + 1.0) ** -2.5
-        a[:, P.emm == 0] = a[:, P.emm == 0].real
-        s0 = a.copy()
-        s0[:, 0] = 0
-        t0 = time.perf_counter()
-        g = P.sh_synthesis(a)
-        P.sh_analysis(g)
-        v = P.qst_synthesis(a, s0, s0)
-        P.qst_analysis(*v)
-        times[nzs] = time.perf_counter() - t0
-    t_sht = times[2] + (W["nz"] - 2) * (times[4] - times[2]) / 2.0
-    Pz = O.Plan(W["lmax"], W["nz"], nlat=W["nlat"], nphi=W["nphi"], C=W["Cz"], d=W["oz"],
-                rint=W["rint"], rext=W["rext"])
-    f = rng.normal(size=(W["nz"], Pz.nlm)) + 1j * rng.normal(size=(W["nz"], Pz.nlm))
+PAIR_SLICES = 16
+
+
+class CpuPair:
+    """The oracle's pair on the benchmark workload, cut into PAIR_SLICES equal
+    slices.  Slice i runs, for all four fields, the z inverse of the lm
+    columns [i nlm/S, (i+1) nlm/S), the angular synthesis (scalar and
+    vector) and analysis of the planes [i nz/S, (i+1) nz/S), and the z
+    forward (with the FC-Gram continuation) of the same columns.  The planes
+    of the angular transforms are independent of one another and so are the
+    columns of the z transforms, so S consecutive slices do exactly the
+    arithmetic of one pair; nothing is extrapolated."""
+
+    def __init__(self, threads=None):
+        from oracle import oracle as O
+        if threads:
+            O.set_threads(threads)
+        self.threads = O.lib().orc_get_threads()
+        S = PAIR_SLICES
+        lmax, nz = W["lmax"], W["nz"]
+        assert nz % S == 0
+        self.Pa = O.Plan(lmax, nz // S, nlat=W["nlat"], nphi=W["nphi"])
+        self.Pz = O.Plan(lmax, nz, nlat=W["nlat"], nphi=W["nphi"], C=W["Cz"], d=W["oz"],
+                         rint=W["rint"], rext=W["rext"])
+        nlm = self.Pa.nlm
+        self.cols = [(i * nlm) // S for i in range(S + 1)]
+        rng = np.random.default_rng(SEED)
+        amp = (self.Pa.ell + 1.0) ** -2.5
+        self.spec = []
+        for f in range(4):
+            a = (rng.normal(size=(nz // S, nlm)) + 1j * rng.normal(size=(nz // S, nlm))) * amp
+            a[:, self.Pa.emm == 0] = a[:, self.Pa.emm == 0].real
+            if f >= 2:
+                a[:, 0] = 0
+            self.spec.append(a)
+        self.zin = [rng.normal(size=(nz, nlm)) + 1j * rng.normal(size=(nz, nlm)) for _ in range(4)]
+
+    def step(self, i):
+        Pa, Pz = self.Pa, self.Pz
+        c0, c1 = self.cols[i % PAIR_SLICES], self.cols[i % PAIR_SLICES + 1]
+        zs = [Pz.z_inverse_cols(x[:, c0:c1]) for x in self.zin]
+        g = Pa.sh_synthesis(self.spec[0])
+        v = Pa.qst_synthesis(self.spec[1], self.spec[2], self.spec[3])
+        Pa.sh_analysis(g)
+        Pa.qst_analysis(*v)
+        for x in zs:
+            Pz.z_forward_cols(x)
+
+    def sample(self):
+        return (f"the oracle on all {self.threads} host threads, all 4 fields; a step is 1/{PAIR_SLICES} "
+                f"of the pair: angular synthesis + analysis of {W['nz'] // PAIR_SLICES} of the {W['nz']} "
+                f"planes and z inverse + forward of {self.cols[1]} of the {self.Pa.nlm} lm columns; "
+                f"{PAIR_SLICES} consecutive steps cover one whole pair")
+
+
+def cpu_pairs_per_s(nslices=PAIR_SLICES // 2, threads=None):
+    """The oracle's pair throughput timed on `nslices` consecutive slices
+    (half a pair by default, 10-20 s on the box's cores)."""
+    cp = CpuPair(threads)
+    cp.step(0)  # warm-up (page-in, thread pool)
     t0 = time.perf_counter()
-    Pz.z_inverse(Pz.z_forward(f))
-    t_z = time.perf_counter() - t0
-    t_pair = t_sht + 4 * t_z
-    sample = ("oracle on all 4 fields: angular transforms on 2 and 4 planes "
-              f"({times[2]:.2f} s, {times[4]:.2f} s) extrapolated to 256 planes, "
-              f"plus one full z forward+inverse x4 ({t_z:.2f} s)")
-    return 1.0 / t_pair, nthreads, sample
+    for i in range(nslices):
+        cp.step(i)
+    dt = time.perf_counter() - t0
+    return (nslices / PAIR_SLICES) / dt, cp.threads, cp.sample() + f"; timed: {nslices} steps in {dt:.1f} s"
 
 
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    v, cores, sample = cpu_pairs_per_s()
+    cp = CpuPair()
+    for i in range(args.warmup):
+        cp.step(i)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        cp.step(i)
+    dt = time.perf_counter() - t0
+    v = (args.steps / PAIR_SLICES) / dt
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "pairs/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "scalar + vector field, lmax=511, 768x1536, nz=256, FC-Gram C=25 d=5",
-                   **W, "fields": 4},
-        "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": cores, "kind": "port",
-                         "sample": sample},
+                   **W, "fields": 4, "step": f"1/{PAIR_SLICES} of the pair (see cpu_baseline.sample)"},
+        "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": cp.threads, "kind": "port",
+                         "sample": cp.sample()},
         "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference (Fortran + SHTns + FFTW + MPI) cannot be built here; "
                 "this is its C++ restatement (the oracle) on the host cores",
@@ -426,6 +469,183 @@ def per_output_errors(S, Pm, Pd, st0, torch):
     return rel, mx
 
 
+def e2e_pairs(S, P, st, grids, steps, stream, torch, dist, world):
+    """The pair through the C ABI with host buffers: every step copies its four
+    spectral fields from pinned host memory, runs the pair and copies the
+    results back.  Steps are pipelined the way a streaming caller would run
+    them: three device state sets, uploads on one stream, the pair on the
+    compute stream, downloads on a third, so that the upload of step i+1 and
+    the download of step i-1 overlap the pair of step i (the two copy
+    directions use separate engines)."""
+    NBUF = 3
+    host_in = [x.cpu().pin_memory() for x in st]
+    host_out = [[torch.empty_like(h).pin_memory() for h in host_in] for _ in range(NBUF)]
+    bufs = [st] + [[x.clone() for x in st] for _ in range(NBUF - 1)]
+    nbytes = sum(h.numel() * h.element_size() for h in host_in)
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    ev = lambda: torch.cuda.Event()
+    in_done, comp_done, out_done = [ev() for _ in range(NBUF)], [ev() for _ in range(NBUF)], [ev() for _ in range(NBUF)]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0.record(stream)
+    s_in.wait_event(e0)
+    s_out.wait_event(e0)
+    for i in range(steps):
+        b = i % NBUF
+        d = bufs[b]
+        if i >= NBUF:
+            s_in.wait_event(out_done[b])  # this state set's previous results are on the host
+        with torch.cuda.stream(s_in):
+            for h, x in zip(host_in, d):
+                x.copy_(h, non_blocking=True)
+        in_done[b].record(s_in)
+        stream.wait_event(in_done[b])
+        with torch.cuda.stream(stream):
+            pair(S, P, d, grids)
+        comp_done[b].record(stream)
+        s_out.wait_event(comp_done[b])
+        with torch.cuda.stream(s_out):
+            for h, x in zip(host_out[b], d):
+                h.copy_(x, non_blocking=True)
+        out_done[b].record(s_out)
+    for b in range(min(NBUF, steps)):
+        stream.wait_event(out_done[b])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ems = _max_over_ranks(torch, dist, world, e0.elapsed_time(e1))
+    del bufs, host_out
+    return {"value": world * steps / (ems * 1e-3), "unit": "pairs/s",
+            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+            "pipeline": f"{NBUF} state sets; upload, pair and download of neighbouring steps overlap"}
+
+
+def kernel_rooflines(stage, work, steps, peaks, peak_fp64, fp64):
+    """Per kernel class: algorithmic bytes (or useful flops) per step times the
+    steps, over the class's event-timed duration; against the measured HBM
+    copy bandwidth, or the tensor peak of the form (bf16 from the measured
+    cuBLAS GEMM, FP64 from the DMMA probe run live)."""
+    out = {}
+    for c, (bound, per_step) in work.items():
+        tms, nl = stage.get(c, (0.0, 0))
+        if not nl or not per_step:
+            continue
+        if bound == "hbm":
+            ach, peak, unit = per_step * steps / (tms * 1e-3) / 1e9, peaks.get("hbm_gbs", 6650.0), "GB/s"
+        else:
+            ach = per_step * steps / (tms * 1e-3) / 1e12
+            peak, unit = (peak_fp64, "TFLOP/s") if fp64 else (peaks.get("bf16_tflops", 1590.0), "TFLOP/s")
+        out[c] = {"bound": bound, "achieved": ach, "peak": peak, "unit": unit,
+                  "frac": ach / peak if peak else None, "launches": nl, "ms_per_launch": tms / nl,
+                  "ms_per_step": tms / steps}
+    return out
+
+
+def c1_seeded(P, rng):
+    """Config 1 input: a_lm(r) = N(0,1)(l+1)^-2 (real for m = 0) times
+    sum_k c_k cos(k pi (r - 0.35)/0.65), c_k ~ N(0,1)/(k+1)^2, k <= 8."""
+    a = (rng.normal(size=P.nlm) + 1j * rng.normal(size=P.nlm)) * (P.ell + 1.0) ** -2.0
+    a[P.emm == 0] = a[P.emm == 0].real
+    c = rng.normal(size=9) / (np.arange(9) + 1.0) ** 2
+    z = P.z
+    prof = sum(c[k] * np.cos(k * np.pi * (z - 0.35) / 0.65) for k in range(9))
+    return prof[:, None] * a[None, :]
+
+
+def config1(S, torch, iters=200):
+    """Config 1 (lmax 31, 48 x 96, r in [0.35, 1], C = 25, d = 5, nz = 33 and
+    58): synthesis -> analysis -> derivr(., 1, 'r'), FP64, on the GPU (device
+    time per chain over `iters` chains) and on the CPU oracle (all host
+    threads), with the GPU outputs' relative L2 against the oracle's."""
+    from oracle import oracle as O
+    out = {}
+    for nz in (33, 58):
+        Po = O.Plan(31, nz, nlat=48, nphi=96, C=25, d=5, rint=0.35, rext=1.0)
+        spec = c1_seeded(Po, np.random.default_rng(20261203 + 1))
+        t0 = time.perf_counter()
+        n_cpu = 0
+        while n_cpu < 5 or time.perf_counter() - t0 < 1.0:
+            g_ref = Po.sh_synthesis(spec)
+            s_ref = Po.sh_analysis(g_ref)
+            d_ref = Po.derivr(s_ref, 1)
+            n_cpu += 1
+        cpu_ms = 1e3 * (time.perf_counter() - t0) / n_cpu
+        G = S.Plan(31, nz, nlat=48, nphi=96, Cz=25, oz=5, rint=0.35, rext=1.0)
+        a = torch.from_numpy(spec).cuda()
+        g, s, d = G.new_grid(), G.new_spec(), G.new_spec()
+
+        def chain():
+            S.fftp2d_complex_to_real_xy(G, a, g)
+            S.fftp2d_real_to_complex_xy(G, g, s)
+            S.derivr(G, s, d, 1, "r")
+        for _ in range(20):
+            chain()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(iters):
+            chain()
+        e1.record()
+        torch.cuda.synchronize()
+        gpu_ms = e0.elapsed_time(e1) / iters
+        rel = lambda x, r: float(np.linalg.norm((x.cpu().numpy() - r).ravel()) / np.linalg.norm(r.ravel()))
+        out[str(nz)] = {"gpu_ms_per_chain": gpu_ms, "cpu_ms_per_chain": cpu_ms, "cpu_over_gpu": cpu_ms / gpu_ms,
+                        "rel_l2_vs_oracle": {"grid": rel(g, g_ref), "spec": rel(s, s_ref), "derivr": rel(d, d_ref)}}
+        G.close()
+    out["chain"] = "synthesis -> analysis -> derivr(.,1,'r'), FP64, one chain after another"
+    return out
+
+
+def config2(S, torch, cpu=True, reps=5):
+    """Config 2 (lmax 255, 384 x 768, nz 128, C = 25, d = 5, r in [0.35, 1]):
+    the vector nonlinear step from a no-slip state (Z, W ~ N(0,1)(l+1)^-3
+    times a smooth radial profile, phi = D_l W, v_imposebc), FP64 and mixed
+    on the GPU (device time per step over `reps` steps), the oracle on the
+    host cores, and the GPU right-hand sides against the oracle's."""
+    from oracle import oracle as O
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from tests._helpers import random_spec
+    Po = O.Plan(255, 128, nlat=384, nphi=768, C=25, d=5, rint=0.35, rext=1.0)
+    Po.bc_setup()
+    rng = np.random.default_rng(20261203 + 2)
+    Z0, W0 = random_spec(Po, rng, power=3.0), random_spec(Po, rng, power=3.0)
+    Z, F, Wp = Po.imposebc(Z0, Po.dlr(W0))
+    out = {"work": "one NL right-hand side (2 vector syntheses, 1 vector analysis, radial derivatives, "
+                   "energy) from a no-slip state", "nu": 1e-3}
+    ref = None
+    if cpu:
+        t0 = time.perf_counter()
+        ref = Po.nl_rhs(Z, Wp, F, 1e-3)
+        out["cpu_ms_per_step"] = 1e3 * (time.perf_counter() - t0)
+        out["cpu_threads"] = O.lib().orc_get_threads()
+    for name, prec in (("fp64", S.SPH_FP64), ("mixed", S.SPH_MIXED)):
+        G = S.Plan(255, 128, nlat=384, nphi=768, Cz=25, oz=5, rint=0.35, rext=1.0, precision=prec)
+        S.setup_bc(G)
+        z, w, f = (torch.from_numpy(x).cuda() for x in (Z, Wp, F))
+        rz, rf = G.new_spec(), G.new_spec()
+        e = S.nl_rhs(G, z, w, f, 1e-3, rz, rf)
+        S.nl_rhs(G, z, w, f, 1e-3, rz, rf)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            S.nl_rhs(G, z, w, f, 1e-3, rz, rf)
+        e1.record()
+        torch.cuda.synchronize()
+        blk = {"gpu_ms_per_step": e0.elapsed_time(e1) / reps}
+        if ref is not None:
+            rel = lambda x, r: float(np.linalg.norm((x.cpu().numpy() - r).ravel()) / np.linalg.norm(r.ravel()))
+            blk["rel_l2_vs_oracle"] = {"rhs_z": rel(rz, ref[0]), "rhs_phi": rel(rf, ref[1]),
+                                       "energy": abs(e - ref[2]) / ref[2]}
+            blk["cpu_over_gpu"] = out["cpu_ms_per_step"] / blk["gpu_ms_per_step"]
+        out[name] = blk
+        S.plan_status(G)
+        G.close()
+        torch.cuda.empty_cache()
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -486,63 +706,12 @@ def main():
     # a pair on a forward-transformed state is the identity up to rounding
     rt = [float((torch.linalg.vector_norm(x - r) / torch.linalg.vector_norm(r)).item()) for x, r in zip(st, st0)]
 
-    # e2e through the C ABI with host buffers: every step copies its four
-    # spectral fields from pinned host memory, runs the pair and copies the
-    # results back.  Steps are pipelined the way a streaming caller would run
-    # them: three device state sets, uploads on one stream, the pair on the
-    # compute stream, downloads on a third, so that the upload of step i+1 and
-    # the download of step i-1 overlap the pair of step i (the two copy
-    # directions use separate engines).
     e2e = None
     if not args.no_e2e:
-        NBUF = 3
-        host_in = [x.cpu().pin_memory() for x in st]
-        host_out = [[torch.empty_like(h).pin_memory() for h in host_in] for _ in range(NBUF)]
-        bufs = [st] + [[x.clone() for x in st] for _ in range(NBUF - 1)]
-        nbytes = sum(h.numel() * h.element_size() for h in host_in)
-        s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
-        ev = lambda: torch.cuda.Event()
-        in_done, comp_done, out_done = [ev() for _ in range(NBUF)], [ev() for _ in range(NBUF)], [ev() for _ in range(NBUF)]
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-        e0.record(stream)
-        s_in.wait_event(e0)
-        s_out.wait_event(e0)
-        for i in range(args.steps):
-            b = i % NBUF
-            d = bufs[b]
-            if i >= NBUF:
-                s_in.wait_event(out_done[b])  # this state set's previous results are on the host
-            with torch.cuda.stream(s_in):
-                for h, x in zip(host_in, d):
-                    x.copy_(h, non_blocking=True)
-            in_done[b].record(s_in)
-            stream.wait_event(in_done[b])
-            with torch.cuda.stream(stream):
-                pair(S, P, d, grids)
-            comp_done[b].record(stream)
-            s_out.wait_event(comp_done[b])
-            with torch.cuda.stream(s_out):
-                for h, x in zip(host_out[b], d):
-                    h.copy_(x, non_blocking=True)
-            out_done[b].record(s_out)
-        for b in range(min(NBUF, args.steps)):
-            stream.wait_event(out_done[b])
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ems = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([ems], device=P.device)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
-        e2e = {"value": world * args.steps / (ems * 1e-3), "unit": "pairs/s",
-               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-               "pipeline": f"{NBUF} state sets; upload, pair and download of neighbouring steps overlap"}
-        del bufs, host_out
+        e2e = e2e_pairs(S, P, st, grids, args.steps, stream, torch, dist, world)
 
-    # the FP64 form on the same state: its time, and the mixed form's error per output
+    # the FP64 form on the same state: its time, per-kernel rooflines and e2e,
+    # and the mixed form's error per output against it
     fp64 = None
     errors = None
     if prec == S.SPH_MIXED and not args.no_fp64:
@@ -551,17 +720,28 @@ def main():
         gd = [Pd.new_grid() for _ in range(4)]
         for _ in range(max(1, args.warmup)):
             pair(S, Pd, std, gd)
+        S.timer_reset(Pd)
+        S.timer_enable(Pd, True)
         msd = time_pairs(S, Pd, std, gd, args.steps, stream, torch, dist, world)
-        fp64 = {"value": world * args.steps / (msd * 1e-3), "unit": "pairs/s", "ms_per_step": msd / args.steps}
+        S.timer_enable(Pd, False)
+        stage_d = S.timer_read(Pd)
+        fp64 = {"value": world * args.steps / (msd * 1e-3), "unit": "pairs/s", "ms_per_step": msd / args.steps,
+                "roofline": kernel_rooflines(stage_d, algorithmic_work(Pd, False), args.steps, peaks, peak_fp64,
+                                             True),
+                "stage_share": {c: round(stage_d[c][0] / max(msd, 1e-9), 4) for c in stage_d if stage_d[c][1]},
+                "gpu_launches": sum(v[1] for v in stage_d.values())}
+        if not args.no_e2e:
+            fp64["e2e"] = e2e_pairs(S, Pd, std, gd, args.steps, stream, torch, dist, world)
         del std, gd
         rel, mx = per_output_errors(S, P, Pd, st0, torch)
         errors = {"rel_l2_vs_fp64": rel, "max_abs_vs_fp64": mx,
-                  "note": "each transform on the same inputs in both forms; the FP64 form matches "
-                          "the CPU oracle to 1e-12 (tests/test_gpu_parity.py)"}
+                  "note": "each transform on the same inputs in both forms; both forms are checked against "
+                          "the CPU oracle at this size (tests/test_gpu_fullsize.py)"}
         Pd.close()
 
-    # roofline of the dominant kernel class
+    # roofline of the dominant kernel class, and every class's
     work = algorithmic_work(P, prec == S.SPH_MIXED)
+    per_class = kernel_rooflines(stage, work, args.steps, peaks, peak_fp64, args.precision == "fp64")
     dom = max(stage, key=lambda c: stage[c][0])
     bound, per_step = work[dom]
     tms, nl = stage[dom]
@@ -601,6 +781,11 @@ def main():
         torch.cuda.empty_cache()
         c5 = serving_c5(S, torch, rank=rank, world=world, dist=dist)
 
+    c1 = c2 = None
+    if world == 1 and args.case == "c3" and not args.no_configs:
+        c1 = config1(S, torch)
+        c2 = config2(S, torch, cpu=not args.no_cpu)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, cores, sample = cpu_pairs_per_s()
@@ -624,10 +809,13 @@ def main():
         "e2e": e2e,
         "gpu_launches": launches,
         "roofline": roofline,
+        "kernels": per_class,
         "stage_share": shares,
         "fp64": fp64,
         "speedup_vs_fp64": (value / fp64["value"]) if fp64 else None,
         "accuracy": errors,
+        "c1": c1,
+        "c2": c2,
         "batched_c4": c4,
         "serve_c5": c5,
         "serve_p99_ms": c5["mixed"]["p99_ms"] if c5 else None,

@@ -55,10 +55,16 @@ typedef struct sph_plan sph_plan;
  *   dir          : host pointer, Cz x oz column-major continuation operator
  *                  dir = A.Q^T (see sph_fcgram_load_tables); NULL if Cz == 0
  *   precision    : SPH_FP64, or SPH_MIXED: Legendre contractions on the
- *                  tensor cores as three fp16 products of power-of-two
- *                  scaled hi/lo splits with fp32 accumulation, phi FFTs in
- *                  fp32 (relative L2 error ~1e-7); z transforms and
- *                  operators stay FP64.  SPH_MIXED needs nphi = 3*2^a,
+ *                  tensor cores (tcgen05, fp32 accumulation in TMEM) with
+ *                  every operand split into three bf16 pieces
+ *                  (hi + mid + lo, 8 significant bits each) and the six
+ *                  piece products of order <= 2 kept (about 24 bits); the
+ *                  hi*hi products and the five smaller ones accumulate
+ *                  separately and are added in FP64.  phi FFTs in fp32
+ *                  with twiddles derived in FP64 (relative L2 error
+ *                  ~1e-7 per transform, <= 4e-7 at lmax 511); z
+ *                  transforms, the FC-Gram continuation and operators
+ *                  stay FP64.  SPH_MIXED needs nphi = 3*2^a,
  *                  12 <= nphi <= 6144.
  * Allocates the plan's device tables and scratch with cudaMalloc on the
  * current device. */
@@ -81,6 +87,32 @@ int sph_plan_sizes(const sph_plan* plan, int* nlm, long long* grid_elems, long l
  * theta(nlat), Gauss weights(nlat), phi(nphi), z(nz), kz(nz), ell(nlm), emm(nlm). */
 int sph_grid(const sph_plan* plan, double* theta, double* weights, double* phi, double* z,
              double* kz, int* ell, int* emm);
+
+/* The caller's slab: the bounds the reference keeps in module mpivars
+ * (ksta, kend, lmsta, lmend; src/sphp/sphp_mod.F90:68-79), computed there
+ * by range (src/sphp/sphp_sca.F90:596-626) for each MPI rank; here 0-based:
+ * planes [k0, k0 + nplanes) and lm columns [lm0, lm0 + nlm_local).  After
+ * this call, on this plan:
+ *   - the 2D transforms (sph_fftp2d_*) take physical arrays of nplanes
+ *     planes, (nlat, nphi, nplanes), and spectral arrays (nlm, nplanes):
+ *     the reference's per-rank in(nlat,nphi,ksta:kend) and carr1(nlm,ksta:kend)
+ *     before its slab transpose (fftp3d_redist_k_to_lm, which a multi-rank
+ *     caller keeps doing itself), src/sphp-gpu/sphp_sca.F90:771-853;
+ *   - the z transforms, the operators and the boundary take (nlm_local, nz)
+ *     arrays, the reference's (lmsta:lmend, nz) (sphp_sca.F90:332-397,
+ *     pseudospec_hd.f90, boundary_mod.f90); prodvec and saxpby_r take the
+ *     nplanes planes (only planes k0 + k < nz - Cz are physical);
+ *   - the 3D transforms, the NL step, RK3 and batches need the whole field
+ *     (they would need the slab transpose) and return SPH_EINVAL otherwise.
+ * sph_plan_set_slab(p, 0, nz, 0, nlm) restores the whole field (the
+ * default).  Results on a slab equal the whole-field results restricted to
+ * it.  SPH_EINVAL for an empty or out-of-range slab. */
+int sph_plan_set_slab(sph_plan* plan, int k0, int nplanes, int lm0, int nlm_local);
+
+/* range (src/sphp/sphp_sca.F90:596-626): the part [ista, iend] (inclusive)
+ * of [n1, n2] that rank irank of nprocs owns; the first mod(n, nprocs)
+ * ranks take one element more. */
+int sph_range(int n1, int n2, int nprocs, int irank, int* ista, int* iend);
 
 /* ---------------------------------------------------------------- transforms */
 
@@ -217,6 +249,43 @@ int sph_nl_rhs(sph_plan* plan, const double* Z, const double* W, const double* p
 int sph_rk3_step(sph_plan* plan, double* Z, double* W, double* phi, double nu, double dt,
                  double* energy, void* stream);
 
+/* ---------------------------------------------------------------- run loop
+ * The time loop around the NL step, with the input and outputs of the
+ * SPECTER-style main program the reference's transforms come from (the
+ * reference ships the transform core without a solver). */
+
+/* Reads a namelist file: &grid lmax, nz, Cz, oz (grid_init,
+ * src/pseudo/pseudospec_mod.f90:41-69; Cz = oz = 0 when absent) and
+ * &boxparams rint, rext (box_init, pseudospec_mod.f90:151-160), both
+ * required; and the optional &run group of this loop (no reference
+ * counterpart): dt, step (number of steps), tstep (steps between balance
+ * lines), sstep (steps between spectra), nu, filter (apply fc_filter after
+ * every step); defaults 0, 0, 1, 0, 0, false.  Keys are case-insensitive,
+ * reals may use the D exponent, '!' starts a comment.  Any output pointer
+ * may be NULL.  SPH_EIO: the file cannot be read; SPH_EINVAL: a required
+ * group or key is missing, a key is unknown or a value malformed. */
+int sph_read_namelist(const char* path, int* lmax, int* nz, int* Cz, int* oz, double* rint, double* rext,
+                      double* dt, int* step, int* tstep, int* sstep, double* nu, int* filter);
+/* box_init's grid files (pseudospec_mod.f90:204-220) in directory dir:
+ * theta.txt (nlat values), phi.txt (nphi) and z.txt (the nz - Cz physical
+ * points), one value per line in Fortran's 1PE23.15 format. */
+int sph_write_grids(const sph_plan* plan, const char* dir);
+/* Kinetic energy per degree of the state (Z, W) (no reference counterpart;
+ * SPECTER writes such spectra): host spec[2l] toroidal (from Z), spec[2l+1]
+ * poloidal (from W and dW/dr), l = 0..lmax, trapezoid in r over the
+ * physical points like the energy of sph_nl_rhs, which their sum equals.
+ * Synchronises the stream.  Needs the whole field. */
+int sph_energy_spectrum(sph_plan* plan, const double* Z, const double* W, double* spec, void* stream);
+/* The time loop: nsteps steps of sph_rk3_step on (Z, W, phi), each followed,
+ * if filter, by fc_filter(., 'r') of Z and phi and v_imposebc.  With outdir
+ * (may be NULL) it writes the grid files there, balance.txt (one line
+ * "step time energy" for every tstep-th state, 0 = none) and
+ * lspectrum.NNNN.txt (l, toroidal, poloidal energy of every sstep-th state,
+ * NNNN = step / sstep, 0 = none).  energy_out (may be NULL): the energy of
+ * the final state.  Needs sph_setup_bc. */
+int sph_run(sph_plan* plan, double* Z, double* W, double* phi, double nu, double dt, int nsteps, int tstep,
+            int sstep, int filter, const char* outdir, double* energy_out, void* stream);
+
 /* ---------------------------------------------------------------- timers
  * The reference accumulates wall time per stage in gtimer handles
  * (src/sphp/sphp_mod.F90:36-41: comtime, ffttime, conttime, tottime;
@@ -243,9 +312,10 @@ int sph_timer_read(sph_plan* plan, double* ms, int* launches);
 int sph_plan_set_tiles(sph_plan* plan, int rows, int ring_pairs, int z_cols);
 
 /* Device status of a plan (no reference counterpart: the reference's
- * kernels have no bounded waits).  The tensor-core kernels of an SPH_MIXED
- * plan bound every wait on a shared-memory barrier; one that gives up
- * records it in the plan.  Synchronises the device, then returns
+ * kernels have no bounded waits).  The kernels that wait on asynchronous
+ * copies (the tensor-core kernels and fp32 phi transforms of an SPH_MIXED
+ * plan, the forward phi transform of either form) bound every wait on a
+ * shared-memory barrier; one that gives up records it in the plan.  Synchronises the device, then returns
  * SPH_ETIMEDOUT if any wait gave up since the plan was created (the
  * outputs of those calls are invalid) and clears the record, else SPH_OK. */
 int sph_plan_status(sph_plan* plan);
@@ -265,8 +335,9 @@ int sph_plan_status(sph_plan* plan);
  * with the Legendre contractions of all problems in one grouped launch per
  * direction and the rest on parallel graph branches.  The graph is built
  * once by sph_batch_create (the arrays and plans must outlive the batch);
- * a plan's scratch is used by its batch, so do not run other work on the
- * same plans concurrently.  sph_batch_status synchronises the device and
+ * a plan's scratch is used by its batch, so every problem needs a plan of
+ * its own (the same plan twice is SPH_EINVAL), and no other work may run on
+ * the batch's plans concurrently.  sph_batch_status synchronises the device and
  * returns SPH_ETIMEDOUT if a bounded device wait of the batch gave up. */
 typedef struct sph_batch sph_batch;
 int sph_batch_create(sph_batch** batch, int nprob, sph_plan* const* plans, const int* nfields,

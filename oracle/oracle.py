@@ -45,6 +45,8 @@ def lib():
             getattr(L, name).argtypes = [P, D, D]
         for name in ("orc_z_forward", "orc_z_inverse", "orc_dirichlet"):
             getattr(L, name).argtypes = [P, D]
+        L.orc_z_forward_cols.argtypes = [P, D, I]
+        L.orc_z_inverse_cols.argtypes = [P, D, I]
         L.orc_qst_analysis.argtypes = [P] + [D] * 6
         L.orc_qst_synthesis.argtypes = [P] + [D] * 6
         L.orc_derivr.argtypes = [P, D, D, I, ctypes.c_char]
@@ -60,13 +62,15 @@ def lib():
         L.orc_nl_rhs.argtypes = [P, D, D, D, ctypes.c_double, D, D, D]
         L.orc_rk3_step.argtypes = [P, D, D, D, ctypes.c_double, ctypes.c_double, D]
         L.orc_velocity.argtypes = [P] + [D] * 9
+        L.orc_energy_spectrum.argtypes = [P, D, D, D]
         for name in ("orc_plan_destroy", "orc_set_threads", "orc_grid", "orc_sh_analysis",
                      "orc_sh_synthesis", "orc_qst_analysis", "orc_qst_synthesis", "orc_z_forward",
                      "orc_z_inverse", "orc_3d_forward", "orc_3d_inverse", "orc_laplang",
                      "orc_multr", "orc_dlr", "orc_saxpby_c", "orc_saxpby_r", "orc_copy",
                      "orc_prodvec", "orc_dirichlet", "orc_derivr_mat", "orc_invDl",
                      "orc_imposebc", "orc_bc_tables", "orc_nl_rhs", "orc_rk3_step",
-                     "orc_velocity"):
+                     "orc_velocity", "orc_z_forward_cols", "orc_z_inverse_cols",
+                     "orc_energy_spectrum"):
             getattr(L, name).restype = None
         _lib = L
     return _lib
@@ -193,6 +197,19 @@ class Plan:
         lib().orc_z_inverse(self.h, _p(s.view(np.float64)))
         return s
 
+    def z_forward_cols(self, spec):
+        """z forward of a (nz, ncols) slice of lm columns (in place on a copy)."""
+        s = np.array(spec, dtype=np.complex128, order="C", copy=True)
+        assert s.shape[0] == self.nz
+        lib().orc_z_forward_cols(self.h, _p(s.view(np.float64)), s.shape[1])
+        return s
+
+    def z_inverse_cols(self, spec):
+        s = np.array(spec, dtype=np.complex128, order="C", copy=True)
+        assert s.shape[0] == self.nz
+        lib().orc_z_inverse_cols(self.h, _p(s.view(np.float64)), s.shape[1])
+        return s
+
     def forward_3d(self, grid):
         g = np.ascontiguousarray(grid, dtype=np.float64)
         out = self.new_spec()
@@ -310,6 +327,13 @@ class Plan:
         e = np.zeros(1)
         lib().orc_rk3_step(self.h, *[_p(x.view(np.float64)) for x in a], nu, dt, _p(e))
         return a[0], a[1], a[2], float(e[0])
+
+    def energy_spectrum(self, Z, W):
+        """(lmax+1, 2): toroidal and poloidal kinetic energy per degree l."""
+        a = [np.ascontiguousarray(x, dtype=np.complex128) for x in (Z, W)]
+        out = np.zeros(2 * (self.lmax + 1))
+        lib().orc_energy_spectrum(self.h, *[_p(x.view(np.float64)) for x in a], _p(out))
+        return out.reshape(self.lmax + 1, 2)
 
     def velocity(self, Z, W, phi, vorticity=True):
         a = [np.ascontiguousarray(x, dtype=np.complex128) for x in (Z, W, phi)]

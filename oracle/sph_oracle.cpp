@@ -507,8 +507,10 @@ static void continuation(const orc_plan* p, cplx* f) {
       F(n - C + ii) = F(n - C + ii) + D(ii, jj) * F(n - C - d + jj) + D(C - ii + 1, jj) * F(d - jj + 1);
 }
 
-static void z_columns(const orc_plan* p, double* spec, int sign, bool cont, bool norm) {
-  const int nz = p->nz, nlm = p->nlm;
+// ncols columns of a (nz, ncols) array: the plan's nlm for whole fields, or
+// any count for a slice of the lm columns (every column is independent)
+static void z_columns(const orc_plan* p, double* spec, int ncols, int sign, bool cont, bool norm) {
+  const int nz = p->nz, nlm = ncols;
   cplx* S = reinterpret_cast<cplx*>(spec);
 #pragma omp parallel OMP_THREADS
   {
@@ -524,9 +526,16 @@ static void z_columns(const orc_plan* p, double* spec, int sign, bool cont, bool
 }
 
 // fftp1d_real_to_complex_z: continuation, FFTW_FORWARD, /nz (sphp_sca.F90:332-397)
-extern "C" void orc_z_forward(const orc_plan* p, double* spec) { z_columns(p, spec, -1, true, true); }
+extern "C" void orc_z_forward(const orc_plan* p, double* spec) { z_columns(p, spec, p->nlm, -1, true, true); }
 // fftp1d_complex_to_real_z: FFTW_BACKWARD, no normalisation (sphp_sca.F90:495-530)
-extern "C" void orc_z_inverse(const orc_plan* p, double* spec) { z_columns(p, spec, +1, false, false); }
+extern "C" void orc_z_inverse(const orc_plan* p, double* spec) { z_columns(p, spec, p->nlm, +1, false, false); }
+// the same on ncols columns of a (nz, ncols) array
+extern "C" void orc_z_forward_cols(const orc_plan* p, double* spec, int ncols) {
+  z_columns(p, spec, ncols, -1, true, true);
+}
+extern "C" void orc_z_inverse_cols(const orc_plan* p, double* spec, int ncols) {
+  z_columns(p, spec, ncols, +1, false, false);
+}
 
 extern "C" void orc_3d_forward(const orc_plan* p, const double* grid, double* spec) {
   orc_sh_analysis(p, grid, spec);
@@ -897,6 +906,37 @@ extern "C" void orc_nl_rhs(const orc_plan* p, const double* Z, const double* W, 
 
 // RK3 in the GHOST/SPECTER low-storage form X = X0 + (dt/o) RHS(X), o = 3,2,1,
 // with v_imposebc after every stage (vboundary.f90:61-63).
+// Per-degree kinetic energy from the QST potentials of u (Q = l(l+1) W/r^2,
+// S = W'/r, T = Z/r), trapezoid in r over the physical points, c_m = 1 for
+// m = 0 and 2 otherwise; spec[2 l] toroidal (T), spec[2 l + 1] poloidal (Q, S).
+// For m = 0 only the real parts count: the synthesis of a real field drops
+// the imaginary part of m = 0 (radial derivatives give one, through the
+// Nyquist wavenumber the reference keeps).  The sum is grid_energy of the
+// same state.
+extern "C" void orc_energy_spectrum(const orc_plan* p, const double* Z, const double* W, double* spec) {
+  const int nlm = p->nlm, N = p->N;
+  std::vector<double> wp(2 * nspec(p));
+  orc_derivr(p, W, wp.data(), 1, 'r');
+  const cplx* z = reinterpret_cast<const cplx*>(Z);
+  const cplx* w = reinterpret_cast<const cplx*>(W);
+  const cplx* d = reinterpret_cast<const cplx*>(wp.data());
+  for (int i = 0; i < 2 * (p->lmax + 1); ++i) spec[i] = 0.0;
+  for (int lm = 0; lm < nlm; ++lm) {
+    const int l = p->ell[lm];
+    const double cm = p->emm[lm] == 0 ? 1.0 : 2.0, L = (double)l * (l + 1);
+    double st = 0.0, sp = 0.0;
+    auto sq = [&](cplx v) { return p->emm[lm] == 0 ? v.real() * v.real() : std::norm(v); };
+    for (int k = 0; k < N; ++k) {
+      const double wk = (k == 0 || k == N - 1) ? 0.5 * p->dz : p->dz, r = p->z[k];
+      const size_t q = (size_t)k * nlm + lm;
+      st += wk * L * sq(z[q]);
+      sp += wk * (L * L * sq(w[q]) / (r * r) + L * sq(d[q]));
+    }
+    spec[2 * l] += 0.5 * cm * st;
+    spec[2 * l + 1] += 0.5 * cm * sp;
+  }
+}
+
 extern "C" void orc_rk3_step(const orc_plan* p, double* Z, double* W, double* phi, double nu,
                              double dt, double* energy) {
   const size_t ns = 2 * nspec(p);

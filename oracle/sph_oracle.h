@@ -52,6 +52,9 @@ void orc_qst_synthesis(const orc_plan* p, const double* q, const double* s,
 /* z transforms on spec (nz x nlm), in place (sphp_sca.F90:332-397, 495-530). */
 void orc_z_forward(const orc_plan* p, double* spec);
 void orc_z_inverse(const orc_plan* p, double* spec);
+/* The same on ncols lm columns of a (nz, ncols) array (a slice of a field). */
+void orc_z_forward_cols(const orc_plan* p, double* spec, int ncols);
+void orc_z_inverse_cols(const orc_plan* p, double* spec, int ncols);
 /* 3D = 2D + z (sphp_sca.F90:237-270, 400-433). */
 void orc_3d_forward(const orc_plan* p, const double* grid, double* spec);
 void orc_3d_inverse(const orc_plan* p, const double* spec, double* grid);
@@ -89,6 +92,9 @@ void orc_nl_rhs(const orc_plan* p, const double* Z, const double* W,
                 double* energy);
 void orc_rk3_step(const orc_plan* p, double* Z, double* W, double* phi,
                   double nu, double dt, double* energy);
+/* Per-degree kinetic energy of the state: spec[2l] toroidal, spec[2l+1]
+ * poloidal, l = 0..lmax; the sum is the grid energy of nl_rhs. */
+void orc_energy_spectrum(const orc_plan* p, const double* Z, const double* W, double* spec);
 /* Velocity (and vorticity) on the grid from (Z, W, phi): 3 grids each. */
 void orc_velocity(const orc_plan* p, const double* Z, const double* W,
                   const double* phi, double* ur, double* ut, double* up,

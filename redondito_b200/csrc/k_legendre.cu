@@ -570,8 +570,8 @@ int launch_leg_analysis(const sph_plan* p, int gfield, double2* spec, cudaStream
   a.gfield = gfield;
   a.out = spec;
   a.tiles = p->tilesA;
-  static bool once = set_smem(leg_analysis_kernel<false>, an::SMEM);
-  if (!once) return SPH_ECUDA;
+  static DeviceOnce once;
+  if (!once.run([] { return set_smem(leg_analysis_kernel<false>, an::SMEM); })) return SPH_ECUDA;
   dim3 grid(p->ntilesA, (a.nkz + an::KZ - 1) / an::KZ);
   TimedLaunch tl(p, T_LEG_ANA, st);
   leg_analysis_kernel<false><<<grid, 128, an::SMEM, st>>>(a, LegGroup{});
@@ -584,8 +584,8 @@ int launch_leg_synthesis(const sph_plan* p, const double2* spec, int gfield, cud
   a.gfield = gfield;
   a.spec = spec;
   a.tiles = p->tilesS;
-  static bool once = set_smem(leg_synthesis_kernel<false>, sy::SMEM);
-  if (!once) return SPH_ECUDA;
+  static DeviceOnce once;
+  if (!once.run([] { return set_smem(leg_synthesis_kernel<false>, sy::SMEM); })) return SPH_ECUDA;
   dim3 grid(p->ntilesS, (a.nkz + sy::KZ - 1) / sy::KZ);
   TimedLaunch tl(p, T_LEG_SYN, st);
   leg_synthesis_kernel<false><<<grid, 256, sy::SMEM, st>>>(a, LegGroup{});
@@ -598,8 +598,8 @@ int launch_vec_analysis(const sph_plan* p, double2* s, double2* t, cudaStream_t 
   a.out = s;
   a.out2 = t;
   a.tiles = p->tilesA;
-  static bool once = set_smem(vec_analysis_kernel, va::SMEM);
-  if (!once) return SPH_ECUDA;
+  static DeviceOnce once;
+  if (!once.run([] { return set_smem(vec_analysis_kernel, va::SMEM); })) return SPH_ECUDA;
   dim3 grid(p->ntilesA, (a.nkz + va::KZ - 1) / va::KZ);
   TimedLaunch tl(p, T_VEC_ANA, st);
   vec_analysis_kernel<<<grid, 256, va::SMEM, st>>>(a);
@@ -612,8 +612,8 @@ int launch_vec_synthesis(const sph_plan* p, const double2* s, const double2* t, 
   a.spec = s;
   a.spec2 = t;
   a.tiles = p->tilesS32;
-  static bool once = set_smem(vec_synthesis_kernel, vs::SMEM);
-  if (!once) return SPH_ECUDA;
+  static DeviceOnce once;
+  if (!once.run([] { return set_smem(vec_synthesis_kernel, vs::SMEM); })) return SPH_ECUDA;
   dim3 grid(p->ntilesS32, (a.nkz + vs::KZ - 1) / vs::KZ);
   TimedLaunch tl(p, T_VEC_SYN, st);
   vec_synthesis_kernel<<<grid, 256, vs::SMEM, st>>>(a);
@@ -663,12 +663,12 @@ int leg_group_launch(const GroupLaunch& g, cudaStream_t st) {
   if (g.total == 0) return SPH_OK;
   const LegGroup grp{static_cast<const LegArgs*>(g.jobs), g.prefix, g.njobs};
   if (g.analysis) {
-    static bool once = set_smem(leg_analysis_kernel<true>, an::SMEM);
-    if (!once) return SPH_ECUDA;
+    static DeviceOnce once;
+    if (!once.run([] { return set_smem(leg_analysis_kernel<true>, an::SMEM); })) return SPH_ECUDA;
     leg_analysis_kernel<true><<<g.grid, 128, an::SMEM, st>>>(LegArgs{}, grp);
   } else {
-    static bool once = set_smem(leg_synthesis_kernel<true>, sy::SMEM);
-    if (!once) return SPH_ECUDA;
+    static DeviceOnce once;
+    if (!once.run([] { return set_smem(leg_synthesis_kernel<true>, sy::SMEM); })) return SPH_ECUDA;
     leg_synthesis_kernel<true><<<g.grid, 256, sy::SMEM, st>>>(LegArgs{}, grp);
   }
   SPH_LAUNCH_OK();

@@ -42,6 +42,7 @@
 #include "fft3.cuh"
 #include "fft_ct.cuh"
 #include "tc05.cuh"
+#include "tma.cuh"
 
 namespace {
 
@@ -775,11 +776,7 @@ struct Phi3Maps {
 };
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* mbar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
-      "[%4];\n" ::"r"(tc05::smem_u32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(tc05::smem_u32(mbar))
-      : "memory");
+  tma::load_2d(dst, map, x, y, mbar);
 }
 
 template <int N>
@@ -1573,9 +1570,11 @@ TcArgs tc_args(const sph_plan* p) {
 
 template <int MODE, bool G>
 bool tc_attr() {
-  static const bool ok =
-      cudaFuncSetAttribute(tc_gemm<MODE, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM) == cudaSuccess;
-  return ok;
+  static DeviceOnce once;
+  return once.run([] {
+    return cudaFuncSetAttribute(tc_gemm<MODE, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM) ==
+           cudaSuccess;
+  });
 }
 
 template <int MODE>
@@ -1672,35 +1671,9 @@ int phi32_dispatch(const sph_plan* p, const Phi32Args& a, dim3 grid, size_t smem
 }
 
 constexpr int PHI3_UNSUPPORTED = 1000;
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
-// against the driver library)
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
-    void* f = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess)
-      f = nullptr;
-    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
-  }();
-  return fn;
-}
-
 // 2D fp64 view [rows][nlat] of a grid array, box NP x box_rows
-#ifndef PHI3_L2_PROMOTION
-#define PHI3_L2_PROMOTION CU_TENSOR_MAP_L2_PROMOTION_L2_256B
-#endif
 int phi3_map(CUtensorMap* map, const double* base, int nlat, int rows, int np, int box_rows) {
-  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
-  if (!enc || !base || rows < 1 || reinterpret_cast<uintptr_t>(base) % 16 || nlat % 2) return PHI3_UNSUPPORTED;
-  const cuuint64_t dims[2] = {(cuuint64_t)nlat, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)nlat * sizeof(double)};
-  const cuuint32_t box[2] = {(cuuint32_t)np, (cuuint32_t)box_rows};
-  const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims, strides, box,
-                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                         PHI3_L2_PROMOTION, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  return r == CUDA_SUCCESS ? SPH_OK : PHI3_UNSUPPORTED;
+  return tma::grid_map(map, base, nlat, rows, np, box_rows) ? SPH_OK : PHI3_UNSUPPORTED;
 }
 
 // three-step kernels: which (N, NP) fit (one step-A item per thread, both

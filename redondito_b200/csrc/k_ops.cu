@@ -2,6 +2,8 @@
 // the FP64 energy reduction.  Memory-bound kernels over the (lm, z) and
 // (theta, phi, z) layouts; grids are sized as a multiple of the SM count by
 // grid-stride loops.
+#include <algorithm>
+
 #include "sph_internal.cuh"
 
 namespace {
@@ -83,11 +85,13 @@ __global__ void dirichlet_kernel(double2* a, int nlm, int N) {
 
 // invDl (boundary_mod.f90:244-292): W(1:N) = M_l phi(3:N-2) for all m of one
 // l, the reference's DGEMM with two columns (re, im) per mode.  CTA: one l and
-// up to 32 m; phi rows staged in shared memory, M_l streamed from L2.
+// up to 32 m; phi rows staged in shared memory, M_l streamed from L2.  The
+// arrays are the caller's lm columns [lm0, lm0 + nlm); modes outside are
+// skipped.
 constexpr int IDL_M = 32;
 __global__ void __launch_bounds__(256) invdl_kernel(const double2* __restrict__ phi, double2* __restrict__ w,
                                                     const double* __restrict__ binv,
-                                                    const int* __restrict__ mbase, int nlm, int N) {
+                                                    const int* __restrict__ mbase, int lm0, int nlm, int N) {
   extern __shared__ double2 Ph[];  // [(N-4)][IDL_M]
   const int l = blockIdx.x + 1;
   const int m0 = blockIdx.y * IDL_M;
@@ -98,8 +102,8 @@ __global__ void __launch_bounds__(256) invdl_kernel(const double2* __restrict__ 
     int j = idx / IDL_M, mm = idx - j * IDL_M;
     double2 v = make_double2(0.0, 0.0);
     if (mm < nm) {
-      int m = m0 + mm;
-      v = phi[(size_t)(j + 2) * nlm + mbase[m] + (l - m)];
+      const int lm = mbase[m0 + mm] + (l - m0 - mm) - lm0;  // column of the caller's slab
+      if (lm >= 0 && lm < nlm) v = phi[(size_t)(j + 2) * nlm + lm];
     }
     Ph[idx] = v;
   }
@@ -114,8 +118,8 @@ __global__ void __launch_bounds__(256) invdl_kernel(const double2* __restrict__ 
       sr += c * v.x;
       si += c * v.y;
     }
-    int m = m0 + mm;
-    w[(size_t)i * nlm + mbase[m] + (l - m)] = make_double2(sr, si);
+    const int lm = mbase[m0 + mm] + (l - m0 - mm) - lm0;
+    if (lm >= 0 && lm < nlm) w[(size_t)i * nlm + lm] = make_double2(sr, si);
   }
 }
 
@@ -192,37 +196,37 @@ __global__ void energy_kernel(const double* __restrict__ ur, const double* __res
 
 int launch_kmul(const sph_plan* p, const double2* a, double2* b, int order, cudaStream_t st) {
   if (order < 0 || order > 4) return SPH_EINVAL;
-  size_t n = spec_elems(p);
+  size_t n = spec_view(p);
   if (order == 0) {
     if (a != b) SPH_CUDA_OK(cudaMemcpyAsync(b, a, n * sizeof(double2), cudaMemcpyDeviceToDevice, st));
     return SPH_OK;
   }
   TimedLaunch tl(p, T_OPS, st);
-  kmul_kernel<<<ew_blocks(n), EW_THREADS, 0, st>>>(a, b, p->kfac + (size_t)(order - 1) * p->nz, p->nlm, n);
+  kmul_kernel<<<ew_blocks(n), EW_THREADS, 0, st>>>(a, b, p->kfac + (size_t)(order - 1) * p->nz, p->nlmv, n);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
 
 int launch_filter_k(const sph_plan* p, double2* a, cudaStream_t st) {
-  size_t n = spec_elems(p);
+  size_t n = spec_view(p);
   TimedLaunch tl(p, T_OPS, st);
-  rowscale_kernel<<<ew_blocks(n), EW_THREADS, 0, st>>>(a, p->filt, p->nlm, n);
+  rowscale_kernel<<<ew_blocks(n), EW_THREADS, 0, st>>>(a, p->filt, p->nlmv, n);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
 
 int launch_laplang(const sph_plan* p, const double2* a, double2* b, cudaStream_t st) {
-  size_t n = spec_elems(p);
+  size_t n = spec_view(p);
   TimedLaunch tl(p, T_OPS, st);
-  laplang_kernel<<<ew_blocks(n), EW_THREADS, 0, st>>>(a, b, p->d_ell, p->nlm, n);
+  laplang_kernel<<<ew_blocks(n), EW_THREADS, 0, st>>>(a, b, p->d_ell + p->lm0, p->nlmv, n);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
 
 int launch_multr(const sph_plan* p, const double2* a, double2* b, int power, cudaStream_t st) {
-  size_t n = spec_elems(p);
+  size_t n = spec_view(p);
   TimedLaunch tl(p, T_OPS, st);
-  multr_kernel<<<ew_blocks(n), EW_THREADS, 0, st>>>(a, b, p->d_z, power, p->nlm, n);
+  multr_kernel<<<ew_blocks(n), EW_THREADS, 0, st>>>(a, b, p->d_z, power, p->nlmv, n);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
@@ -237,8 +241,10 @@ int launch_saxpby(const sph_plan* p, double* z, const double* x, double a, const
 
 int launch_prodvec(const sph_plan* p, const double* const* A, const double* const* B,
                    double* const* Cout, cudaStream_t st) {
+  // the caller's planes [k0, k0 + nzv); physical where k < N
   size_t plane = (size_t)p->nlat * p->nphi;
-  size_t ntot = plane * p->nz, nphys = plane * p->N;
+  const int nphys_planes = std::max(0, std::min(p->nzv, p->N - p->k0));
+  size_t ntot = plane * p->nzv, nphys = plane * nphys_planes;
   TimedLaunch tl(p, T_OPS, st);
   prodvec_kernel<<<ew_blocks(ntot), EW_THREADS, 0, st>>>(A[0], A[1], A[2], B[0], B[1], B[2], Cout[0],
                                                         Cout[1], Cout[2], nphys, ntot);
@@ -248,29 +254,32 @@ int launch_prodvec(const sph_plan* p, const double* const* A, const double* cons
 
 int launch_dirichlet(const sph_plan* p, double2* a, cudaStream_t st) {
   TimedLaunch tl(p, T_OPS, st);
-  dirichlet_kernel<<<ew_blocks(p->nlm), EW_THREADS, 0, st>>>(a, p->nlm, p->N);
+  dirichlet_kernel<<<ew_blocks(p->nlmv), EW_THREADS, 0, st>>>(a, p->nlmv, p->N);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
 
 int launch_invDl(const sph_plan* p, const double2* phi, double2* w, cudaStream_t st) {
-  SPH_CUDA_OK(cudaMemsetAsync(w, 0, spec_elems(p) * sizeof(double2), st));
+  SPH_CUDA_OK(cudaMemsetAsync(w, 0, spec_view(p) * sizeof(double2), st));
   if (p->lmax < 1) return SPH_OK;
   size_t smem = (size_t)(p->N - 4) * IDL_M * sizeof(double2);
   if (smem > 200 * 1024) return SPH_EINVAL;
-  static bool once = cudaFuncSetAttribute(invdl_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          200 * 1024) == cudaSuccess;
-  if (!once) return SPH_ECUDA;
+  static DeviceOnce once;
+  if (!once.run([] {
+        return cudaFuncSetAttribute(invdl_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) ==
+               cudaSuccess;
+      }))
+    return SPH_ECUDA;
   dim3 grid(p->lmax, (p->lmax + 1 + IDL_M - 1) / IDL_M);
   TimedLaunch tl(p, T_OPS, st);
-  invdl_kernel<<<grid, 256, smem, st>>>(phi, w, p->binv, p->d_mbase, p->nlm, p->N);
+  invdl_kernel<<<grid, 256, smem, st>>>(phi, w, p->binv, p->d_mbase, p->lm0, p->nlmv, p->N);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
 
 int launch_bc_fast_rows(const sph_plan* p, double2* phi, const double2* w, cudaStream_t st) {
   TimedLaunch tl(p, T_OPS, st);
-  bc_fast_kernel<<<ew_blocks(p->nlm), EW_THREADS, 0, st>>>(phi, w, p->d2bor, p->d_ell, p->d_z, p->nlm,
+  bc_fast_kernel<<<ew_blocks(p->nlmv), EW_THREADS, 0, st>>>(phi, w, p->d2bor, p->d_ell + p->lm0, p->d_z, p->nlmv,
                                                             p->nz, p->N);
   SPH_LAUNCH_OK();
   return SPH_OK;

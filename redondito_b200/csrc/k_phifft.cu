@@ -14,8 +14,12 @@
 // (synthesised even/odd sums) and writes both rings of the grid.
 // Lengths 2^a 3^b use the compile-time FFT of fft_ct.cuh; others the
 // runtime engine of fft_engine.cuh.
+#include <algorithm>
+
 #include "fft3.cuh"
 #include "fft_ct.cuh"
+#include "tc05.cuh"
+#include "tma.cuh"
 
 namespace {
 
@@ -39,6 +43,7 @@ struct PhiArgs {
   const int* kzl;  // planes to transform (nullptr: all nz)
   const double* wfold;
   FftDesc fd;
+  int* flag;  // set when a bounded wait gives up (cluster three-step forward)
 };
 
 // ---------------------------------------------------------------- lengths 2^a 3^b
@@ -417,6 +422,300 @@ int phi3d_dispatch_n(const sph_plan* p, const PhiArgs& a, int nfields, cudaStrea
   return PHI3D_UNSUPPORTED;
 }
 
+// ---------------------------------------------------------------- three-step forward (FP64, cluster tiles)
+// The forward transform reads NP consecutive rings and their NP mirrors from
+// each of the N rows of a plane; a request carries 8 NP contiguous bytes,
+// and the bandwidth an SM draws grows with that run (16, 32, 64 bytes:
+// 1.1, 1.8, 2.7 TB/s).  An FP64 tile of 4 ring pairs already fills half of
+// an SM's shared memory, so a tile of NPC = 4 CL ring pairs is shared by a
+// cluster of CL CTAs: CTA rank r loads, by TMA, the rows [r N/CL, (r+1) N/CL)
+// of all NPC rings and mirrors (runs of 8 NPC bytes: 64 B for CL = 2, 128 B
+// for CL = 4), double buffered, and transforms ring pairs 4r .. 4r+3, whose
+// samples it reads across the cluster from distributed shared memory in
+// step (A).  Two cluster barriers per tile: (1) every CTA's rows have landed
+// (or a bounded wait gave up, which every CTA then sees), (2) no CTA reads
+// another's staged rows any more, so each overwrites its own with its
+// transform area.  Steps (A), (B), (C) and the fold are those of the
+// three-step inverse run forwards (sign -1); the fold writes the folded
+// coefficients G[m][parity][k][node] like phi_fwd_ct.  The staged rows are
+// swizzled by the TMA (16-byte chunk index XOR 128-byte row index), so the
+// step-(A) reads of a half warp (4 ring pairs x 4 rows) spread over the
+// banks; the transform area has an odd row pitch and a ring-pair stride of
+// 2 (mod 8) 16-byte slots.
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+// shared::cluster address of `p` (a shared-memory location of this CTA) in CTA `rank`
+__device__ __forceinline__ uint32_t cluster_map(const void* p, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(tc05::smem_u32(p)), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ double ld_cluster_f64(uint32_t addr) {
+  double v;
+  asm volatile("ld.shared::cluster.f64 %0, [%1];\n" : "=d"(v) : "r"(addr) : "memory");
+  return v;
+}
+__device__ __forceinline__ int ld_cluster_s32(uint32_t addr) {
+  int v;
+  asm volatile("ld.shared::cluster.s32 %0, [%1];\n" : "=r"(v) : "r"(addr) : "memory");
+  return v;
+}
+
+constexpr int largest_divisor_le(int n, int cap) {
+  int d = cap < n ? cap : n;
+  while (d > 1 && n % d) --d;
+  return d;
+}
+constexpr size_t round_up(size_t x, size_t q) { return (x + q - 1) / q * q; }
+
+template <int N, int CL>
+struct P3c {
+  static constexpr int NPL = 4, NPC = NPL * CL;  // ring pairs per CTA, per cluster tile
+  static constexpr int A = 16, M = N / A, B = ct::pow2_part_cap16(M), C = M / B;
+  static constexpr int ROWS = N / CL;                          // phi rows staged by one CTA
+  static constexpr int BR = largest_divisor_le(ROWS, 256);     // rows per TMA box
+  static constexpr int ROWB = NPC * 8;                         // bytes per staged row
+  static constexpr int SWB = CL == 4 ? 3 : 2;                  // swizzle: 2^SWB chunks of 16 bytes
+  static constexpr int ITEMS_A = NPL * M, ITEMS_B = NPL * A * C, ITEMS_C = NPL * A * B;
+  static constexpr int THREADS = ITEMS_A <= 64 ? 64 : (ITEMS_A + 31) / 32 * 32;
+  static constexpr int PR = M | 1;
+  static constexpr int SB = up_mod16(A * PR, 8 / NPL);
+  static constexpr size_t XBYTES = (size_t)NPL * SB * sizeof(double2);
+  static constexpr size_t TILE_BYTES = (size_t)2 * ROWS * ROWB;  // rings and mirrors
+  static constexpr size_t STAGE = round_up(XBYTES > TILE_BYTES ? XBYTES : TILE_BYTES, 1024);
+  static constexpr size_t SMEM = 2 * STAGE + (size_t)N * sizeof(double2) + 64;
+  // byte offset of staged element (row, column) within one half of a stage
+  static __device__ __forceinline__ uint32_t off(int row, int col) {
+    const uint32_t o = (uint32_t)(row * ROWB + col * 8);
+    return o ^ (((o >> 7) & ((1u << SWB) - 1)) << 4);
+  }
+};
+
+template <int N, int CL>
+constexpr bool phi3c_ok() {
+  if constexpr (N % 16 != 0 || N < 48 || (CL != 2 && CL != 4)) {
+    return false;
+  } else {
+    using G = P3c<N, CL>;
+    // every TMA box and both halves of a stage start on a 1024-byte boundary (swizzle atoms)
+    return G::THREADS <= 1024 && ((size_t)G::ROWS * G::ROWB) % 1024 == 0 && (G::BR * G::ROWB) % 1024 == 0 &&
+           G::SMEM <= 227 * 1024;
+  }
+}
+
+struct GridMaps {
+  CUtensorMap m[SPH_MAX_FIELDS];
+};
+
+template <int N, int CL>
+__global__ void __launch_bounds__(P3c<N, CL>::THREADS, 1)
+    phi3c_fwd64(PhiArgs a, int ntiles, const __grid_constant__ GridMaps maps) {
+  using G = P3c<N, CL>;
+  constexpr int A = G::A, M = G::M, B = G::B, C = G::C, T = G::THREADS, NPL = G::NPL, NPC = G::NPC;
+  constexpr int ROWS = G::ROWS, BR = G::BR;
+  extern __shared__ __align__(1024) unsigned char sm3c[];
+  double2* tw = reinterpret_cast<double2*>(sm3c + 2 * G::STAGE);
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm3c + 2 * G::STAGE + (size_t)N * sizeof(double2));
+  int* bad = reinterpret_cast<int*>(full + 2);  // this CTA's last wait gave up (read by the cluster)
+  const int t = threadIdx.x;
+  const uint32_t rank = cluster_rank();
+  const int cid = blockIdx.x / CL, ncl = gridDim.x / CL;
+  const int nlat = a.nlat, ngroups = nlat / 2 / NPC;
+  for (int i = t; i < N; i += T) tw[i] = __ldg(a.fd.tw + i);
+  if (t == 0) {
+    tc05::mbar_init(&full[0], 1);
+    tc05::mbar_init(&full[1], 1);
+    *bad = 0;
+    tc05::mbar_fence_init();
+  }
+  __syncthreads();
+  cluster_sync_all();  // every CTA of the cluster runs before any reads another's shared memory
+  auto stage = [&](int w) { return sm3c + (size_t)w * G::STAGE; };
+  // one thread: this CTA's rows of a tile, rings then mirrors
+  auto issue = [&](int tile, int w) {
+    const int g = tile % ngroups, r = tile / ngroups, k = r % a.nz, f = r / a.nz;
+    unsigned char* st = stage(w);
+    tma::expect_tx(&full[w], (uint32_t)G::TILE_BYTES);
+    const int y0 = k * N + (int)rank * ROWS;
+#pragma unroll 1
+    for (int i = 0; i < ROWS / BR; ++i) {
+      tma::load_2d(st + (size_t)i * BR * G::ROWB, &maps.m[f], g * NPC, y0 + i * BR, &full[w]);
+      tma::load_2d(st + (size_t)(ROWS + i * BR) * G::ROWB, &maps.m[f], nlat - g * NPC - NPC, y0 + i * BR,
+                   &full[w]);
+    }
+  };
+  int tile = cid;
+  if (t == 0 && tile < ntiles) issue(tile, 0);
+  int s = 0;
+  uint32_t phase = 0;  // bit s: parity of the next completion of stage s
+  bool gave_up = false;
+  for (; tile < ntiles; tile += ncl, s ^= 1) {
+    const bool ok = tc05::mbar_wait(&full[s], (phase >> s) & 1);
+    const int mine = __syncthreads_or(!ok);
+    if (t == 0) *bad = mine;
+    cluster_sync_all();  // (1)
+    int any = 0;
+#pragma unroll
+    for (int r = 0; r < CL; ++r) any |= ld_cluster_s32(cluster_map(bad, r));
+    if (any) {  // every CTA of the cluster leaves here, on the same tile
+      gave_up = mine != 0;
+      break;
+    }
+    phase ^= 1u << s;
+    if (t == 0 && tile + ncl < ntiles) {
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      issue(tile + ncl, s ^ 1);
+    }
+    const int g = tile % ngroups, rr = tile / ngroups, k = rr % a.nz, f = rr / a.nz;
+    const int p0 = g * NPC + (int)rank * NPL;
+    // (A) the samples x[nm + M n1] of local ring pair b (ring: real part, mirror: imaginary part)
+    const bool act = t < G::ITEMS_A;
+    const int b = t % NPL, nm = t / NPL;
+    double2 v[A];
+    if (act) {
+      const int col = (int)rank * NPL + b;
+      uint32_t base[CL];
+#pragma unroll
+      for (int o = 0; o < CL; ++o) base[o] = cluster_map(stage(s), o);
+#pragma unroll
+      for (int n1 = 0; n1 < A; ++n1) {
+        constexpr int PER = A / CL;  // n1 values per staged row range
+        const int o = n1 / PER, jr = nm + M * (n1 - o * PER);
+        v[n1] = make_double2(ld_cluster_f64(base[o] + G::off(jr, col)),
+                             ld_cluster_f64(base[o] + (uint32_t)(ROWS * G::ROWB) + G::off(jr, NPC - 1 - col)));
+      }
+    }
+    cluster_sync_all();  // (2)
+    double2* X = reinterpret_cast<double2*>(stage(s));
+    if (act) {
+      ct::RD<double2, A, -1>::run(v);
+      double2* xo = X + b * G::SB + nm;
+#pragma unroll
+      for (int ka = 0; ka < A; ++ka) xo[ka * G::PR] = ka ? ct::mul(v[ka], tw[nm * ka]) : v[ka];
+    }
+    __syncthreads();
+    if constexpr (B > 1) {  // (B)
+      for (int it = t; it < G::ITEMS_B; it += T) {
+        const int ka = it % A, r2 = it / A, c = r2 % C, bb = r2 / C;
+        double2* row = X + bb * G::SB + ka * G::PR + c;
+        double2 w[B];
+#pragma unroll
+        for (int nb = 0; nb < B; ++nb) w[nb] = row[C * nb];
+        ct::RD<double2, B, -1>::run(w);
+#pragma unroll
+        for (int kb = 0; kb < B; ++kb) row[C * kb] = (kb && c) ? ct::mul(w[kb], tw[A * c * kb]) : w[kb];
+      }
+      __syncthreads();
+    }
+    if constexpr (C > 1) {  // (C)
+      for (int it = t; it < G::ITEMS_C; it += T) {
+        const int ka = it % A, r2 = it / A, kb = r2 % B, bb = r2 / B;
+        double2* row = X + bb * G::SB + ka * G::PR + C * kb;
+        double2 u[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) u[c] = row[c];
+        ct::RD<double2, C, -1>::run(u);
+#pragma unroll
+        for (int kc = 0; kc < C; ++kc) row[kc] = u[kc];
+      }
+      __syncthreads();
+    }
+    // fold both parities of one (m, pair) from Z(m), Z(-m), as phi_fwd_ct
+    double2* Gp = a.G + (size_t)f * a.Gfield + (size_t)k * a.ldn + p0;
+    const size_t mstride = (size_t)2 * a.nz * a.ldn, pstride = (size_t)a.nz * a.ldn;
+    const double W = __ldg(a.wfold + p0 + b);
+    auto zpos = [&](int m) {
+      const int q = m / A;
+      return (m % A) * G::PR + C * (q % B) + q / B;
+    };
+    for (int m = t / NPL; m <= a.lmax; m += T / NPL) {
+      const double2 Z = X[b * G::SB + zpos(m)];
+      const double2 Zc = X[b * G::SB + zpos(m == 0 ? 0 : N - m)];
+      // F(i) = (Z + conj Z(-m))/2, F(mirror) = -i (Z - conj Z(-m))/2
+      double2 Fi = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y - Zc.y));
+      double2 Fm = make_double2(0.5 * (Z.y + Zc.y), -0.5 * (Z.x - Zc.x));
+      Gp[m * mstride + b] = cscale(cadd(Fi, Fm), W);
+      Gp[m * mstride + pstride + b] = cscale(csub(Fi, Fm), W);
+    }
+    // this stage is refilled by TMA (async proxy) after the next barrier
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  }
+  if (gave_up && t == 0) {  // report, and let the copy still in flight land before leaving
+    atomicExch(a.flag, 1);
+    tc05::mbar_wait(&full[s], (phase >> s) & 1);
+  }
+  cluster_sync_all();  // no CTA leaves while another may still read its shared memory
+}
+
+constexpr int PHI3C_UNSUPPORTED = 1000;
+
+template <int N, int CL>
+int phi3c_run(const sph_plan* p, const PhiArgs& a, int nfields, cudaStream_t st) {
+  if constexpr (!phi3c_ok<N, CL>()) {
+    return PHI3C_UNSUPPORTED;
+  } else {
+    using G = P3c<N, CL>;
+    if (p->nlat2 % G::NPC || !a.flag) return PHI3C_UNSUPPORTED;
+    const long long ntiles = (long long)(p->nlat2 / G::NPC) * p->nz * nfields;
+    if (ntiles == 0) return SPH_OK;
+    if (ntiles > (1ll << 30) || (long long)N * p->nz > (1ll << 31) - 1) return PHI3C_UNSUPPORTED;
+    GridMaps maps;
+    const CUtensorMapSwizzle swz = CL == 4 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
+    for (int f = 0; f < nfields; ++f)
+      if (!tma::grid_map(&maps.m[f], a.gin[f], p->nlat, (long long)N * p->nz, G::NPC, G::BR,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, swz))
+        return PHI3C_UNSUPPORTED;
+    for (int f = nfields; f < SPH_MAX_FIELDS; ++f) maps.m[f] = maps.m[0];
+    auto kern = phi3c_fwd64<N, CL>;
+    static DeviceOnce once;
+    if (!once.run([] {
+          return cudaFuncSetAttribute(phi3c_fwd64<N, CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)G::SMEM) == cudaSuccess &&
+                 cudaFuncSetAttribute(phi3c_fwd64<N, CL>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) ==
+                     cudaSuccess;
+        }))
+      return SPH_ECUDA;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(G::THREADS);
+    cfg.dynamicSmemBytes = G::SMEM;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3(CL);
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg) != cudaSuccess || nclusters < 1)
+      return PHI3C_UNSUPPORTED;
+    const long long ncl = std::min<long long>(nclusters, (ntiles + 0));
+    cfg.gridDim = dim3((unsigned)(ncl * CL));
+    if (cudaLaunchKernelEx(&cfg, kern, a, (int)ntiles, maps) != cudaSuccess) return SPH_ECUDA;
+    return SPH_OK;
+  }
+}
+
+// cluster size: 4 (128-byte runs) where nlat/2 splits into tiles of 16 ring
+// pairs, else 2; ring_pairs tuned to 8 selects 2
+template <int N>
+int phi3c_dispatch_n(const sph_plan* p, const PhiArgs& a, int nfields, cudaStream_t st) {
+  if (p->tile_np && p->tile_np != 8) return PHI3C_UNSUPPORTED;
+  if (!p->tile_np && p->nlat2 % 16 == 0) {
+    const int rc = phi3c_run<N, 4>(p, a, nfields, st);
+    if (rc != PHI3C_UNSUPPORTED) return rc;
+  }
+  if (p->nlat2 % 8 == 0) return phi3c_run<N, 2>(p, a, nfields, st);
+  return PHI3C_UNSUPPORTED;
+}
+
 // ring pairs per CTA: the largest of 8, 4, 2, 1 that divides nlat/2 and
 // keeps NP*nphi <= PMAXC
 int pairs_per_cta(const sph_plan* p) {
@@ -496,6 +795,17 @@ int launch_phi_fwd(const sph_plan* p, const double* const* grids, int nfields, c
   dim3 grid(p->nlat2 / a.NP, p->sel_kz ? p->sel_n : p->nz, nfields);
   size_t smem = (size_t)a.NP * seq_stride(p->nphi) * sizeof(double2);
   TimedLaunch tl(p, T_PHI_FWD, st);
+  if (!p->sel_kz) {  // the cluster three-step kernel walks every plane
+    a.flag = p->dflag;
+    int rc = PHI3C_UNSUPPORTED;
+    switch (p->nphi) {
+#define CASE(n) \
+  case n: rc = phi3c_dispatch_n<n>(p, a, nfields, st); break;
+      PHI_SIZES(CASE)
+#undef CASE
+    }
+    if (rc != PHI3C_UNSUPPORTED) return rc;
+  }
   switch (p->nphi) {
 #define CASE(n) \
   case n: return launch_fwd_n<n>(a, grid, smem, st);

@@ -173,11 +173,14 @@ __global__ void __launch_bounds__(ZTHREADS) zfft_kernel(ZArgs a) {
 
 template <int MODE, int CTN>
 int launch_ct(const ZArgs& a, int nblocks, size_t smem, cudaStream_t st) {
-  static bool once = cudaFuncSetAttribute(zfft_kernel<MODE, CTN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          200 * 1024) == cudaSuccess &&
-                     cudaFuncSetAttribute(zfft_kernel<MODE, CTN>,
-                                          cudaFuncAttributePreferredSharedMemoryCarveout, 100) == cudaSuccess;
-  if (!once) return SPH_ECUDA;
+  static DeviceOnce once;
+  if (!once.run([] {
+        return cudaFuncSetAttribute(zfft_kernel<MODE, CTN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    200 * 1024) == cudaSuccess &&
+               cudaFuncSetAttribute(zfft_kernel<MODE, CTN>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    100) == cudaSuccess;
+      }))
+    return SPH_ECUDA;
   zfft_kernel<MODE, CTN><<<nblocks, ZTHREADS, smem, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;
@@ -203,7 +206,7 @@ int launch_zfft(const sph_plan* p, int mode, const double2* in, double2* out, in
   ZArgs a;
   a.in = in;
   a.out = out;
-  a.nlm = p->nlm;
+  a.nlm = p->nlmv;  // the caller's lm columns [lm0, lm0 + nlmv)
   a.nz = p->nz;
   a.N = cont ? p->N : p->nz;
   a.C = cont ? p->C : 0;
@@ -213,7 +216,7 @@ int launch_zfft(const sph_plan* p, int mode, const double2* in, double2* out, in
   a.kfac = (order >= 1 && order <= 4) ? p->kfac + (size_t)(order - 1) * p->nz : nullptr;
   a.filt = p->filt;
   a.zinv2 = p->zinv2;
-  a.ell = p->d_ell;
+  a.ell = p->d_ell + p->lm0;
   a.fd = p->fz;
   // columns per CTA: a power of two with LB*nz <= ZMAXCOL/2, at most 64
   // (32 KB slabs: 4 CTAs per SM, still full 128-byte lines per row at nz = 256)
@@ -222,7 +225,7 @@ int launch_zfft(const sph_plan* p, int mode, const double2* in, double2* out, in
   if (p->tile_lb) LB = p->tile_lb;
   if (LB * p->nz > ZMAXCOL) return SPH_EINVAL;
   a.LB = LB;
-  int nblocks = (p->nlm + LB - 1) / LB;
+  int nblocks = (p->nlmv + LB - 1) / LB;
   size_t smem = (size_t)LB * p->nz * sizeof(double2) * (mode == Z_DLR ? 2 : 1);
   TimedLaunch tl(p, T_ZFFT, st);
   switch (mode) {

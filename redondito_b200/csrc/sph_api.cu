@@ -168,7 +168,8 @@ static void plan_free(sph_plan* p) {
   void* ptrs[] = {p->P, p->dP, p->mPs, p->wfold, p->wfull, p->d_dir, p->d_z, p->kfac, p->filt,
                   p->zinv2, p->d_ell, p->d_mbase, p->twz, p->twphi, p->twzf, p->twphif, p->revz,
                   p->revphi, p->twpz, p->twpphi, p->twpzf, p->twpphif, p->tw4f, p->tw4d, p->tilesA,
-                  p->tilesA32, p->tilesS, p->tilesS32, p->G, p->binv, p->d2bor, p->energy, p->d_bplanes};
+                  p->tilesA32, p->tilesS, p->tilesS32, p->G, p->binv, p->d2bor, p->energy, p->d_bplanes,
+                  p->spectrum};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (auto& q : p->sp)
@@ -210,6 +211,8 @@ extern "C" int sph_plan_create(sph_plan** out, int lmax, int nlat, int nphi, int
   p->d = oz;
   p->nlm = (lmax + 1) * (lmax + 2) / 2;
   p->N = nz - Cz;
+  p->nzv = nz;
+  p->nlmv = p->nlm;
   p->precision = precision;
   p->rint = rint;
   p->rext = rext;
@@ -370,6 +373,12 @@ extern "C" int sph_plan_create(sph_plan** out, int lmax, int nlat, int nphi, int
     rc = SPH_ECUDA;
   if (rc == SPH_OK && cudaMalloc((void**)&p->energy, sizeof(double)) != cudaSuccess) rc = SPH_ENOMEM;
   if (rc == SPH_OK && precision == SPH_MIXED) rc = mixed_setup(p, hP, hdP, hmPs);
+  // status word of the kernels with bounded waits (every plan: the FP64
+  // forward phi transform waits on its TMA copies too)
+  if (rc == SPH_OK && !p->dflag) {
+    if (cudaMalloc((void**)&p->dflag, sizeof(int)) != cudaSuccess) rc = SPH_ENOMEM;
+    else if (cudaMemset(p->dflag, 0, sizeof(int)) != cudaSuccess) rc = SPH_ECUDA;
+  }
   if (rc == SPH_OK && precision == SPH_MIXED && Cz > 0 && oz > 0) {
     std::vector<int> bp;
     for (int k = 0; k < p->N; ++k)
@@ -543,8 +552,39 @@ struct BoundaryPlanes {
   }
 };
 
+// While it lives, the angular launchers (which take their plane count from
+// nz) see the caller's plane slab as the plan's planes.  The angular
+// transform of a plane does not depend on the plane's index.
+struct PlaneSlab {
+  sph_plan* p;
+  int nz0;
+  explicit PlaneSlab(sph_plan* p_) : p(p_), nz0(p_->nz) { p->nz = p->nzv; }
+  ~PlaneSlab() { p->nz = nz0; }
+};
+
+extern "C" int sph_plan_set_slab(sph_plan* p, int k0, int nplanes, int lm0, int nlm_local) {
+  if (!p || k0 < 0 || nplanes < 1 || k0 + nplanes > p->nz || lm0 < 0 || nlm_local < 1 ||
+      lm0 + nlm_local > p->nlm)
+    return SPH_EINVAL;
+  p->k0 = k0;
+  p->nzv = nplanes;
+  p->lm0 = lm0;
+  p->nlmv = nlm_local;
+  return SPH_OK;
+}
+
+extern "C" int sph_range(int n1, int n2, int nprocs, int irank, int* ista, int* iend) {
+  if (!ista || !iend || nprocs < 1 || irank < 0 || irank >= nprocs || n2 < n1 - 1) return SPH_EINVAL;
+  // range (src/sphp/sphp_sca.F90:596-626): the first mod(n, nprocs) ranks take one more
+  const int n = n2 - n1 + 1, w1 = n / nprocs, w2 = n % nprocs;
+  *ista = irank * w1 + n1 + std::min(irank, w2);
+  *iend = *ista + w1 - 1 + (w2 > irank ? 1 : 0);
+  return SPH_OK;
+}
+
 extern "C" int sph_fftp2d_real_to_complex_xy(sph_plan* p, const double* in, double* out, void* s) {
   if (!p || !in || !out) return SPH_EINVAL;
+  PlaneSlab view(p);
   const double* g[1] = {in};
   if (p->precision == SPH_MIXED) {
     RC(launch_phi_fwd32(p, g, 1, ST(s)));
@@ -560,6 +600,7 @@ extern "C" int sph_fftp2d_real_to_complex_xy(sph_plan* p, const double* in, doub
 
 extern "C" int sph_fftp2d_complex_to_real_xy(sph_plan* p, const double* in, double* out, void* s) {
   if (!p || !in || !out) return SPH_EINVAL;
+  PlaneSlab view(p);
   double* g[1] = {out};
   if (p->precision == SPH_MIXED) {
     RC(launch_tc_synthesis(p, 0, CD2(in), nullptr, ST(s)));
@@ -584,6 +625,7 @@ extern "C" int sph_fftp1d_complex_to_real_z(sph_plan* p, double* inout, void* s)
 }
 
 extern "C" int sph_fftp3d_real_to_complex(sph_plan* p, const double* in, double* out, void* s) {
+  if (!p || !slab_whole(p)) return SPH_EINVAL;  // the 3D transforms need the slab transpose
   if (p && in && out && p->precision == SPH_MIXED && p->C > 0 && p->contg) {
     // continue the physical planes first (FP64): the continuation then acts
     // on exact data and the angular round-off of every plane stays local
@@ -599,6 +641,7 @@ extern "C" int sph_fftp3d_real_to_complex(sph_plan* p, const double* in, double*
 }
 
 extern "C" int sph_fftp3d_complex_to_real(sph_plan* p, double* in, double* out, void* s) {
+  if (!p || !slab_whole(p)) return SPH_EINVAL;
   RC(sph_fftp1d_complex_to_real_z(p, in, s));
   return sph_fftp2d_complex_to_real_xy(p, in, out, s);
 }
@@ -606,6 +649,7 @@ extern "C" int sph_fftp3d_complex_to_real(sph_plan* p, double* in, double* out, 
 extern "C" int sph_fftp2d_vec_to_qst(sph_plan* p, const double* vr, const double* vt, const double* vp,
                                      double* q, double* sO, double* t, void* s) {
   if (!p || !vr || !vt || !vp || !q || !sO || !t) return SPH_EINVAL;
+  PlaneSlab view(p);
   const double* g[3] = {vr, vt, vp};
   if (p->precision == SPH_MIXED) {
     RC(launch_phi_fwd32(p, g, 3, ST(s)));
@@ -625,6 +669,7 @@ extern "C" int sph_fftp2d_vec_to_qst(sph_plan* p, const double* vr, const double
 extern "C" int sph_fftp2d_qst_to_vec(sph_plan* p, const double* q, const double* sI, const double* t,
                                      double* vr, double* vt, double* vp, void* s) {
   if (!p || !vr || !vt || !vp || !q || !sI || !t) return SPH_EINVAL;
+  PlaneSlab view(p);
   double* g[3] = {vr, vt, vp};
   if (p->precision == SPH_MIXED) {
     RC(launch_tc_synthesis(p, 0, CD2(q), nullptr, ST(s)));
@@ -643,7 +688,7 @@ extern "C" int sph_fftp2d_qst_to_vec(sph_plan* p, const double* q, const double*
 
 extern "C" int sph_fftp3d_vec_to_qst(sph_plan* p, const double* vr, const double* vt, const double* vp,
                                      double* q, double* sO, double* t, void* s) {
-  if (!p || !vr || !vt || !vp || !q || !sO || !t) return SPH_EINVAL;
+  if (!p || !vr || !vt || !vp || !q || !sO || !t || !slab_whole(p)) return SPH_EINVAL;
   if (p->precision == SPH_MIXED && p->C > 0 && p->contg) {
     const double* g[3] = {vr, vt, vp};
     const double* gh[3] = {p->contg, p->contg + (size_t)p->C * p->nphi * p->nlat,
@@ -662,7 +707,7 @@ extern "C" int sph_fftp3d_vec_to_qst(sph_plan* p, const double* vr, const double
 
 extern "C" int sph_fftp3d_qst_to_vec(sph_plan* p, double* q, double* sI, double* t, double* vr, double* vt,
                                      double* vp, void* s) {
-  if (!p || !vr || !vt || !vp || !q || !sI || !t) return SPH_EINVAL;
+  if (!p || !vr || !vt || !vp || !q || !sI || !t || !slab_whole(p)) return SPH_EINVAL;
   for (double* x : {q, sI, t}) RC(sph_fftp1d_complex_to_real_z(p, x, s));
   return sph_fftp2d_qst_to_vec(p, q, sI, t, vr, vt, vp, s);
 }
@@ -697,13 +742,13 @@ extern "C" int sph_dlr(sph_plan* p, const double* a, double* b, void* s) {
 extern "C" int sph_saxpby_c(sph_plan* p, double* z, const double* x, double a, const double* y, double b,
                             void* s) {
   if (!p || !z || !x || !y) return SPH_EINVAL;
-  return launch_saxpby(p, z, x, a, y, b, 2 * spec_elems(p), ST(s));
+  return launch_saxpby(p, z, x, a, y, b, 2 * spec_view(p), ST(s));
 }
 
 extern "C" int sph_saxpby_r(sph_plan* p, double* z, const double* x, double a, const double* y, double b,
                             void* s) {
   if (!p || !z || !x || !y) return SPH_EINVAL;
-  return launch_saxpby(p, z, x, a, y, b, grid_elems(p), ST(s));
+  return launch_saxpby(p, z, x, a, y, b, grid_view(p), ST(s));
 }
 
 extern "C" int sph_fc_filter(sph_plan* p, double* a, char esp, void* s) {
@@ -715,7 +760,7 @@ extern "C" int sph_fc_filter(sph_plan* p, double* a, char esp, void* s) {
 
 extern "C" int sph_copy(sph_plan* p, const double* a, double* b, void* s) {
   if (!p || !a || !b) return SPH_EINVAL;
-  SPH_CUDA_OK(cudaMemcpyAsync(b, a, spec_elems(p) * sizeof(double2), cudaMemcpyDeviceToDevice, ST(s)));
+  SPH_CUDA_OK(cudaMemcpyAsync(b, a, spec_view(p) * sizeof(double2), cudaMemcpyDeviceToDevice, ST(s)));
   return SPH_OK;
 }
 
@@ -968,7 +1013,7 @@ static int nl_rhs_impl(sph_plan* p, const double2* Z, const double2* W, const do
 
 extern "C" int sph_nl_rhs(sph_plan* p, const double* Z, const double* W, const double* phi, double nu,
                           double* rhs_z, double* rhs_phi, double* energy, void* s) {
-  if (!p || !Z || !W || !phi || !rhs_z || !rhs_phi) return SPH_EINVAL;
+  if (!p || !Z || !W || !phi || !rhs_z || !rhs_phi || !slab_whole(p)) return SPH_EINVAL;
   if (!p->bc_ready) return SPH_ENOTREADY;
   RC(nl_rhs_impl(p, CD2(Z), CD2(W), CD2(phi), nu, D2(rhs_z), D2(rhs_phi), ST(s)));
   if (energy) {
@@ -980,7 +1025,7 @@ extern "C" int sph_nl_rhs(sph_plan* p, const double* Z, const double* W, const d
 
 extern "C" int sph_rk3_step(sph_plan* p, double* Z, double* W, double* phi, double nu, double dt,
                             double* energy, void* s) {
-  if (!p || !Z || !W || !phi) return SPH_EINVAL;
+  if (!p || !Z || !W || !phi || !slab_whole(p)) return SPH_EINVAL;
   if (!p->bc_ready) return SPH_ENOTREADY;
   cudaStream_t st = ST(s);
   const size_t bytes = spec_elems(p) * sizeof(double2);

@@ -143,10 +143,18 @@ extern "C" int sph_batch_create(sph_batch** out, int nprob, sph_plan* const* pla
   int k = 0;
   for (int p = 0; p < nprob; ++p) {
     if (!plans[p] || plans[p]->precision != b->precision || nfields[p] < 1 || nfields[p] > SPH_MAX_FIELDS ||
-        plans[p]->timing) {
+        plans[p]->timing || !slab_whole(plans[p])) {
       delete b;
       return SPH_EINVAL;
     }
+    // a plan's per-field scratch (folded coefficients, synthesis tiles,
+    // continued planes) serves one problem: two problems on one plan would
+    // race on it from their graph branches
+    for (int q = 0; q < p; ++q)
+      if (plans[q] == plans[p]) {
+        delete b;
+        return SPH_EINVAL;
+      }
     b->plans.push_back(plans[p]);
     b->nf.push_back(nfields[p]);
     b->spec.emplace_back();

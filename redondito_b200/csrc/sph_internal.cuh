@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -115,6 +116,7 @@ struct sph_plan {
   double* binv = nullptr;   // [lmax][N-4][N]  M_l column-major per l
   double* d2bor = nullptr;  // [N][4]
   double* energy = nullptr; // device accumulator (1 double)
+  double* spectrum = nullptr;  // device [lmax+1][2] per-degree energies (sph_energy_spectrum)
   // mixed precision: bf16 table tiles for the tcgen05 GEMMs, bf16 data tiles
   // (analysis: written by the phi FFT; synthesis: from the spectra), fp32
   // folded coefficients G32 of the synthesis (reusing the G allocation)
@@ -145,6 +147,12 @@ struct sph_plan {
   // two-pass forward phi transform (mixed): tile images of phi2_planes plane-fields
   float2* phi2 = nullptr;
   int phi2_planes = 0;
+  // the caller's slab (sph_plan_set_slab; the whole field by default): the
+  // radial transforms, spectral operators and boundary act on the lm
+  // columns [lm0, lm0 + nlmv) of (nlmv, nz) arrays; the 2D angular
+  // transforms on the planes [k0, k0 + nzv) of (nlat, nphi, nzv) and
+  // (nlm, nzv) arrays (the reference's per-rank arrays in, carr1)
+  int k0 = 0, nzv = 0, lm0 = 0, nlmv = 0;
   // stage timers (sph_timer_*): event pairs recorded around each launch
   int timing = 0;
   std::vector<cudaEvent_t> ev_pool;
@@ -168,6 +176,12 @@ enum { T_PHI_FWD = 0, T_PHI_INV, T_LEG_ANA, T_LEG_SYN, T_VEC_ANA, T_VEC_SYN, T_Z
 
 static inline size_t spec_elems(const sph_plan* p) { return (size_t)p->nz * p->nlm; }
 static inline size_t grid_elems(const sph_plan* p) { return (size_t)p->nz * p->nphi * p->nlat; }
+// the caller's slab: (nlmv, nz) spectral and (nlat, nphi, nzv) physical arrays
+static inline size_t spec_view(const sph_plan* p) { return (size_t)p->nz * p->nlmv; }
+static inline size_t grid_view(const sph_plan* p) { return (size_t)p->nzv * p->nphi * p->nlat; }
+static inline bool slab_whole(const sph_plan* p) {
+  return p->k0 == 0 && p->nzv == p->nz && p->lm0 == 0 && p->nlmv == p->nlm;
+}
 
 // ---------------------------------------------------------------- device helpers
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
@@ -253,6 +267,25 @@ int tc_group_launch(const GroupLaunch& g, int* flag, cudaStream_t st);
 void group_free(GroupLaunch* g);
 // spectra -> synthesis data tiles of field slot `field` (mixed plans)
 int launch_spec_to_tiles_field(const sph_plan* p, const double2* in, int field, cudaStream_t st);
+
+// Runs a set-up step (typically cudaFuncSetAttribute: a kernel's dynamic
+// shared-memory limit) once per device.  Function attributes belong to the
+// context of the device current at the call, so a process that drives
+// several GPUs must set them on each; devices 0..63 are remembered, others
+// repeat the step on every call.
+struct DeviceOnce {
+  std::atomic<unsigned long long> mask{0};
+  template <typename F>
+  bool run(F&& step) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    const unsigned long long bit = (dev >= 0 && dev < 64) ? 1ull << dev : 0ull;
+    if (bit && (mask.load(std::memory_order_acquire) & bit)) return true;
+    if (!step()) return false;
+    if (bit) mask.fetch_or(bit, std::memory_order_acq_rel);
+    return true;
+  }
+};
 
 #define SPH_CUDA_OK(call)                     \
   do {                                        \

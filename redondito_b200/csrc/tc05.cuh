@@ -138,13 +138,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, uint64_t
   }
 }
 
-// ---------------------------------------------------------------- fp16 split
-// x*scale = hi + lo with hi = fp16(x*scale), lo = fp16(x*scale - hi).
-__device__ __forceinline__ void split16(float xs, __half& hi, __half& lo) {
-  hi = __float2half_rn(xs);
-  lo = __float2half_rn(xs - __half2float(hi));
-}
-
 // byte offset of element (row r, k) in the no-swizzle K-major layout of a
 // tile with R rows (R % 8 == 0), 16-bit elements
 __host__ __device__ __forceinline__ uint32_t kmaj_off(int r, int k, int R) {

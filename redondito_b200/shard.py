@@ -30,21 +30,20 @@ NL_STAGE_DIRECTIONS = 3 * VEC_DIRECTIONS  # u and w synthesised, u x w analysed
 RK3_STAGES = 3
 
 
-def direction_flops(lmax, nz, nlat, nphi, cont=25):
-    """Flops of one scalar 3D transform in one direction."""
+def direction_flops(lmax, nz, nlat, nphi):
+    """Flops of one scalar 3D transform in one direction; nz counts the
+    radial points including the continuation points (the FFT length)."""
     nlm = (lmax + 1) * (lmax + 2) // 2
     leg = 4.0 * nz * (nlat // 2) * nlm
     phi = 2.5 * nphi * math.log2(nphi) * nlat * nz
-    nzc = nz + cont
-    zfft = 5.0 * nzc * math.log2(nzc) * nlm
+    zfft = 5.0 * nz * math.log2(nz) * nlm
     return leg + phi + zfft
 
 
 def problem_flops(lmax, nz, nlat, nphi, nfields=1):
     """A batch problem: per field a 3D inverse, a radial derivative and a 3D forward."""
     nlm = (lmax + 1) * (lmax + 2) // 2
-    nzc = nz + 25
-    return nfields * (2.0 * direction_flops(lmax, nz, nlat, nphi) + 5.0 * nzc * math.log2(nzc) * nlm)
+    return nfields * (2.0 * direction_flops(lmax, nz, nlat, nphi) + 5.0 * nz * math.log2(nz) * nlm)
 
 
 def request_flops(lmax, nz, nlat, nphi, kind, steps=0):

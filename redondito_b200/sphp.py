@@ -47,7 +47,8 @@ SYMBOLS = (
     "sph_timer_enable", "sph_timer_reset", "sph_timer_read",
     "sph_derivr_noalloc", "sph_plan_status", "sph_fftp3d_vec_to_qst", "sph_fftp3d_qst_to_vec",
     "sph_batch_create", "sph_batch_run", "sph_batch_status", "sph_batch_destroy",
-    "sph_plan_set_tiles",
+    "sph_plan_set_tiles", "sph_plan_set_slab", "sph_range",
+    "sph_read_namelist", "sph_write_grids", "sph_energy_spectrum", "sph_run",
 )
 TIMER_CLASSES = ("phi_fwd", "phi_inv", "leg_analysis", "leg_synthesis", "vec_analysis",
                  "vec_synthesis", "zfft", "ops")
@@ -117,6 +118,12 @@ def lib(build_if_missing=True):
             "sph_batch_status": [P],
             "sph_batch_destroy": [P],
             "sph_plan_set_tiles": [P, I, I, I],
+            "sph_plan_set_slab": [P, I, I, I, I],
+            "sph_range": [I, I, I, I, pI, pI],
+            "sph_read_namelist": [ctypes.c_char_p, pI, pI, pI, pI, pD, pD, pD, pI, pI, pI, pD, pI],
+            "sph_write_grids": [P, ctypes.c_char_p],
+            "sph_energy_spectrum": [P, Vp, Vp, pD, Vp],
+            "sph_run": [P, Vp, Vp, Vp, D, D, I, I, I, I, ctypes.c_char_p, pD, Vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -152,7 +159,9 @@ class Plan:
     continuation in z, the device tables and the plan's scratch."""
 
     def __init__(self, lmax, nz, nlat=None, nphi=None, Cz=0, oz=0, rint=0.35, rext=1.0,
-                 tdir=TABLES_DIR, precision=SPH_FP64, device=None):
+                 tdir=TABLES_DIR, precision=SPH_FP64, device=None, dir=None):
+        """dir: the Cz x oz continuation operator, column-major (Cz*oz
+        values); by default it is read from the FC-Gram tables in tdir."""
         if not torch.cuda.is_available():
             raise RuntimeError("redondito_b200 needs a CUDA device (B200, sm_100a)")
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
@@ -163,7 +172,9 @@ class Plan:
         self.precision = precision
         dirp = None
         if Cz > 0:
-            d = load_dirichlet_tables(Cz, oz, tdir)
+            d = load_dirichlet_tables(Cz, oz, tdir) if dir is None else [float(x) for x in dir]
+            if len(d) != Cz * oz:
+                raise ValueError(f"dir must hold Cz*oz = {Cz * oz} values")
             self._dir = (ctypes.c_double * len(d))(*d)
             dirp = self._dir
         h = ctypes.c_void_p()
@@ -173,6 +184,7 @@ class Plan:
         self.h = h
         self.nlm = (lmax + 1) * (lmax + 2) // 2
         self.N = nz - Cz
+        self.k0, self.nzv, self.lm0, self.nlmv = 0, nz, 0, self.nlm
         self._grid_arrays()
         self._bc = False
 
@@ -201,12 +213,16 @@ class Plan:
         except Exception:
             pass
 
-    # allocation helpers
+    # allocation helpers (the caller's slab: see set_slab)
     def new_grid(self):
-        return torch.zeros((self.nz, self.nphi, self.nlat), dtype=torch.float64, device=self.device)
+        return torch.zeros((self.nzv, self.nphi, self.nlat), dtype=torch.float64, device=self.device)
 
     def new_spec(self):
-        return torch.zeros((self.nz, self.nlm), dtype=torch.complex128, device=self.device)
+        return torch.zeros((self.nz, self.nlmv), dtype=torch.complex128, device=self.device)
+
+    def new_plane_spec(self):
+        """per-plane spectra of the caller's planes, (nplanes, nlm)"""
+        return torch.zeros((self.nzv, self.nlm), dtype=torch.complex128, device=self.device)
 
     def lm(self, l, m):
         return m * (2 * self.lmax + 1 - m) // 2 + l
@@ -222,11 +238,34 @@ def _ptr(t, shape, dtype):
 
 
 def _g(plan, t):
-    return _ptr(t, (plan.nz, plan.nphi, plan.nlat), torch.float64)
+    """physical array of the caller's planes: (nplanes, nphi, nlat)"""
+    return _ptr(t, (plan.nzv, plan.nphi, plan.nlat), torch.float64)
 
 
 def _s(plan, t):
-    return _ptr(t, (plan.nz, plan.nlm), torch.complex128)
+    """spectral array of the caller's lm columns: (nz, nlm_local)"""
+    return _ptr(t, (plan.nz, plan.nlmv), torch.complex128)
+
+
+def _sp(plan, t):
+    """per-plane spectra of the caller's planes (the 2D transforms): (nplanes, nlm)"""
+    return _ptr(t, (plan.nzv, plan.nlm), torch.complex128)
+
+
+def set_slab(plan, k0, nplanes, lm0, nlm_local):
+    """The caller's slab (see sph_plan_set_slab): planes [k0, k0+nplanes) for
+    the 2D transforms, lm columns [lm0, lm0+nlm_local) for the z transforms,
+    operators and boundary.  set_slab(plan, 0, nz, 0, nlm) restores the
+    whole field."""
+    _call("sph_plan_set_slab", plan.h, int(k0), int(nplanes), int(lm0), int(nlm_local))
+    plan.k0, plan.nzv, plan.lm0, plan.nlmv = int(k0), int(nplanes), int(lm0), int(nlm_local)
+
+
+def range_(n1, n2, nprocs, irank):
+    """range (src/sphp/sphp_sca.F90:596-626): (ista, iend), inclusive."""
+    a, b = ctypes.c_int(), ctypes.c_int()
+    _call("sph_range", int(n1), int(n2), int(nprocs), int(irank), ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value
 
 
 def _stream(stream=None):
@@ -236,11 +275,11 @@ def _stream(stream=None):
 
 # ---------------------------------------------------------------- transforms
 def fftp2d_real_to_complex_xy(plan, in_, out, stream=None):
-    _call("sph_fftp2d_real_to_complex_xy", plan.h, _g(plan, in_), _s(plan, out), _stream(stream))
+    _call("sph_fftp2d_real_to_complex_xy", plan.h, _g(plan, in_), _sp(plan, out), _stream(stream))
 
 
 def fftp2d_complex_to_real_xy(plan, in_, out, stream=None):
-    _call("sph_fftp2d_complex_to_real_xy", plan.h, _s(plan, in_), _g(plan, out), _stream(stream))
+    _call("sph_fftp2d_complex_to_real_xy", plan.h, _sp(plan, in_), _g(plan, out), _stream(stream))
 
 
 def fftp1d_real_to_complex_z(plan, inout, stream=None):
@@ -262,11 +301,11 @@ def fftp3d_complex_to_real(plan, in_, out, stream=None):
 
 def fftp2d_vec_to_qst(plan, vr, vt, vp, q, s, t, stream=None):
     _call("sph_fftp2d_vec_to_qst", plan.h, _g(plan, vr), _g(plan, vt), _g(plan, vp),
-          _s(plan, q), _s(plan, s), _s(plan, t), _stream(stream))
+          _sp(plan, q), _sp(plan, s), _sp(plan, t), _stream(stream))
 
 
 def fftp2d_qst_to_vec(plan, q, s, t, vr, vt, vp, stream=None):
-    _call("sph_fftp2d_qst_to_vec", plan.h, _s(plan, q), _s(plan, s), _s(plan, t),
+    _call("sph_fftp2d_qst_to_vec", plan.h, _sp(plan, q), _sp(plan, s), _sp(plan, t),
           _g(plan, vr), _g(plan, vt), _g(plan, vp), _stream(stream))
 
 
@@ -369,6 +408,43 @@ def rk3_step(plan, Z, W, phi, nu, dt, stream=None, energy=True):
     e = ctypes.c_double(0.0)
     _call("sph_rk3_step", plan.h, _s(plan, Z), _s(plan, W), _s(plan, phi), float(nu), float(dt),
           ctypes.byref(e) if energy else None, _stream(stream))
+    return e.value
+
+
+# ---------------------------------------------------------------- run loop
+def read_namelist(path):
+    """&grid, &boxparams and the optional &run group (see sph_read_namelist)."""
+    ints = {k: ctypes.c_int() for k in ("lmax", "nz", "Cz", "oz", "step", "tstep", "sstep", "filter")}
+    dbls = {k: ctypes.c_double() for k in ("rint", "rext", "dt", "nu")}
+    _call("sph_read_namelist", os.fsencode(path), *(ctypes.byref(ints[k]) for k in ("lmax", "nz", "Cz", "oz")),
+          ctypes.byref(dbls["rint"]), ctypes.byref(dbls["rext"]), ctypes.byref(dbls["dt"]),
+          *(ctypes.byref(ints[k]) for k in ("step", "tstep", "sstep")), ctypes.byref(dbls["nu"]),
+          ctypes.byref(ints["filter"]))
+    out = {k: v.value for k, v in ints.items()}
+    out.update({k: v.value for k, v in dbls.items()})
+    out["filter"] = bool(out["filter"])
+    return out
+
+
+def write_grids(plan, dir):
+    """theta.txt, phi.txt, z.txt in dir (box_init's grid files)."""
+    _call("sph_write_grids", plan.h, os.fsencode(dir))
+
+
+def energy_spectrum(plan, Z, W, stream=None):
+    """Kinetic energy per degree: a list of (toroidal, poloidal) for l = 0..lmax."""
+    out = (ctypes.c_double * (2 * (plan.lmax + 1)))()
+    _call("sph_energy_spectrum", plan.h, _s(plan, Z), _s(plan, W), out, _stream(stream))
+    return [(out[2 * l], out[2 * l + 1]) for l in range(plan.lmax + 1)]
+
+
+def run(plan, Z, W, phi, nu, dt, nsteps, tstep=1, sstep=0, filter=False, outdir=None, stream=None):
+    """nsteps RK3 steps with the optional filter and outputs (see sph_run);
+    returns the energy of the final state."""
+    e = ctypes.c_double(0.0)
+    _call("sph_run", plan.h, _s(plan, Z), _s(plan, W), _s(plan, phi), float(nu), float(dt), int(nsteps),
+          int(tstep), int(sstep), int(bool(filter)), os.fsencode(outdir) if outdir else None, ctypes.byref(e),
+          _stream(stream))
     return e.value
 
 

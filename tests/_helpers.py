@@ -23,3 +23,12 @@ def random_spec(P, rng, power=2.0, radial=True):
         prof = radial_profile(P.z, P.rint, P.rext, rng)
         return prof[:, None] * a[None, :]
     return np.repeat(a[None, :], P.nz, axis=0) * (1.0 + np.arange(P.nz))[:, None]
+
+
+def check(err, tol, label=""):
+    """Assert err < tol and print the measured figure (run pytest with -s to
+    see every one): 'ERR <test>:<line> [label] <err> < <tol>'."""
+    import inspect
+    fr = inspect.stack()[1]
+    print(f"ERR {fr.function}:{fr.lineno} {label} {err:.3e} < {tol:.0e}", flush=True)
+    assert err < tol, f"{fr.function}:{fr.lineno} {label}: {err:.3e} >= {tol:.0e}"

@@ -47,3 +47,22 @@ def test_fcgram_tables_match_generator_definition():
     A = np.fromfile(os.path.join(S.TABLES_DIR, "A25-5.dat")).reshape(5, 25).T
     Q = np.fromfile(os.path.join(S.TABLES_DIR, "Q5.dat")).reshape(5, 5).T
     assert np.abs(d - A @ Q.T).max() < 1e-12
+
+
+def test_range_matches_the_reference_rule():
+    """sph_range against range (src/sphp/sphp_sca.F90:596-626) restated here:
+    the parts tile [n1, n2] in order, sizes differ by at most one, the
+    first mod(n, nprocs) ranks take the extra element."""
+    from redondito_b200 import sphp as S
+    for n1, n2 in ((1, 1), (1, 7), (0, 63), (1, 131328), (5, 4)):
+        for nprocs in range(1, 7):
+            parts = [S.range_(n1, n2, nprocs, r) for r in range(nprocs)]
+            n = n2 - n1 + 1
+            w1, w2 = divmod(n, nprocs)
+            for r, (a, b) in enumerate(parts):
+                ista = r * w1 + n1 + min(r, w2)
+                iend = ista + w1 - 1 + (1 if w2 > r else 0)
+                assert (a, b) == (ista, iend)
+            assert parts[0][0] == n1 and parts[-1][1] == n2
+            for (a0, b0), (a1, b1) in zip(parts, parts[1:]):
+                assert a1 == b0 + 1

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from tests._helpers import rel_l2, random_spec
+from tests._helpers import check, rel_l2, random_spec
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
@@ -71,9 +71,9 @@ def test_batch_equals_single_plan_calls(precision):
             if precision == "fp64":
                 P = orcs[p]
                 sr = P.z_inverse(x)
-                assert rel_l2(host(g), P.sh_synthesis(sr)) < TOL_CONT
-                assert rel_l2(host(d), P.derivr(sr, 1)) < TOL_DERIV
-                assert rel_l2(host(out), P.forward_3d(P.sh_synthesis(sr))) < TOL_CONT
+                check(rel_l2(host(g), P.sh_synthesis(sr)), TOL_CONT)
+                check(rel_l2(host(d), P.derivr(sr, 1)), TOL_DERIV)
+                check(rel_l2(host(out), P.forward_3d(P.sh_synthesis(sr))), TOL_CONT)
 
 
 def test_batch_replays():
@@ -91,7 +91,7 @@ def test_batch_replays():
         B.status()
         for f, y in enumerate(ys):
             ref = P.sh_synthesis(P.z_inverse(y))
-            assert rel_l2(host(B.grid[0][f]), ref) < 1e-6
+            check(rel_l2(host(B.grid[0][f]), ref), 1e-6)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
@@ -116,8 +116,8 @@ def test_tile_shapes_do_not_change_results(precision):
     g2, o2 = run()
     tol = 1e-13 if precision == "fp64" else 1e-9
     for g, o in ((g1, o1), (g2, o2)):
-        assert rel_l2(g, g0) < tol
-        assert rel_l2(o, o0) < tol
+        check(rel_l2(g, g0), tol)
+        check(rel_l2(o, o0), tol)
     with pytest.raises(S.SphError):
         S.set_tiles(G, 48, 0, 0)
     with pytest.raises(S.SphError):
