@@ -71,13 +71,40 @@ typedef struct sph_plan sph_plan;
 int sph_plan_create(sph_plan** plan, int lmax, int nlat, int nphi, int nz, int Cz, int oz,
                     double rint, double rext, const double* dir, int precision);
 
-/* fcgram_destroy_plan (src/sphp/fcgram_mod.f90:153-182). */
+/* fcgram_destroy_plan (src/sphp/fcgram_mod.f90:153-182).  A plan's tables
+ * outlive it while clones share them. */
 int sph_plan_destroy(sph_plan* plan);
+
+/* A second plan of the same sizes and precision (no reference counterpart:
+ * a reference plan owns everything).  It shares src's read-only device
+ * tables -- the Legendre tables, FFT twiddles, work lists, the tensor-core
+ * table tiles and, once either plan has called sph_setup_bc, the boundary
+ * matrices -- and allocates only its own scratch, so it costs a fraction of
+ * sph_plan_create's memory and none of its host table work.  The two plans
+ * may run concurrently on different streams (each has its own scratch).
+ * The tables are freed with the last plan that shares them.  sph_setup_bc
+ * on the clone is still required before boundary and NL calls (cheap when
+ * the tables hold the matrices).  sph_plan_set_tiles cannot change the MMA
+ * rows of a plan whose tables are shared (SPH_EINVAL). */
+int sph_plan_clone(const sph_plan* src, sph_plan** plan);
 
 /* load_dirichlet_tables (src/sphp/fcgram_mod.f90:186-263): reads
  * tdir/A{C}-{d}.dat and tdir/Q{d}.dat (raw column-major float64) and writes
  * dir = A.Q^T (C x d, column-major) to the host array dir. */
 int sph_fcgram_load_tables(const char* tdir, int C, int d, double* dir);
+
+/* load_neumann_tables (src/sphp/fcgram_mod.f90:267-365): reads tdir/Q{d}.dat
+ * and tdir/Q{ord}n{d}.dat (its first double the tables' grid spacing dxp,
+ * then d x d column-major) and writes to the host array neu (d values) the
+ * reconstructor neu = Q(d,:).Qn^T, its last entry scaled by (dx/dxp)^ord:
+ * the boundary value from the ord-th (1 or 2) outward normal derivative and
+ * the d-1 values inside.  dx: the radial grid step of the plan it serves. */
+int sph_fcgram_load_neumann_tables(const char* tdir, int d, int ord, double dx, double* neu);
+
+/* The plan's Neumann reconstructors (host arrays of oz values; either may be
+ * NULL to keep the current one), needed by sph_neumann_reconstruct,
+ * sph_robin_reconstruct and the freeslip boundary kind. */
+int sph_plan_set_neumann(sph_plan* plan, const double* neu1, const double* neu2);
 
 /* Sizes of a plan: nlm, and the element counts of one physical field
  * (nlat*nphi*nz doubles) and one spectral field (nlm*nz complex). */
@@ -219,16 +246,35 @@ int sph_prodvec(sph_plan* plan, const double* ar, const double* at, const double
  * src/boundary/boundary_mod.f90, src/boundary/vboundary.f90 */
 
 /* setup_bc / v_setup / invDl_setup (boundary_mod.f90:35-59,140-241;
- * vboundary.f90:34-56): bcint, bcext = "noslip" (the only type).  Builds the
- * FC-Gram derivative matrices, the row-scaled LU per l in FP64 on the host,
- * and uploads M_l (N x (N-4) per l) and the d2/dr2 border rows. */
+ * vboundary.f90:34-56): the kinds of the inner (bcint) and outer (bcext)
+ * wall, parsed like v_parsebc (vboundary.f90:10-31):
+ *   "noslip"   (the reference's only kind)  W = dW/dr = Z = 0;
+ *   "freeslip" (no reference counterpart; stress-free, no penetration)
+ *              W = 0, W'' - 2 W'/r = 0, Z' - 2 Z/r = 0, the last by the
+ *              Robin reconstruction (needs sph_plan_set_neumann, else
+ *              SPH_ENOTREADY).
+ * Builds the FC-Gram derivative matrices, the row-scaled LU per l in FP64
+ * on the host (rows 2 and N-1 of B_l by the kind of their wall), and uploads
+ * M_l (N x (N-4) per l) and the d2/dr2 border rows; a clone whose source
+ * built them for the same kinds shares them. */
 int sph_setup_bc(sph_plan* plan, const char* bcint, const char* bcext);
+/* neumann_reconstruct (src/sphp/fcgram_mod.f90:368-520, the z boundaries)
+ * on spectral (nlm, nz) f: boun 0 = inner wall (z index 0), 1 = outer wall
+ * (index nz - Cz - 1); on input the wall row holds the ord-th outward normal
+ * derivative g, on output the reconstructed value; other rows unchanged. */
+int sph_neumann_reconstruct(sph_plan* plan, double* f, int boun, int ord, void* stream);
+/* robin_reconstruct (fcgram_mod.f90:523-650): f' + a f = g at the wall, g in
+ * the wall row on input; a: DEVICE array of nlm real coefficients (one per
+ * lm column, the reference's a over the other coordinates). */
+int sph_robin_reconstruct(sph_plan* plan, double* f, int boun, const double* a, void* stream);
 /* dirichlet (boundary_mod.f90:62-93): a(lm,1) = a(lm,N) = 0 */
 int sph_dirichlet(sph_plan* plan, double* a, void* stream);
 /* invDl (boundary_mod.f90:244-292): W = M_l phi(3:N-2), batched FP64 GEMM on
  * the device; l = 0 and the continuation points are zero. */
 int sph_invDl(sph_plan* plan, const double* phi, double* w, void* stream);
-/* v_imposebc (vboundary.f90:59-87): dirichlet(tor), pol = invDl(phi), phi = D_l pol */
+/* v_imposebc (vboundary.f90:59-87): dirichlet(tor) (freeslip walls: the
+ * Robin reconstruction of Z' - 2Z/r = 0 instead), pol = invDl(phi),
+ * phi = D_l pol */
 int sph_v_imposebc(sph_plan* plan, double* tor, double* phi, double* pol, void* stream);
 /* v_imposebc_fast (vboundary.f90:90-130): phi recomputed at rows 1,2,N-1,N only */
 int sph_v_imposebc_fast(sph_plan* plan, double* tor, double* phi, double* pol, void* stream);

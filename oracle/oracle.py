@@ -63,6 +63,12 @@ def lib():
         L.orc_rk3_step.argtypes = [P, D, D, D, ctypes.c_double, ctypes.c_double, D]
         L.orc_velocity.argtypes = [P] + [D] * 9
         L.orc_energy_spectrum.argtypes = [P, D, D, D]
+        L.orc_load_neumann_tables.argtypes = [ctypes.c_char_p, I, I, ctypes.c_double, D]
+        L.orc_set_neumann.argtypes = [P, D, D]
+        L.orc_set_neumann.restype = None
+        L.orc_neumann_reconstruct.argtypes = [P, D, I, I]
+        L.orc_robin_reconstruct.argtypes = [P, D, I, D]
+        L.orc_bc_setup_kinds.argtypes = [P, I, I]
         for name in ("orc_plan_destroy", "orc_set_threads", "orc_grid", "orc_sh_analysis",
                      "orc_sh_synthesis", "orc_qst_analysis", "orc_qst_synthesis", "orc_z_forward",
                      "orc_z_inverse", "orc_3d_forward", "orc_3d_inverse", "orc_laplang",
@@ -92,6 +98,14 @@ def load_dir(C=25, d=5, tdir=TABLES_DIR):
     rc = lib().orc_load_dirichlet_tables(tdir.encode(), C, d, _p(out))
     if rc:
         raise FileNotFoundError(f"FC-Gram tables A{C}-{d}.dat/Q{d}.dat not readable in {tdir}")
+    return out
+
+
+def load_neumann(d=5, ord=1, dx=1.0, tdir=TABLES_DIR):
+    out = np.zeros(d)
+    rc = lib().orc_load_neumann_tables(tdir.encode(), d, ord, float(dx), _p(out))
+    if rc:
+        raise FileNotFoundError(f"Neumann tables Q{d}.dat/Q{ord}n{d}.dat not readable in {tdir} ({rc})")
     return out
 
 
@@ -130,6 +144,11 @@ class Plan:
                        self.emm.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
         self.phi = 2 * np.pi * np.arange(self.nphi) / self.nphi
         self._bc = False
+        self.dz = (rext - rint) / (nz - C - 1) if nz - C > 1 else 1.0
+        self.neu = None
+        if C > 0 and os.path.exists(os.path.join(TABLES_DIR, f"Q1n{d}.dat")):
+            self.neu = (load_neumann(d, 1, self.dz), load_neumann(d, 2, self.dz))
+            lib().orc_set_neumann(self.h, _p(self.neu[0]), _p(self.neu[1]))
 
     def __del__(self):
         try:
@@ -278,12 +297,36 @@ class Plan:
         lib().orc_dirichlet(self.h, _p(s.view(np.float64)))
         return s
 
-    def bc_setup(self):
-        if not self._bc:
-            rc = lib().orc_bc_setup(self.h)
+    def bc_setup(self, kinds=None):
+        """Boundary kinds at the inner and outer wall: noslip or freeslip
+        (None: keep the kinds set up, noslip if none)."""
+        code = {"noslip": 0, "freeslip": 1}
+        if kinds is None:
+            if self._bc:
+                return
+            kinds = ("noslip", "noslip")
+        k = (code[kinds[0]], code[kinds[1]])
+        if not self._bc or getattr(self, "_bck", (0, 0)) != k:
+            rc = lib().orc_bc_setup_kinds(self.h, *k)
             if rc:
                 raise ValueError(f"bc_setup failed ({rc})")
             self._bc = True
+            self._bck = k
+
+    def neumann_reconstruct(self, a, boun, ord=1):
+        """The boundary row (boun 0 inner, 1 outer) of a copy of a, from the
+        ord-th outward normal derivative held there."""
+        s = np.array(a, dtype=np.complex128, order="C", copy=True)
+        if lib().orc_neumann_reconstruct(self.h, _p(s.view(np.float64)), boun, ord):
+            raise ValueError("neumann_reconstruct failed")
+        return s
+
+    def robin_reconstruct(self, a, boun, coef):
+        s = np.array(a, dtype=np.complex128, order="C", copy=True)
+        c = np.ascontiguousarray(np.broadcast_to(np.asarray(coef, dtype=np.float64), (self.nlm,)))
+        if lib().orc_robin_reconstruct(self.h, _p(s.view(np.float64)), boun, _p(c)):
+            raise ValueError("robin_reconstruct failed")
+        return s
 
     def derivr_mat(self, order):
         d = np.zeros((self.N, self.N), order="F")

@@ -93,7 +93,11 @@ struct orc_plan {
   std::vector<double> dir;               // C*d col-major
   std::vector<int> ell, emm, mbase;      // nlm, nlm, lmax+2
   OFFT fphi, fz;
-  // boundary
+  // Neumann reconstructors (fcgram_mod.f90:267-365): neu[0] first, neu[1]
+  // second normal derivative, d values each (empty: not loaded)
+  std::vector<double> neu[2];
+  // boundary: kinds at the inner and outer wall (0 noslip, 1 freeslip)
+  int bck[2] = {0, 0};
   int bc_ready = 0;
   std::vector<double> binv;   // N x (N-4) x lmax
   std::vector<double> d2bor;  // 4 x N (col-major: d2bor[k + 4*j])
@@ -729,6 +733,92 @@ static void lu_solve(int n, const double* a, const int* piv, double* b, int nrhs
 }
 
 // invDl_setup (boundary_mod.f90:140-241)
+// load_neumann_tables (fcgram_mod.f90:267-365): neu = Q(d,:) . Qn^T from
+// Q{d}.dat and Q{ord}n{d}.dat (its first double the tables' spacing dxp),
+// the last entry scaled by (dx/dxp)^ord.  0 on success.
+extern "C" int orc_load_neumann_tables(const char* tdir, int d, int ord, double dx, double* neu) {
+  if (ord != 1 && ord != 2) return 3;
+  std::vector<double> Q((size_t)d * d), Qn((size_t)d * d);
+  char path[4096];
+  snprintf(path, sizeof path, "%s/Q%d.dat", tdir, d);
+  FILE* f = fopen(path, "rb");
+  if (!f) return 1;
+  size_t got = fread(Q.data(), sizeof(double), Q.size(), f);
+  fclose(f);
+  if (got != Q.size()) return 2;
+  snprintf(path, sizeof path, "%s/Q%dn%d.dat", tdir, ord, d);
+  f = fopen(path, "rb");
+  if (!f) return 1;
+  double dxp = 0.0;
+  got = fread(&dxp, sizeof(double), 1, f);
+  got += fread(Qn.data(), sizeof(double), Qn.size(), f);
+  fclose(f);
+  if (got != Qn.size() + 1 || dxp <= 0.0) return 2;
+  // neu(k) = sum_j Q(d, j) Qn(k, j)   (column-major Q(i,j) = Q[i-1 + d (j-1)])
+  for (int k = 0; k < d; ++k) {
+    double acc = 0.0;
+    for (int j = 0; j < d; ++j) acc += Q[(d - 1) + (size_t)d * j] * Qn[k + (size_t)d * j];
+    neu[k] = acc;
+  }
+  neu[d - 1] *= ord == 1 ? dx / dxp : (dx / dxp) * (dx / dxp);
+  return 0;
+}
+
+extern "C" void orc_set_neumann(orc_plan* p, const double* neu1, const double* neu2) {
+  if (neu1) p->neu[0].assign(neu1, neu1 + p->d);
+  if (neu2) p->neu[1].assign(neu2, neu2 + p->d);
+}
+
+// The boundary value of one column from its outward normal derivative (of
+// order ord) held at the boundary point and the d-1 values inside, as
+// neumann_reconstruct (fcgram_mod.f90:368-520, z boundaries 5 and 6, in the
+// reference's summation order); with `a`, robin_reconstruct
+// (fcgram_mod.f90:523-650): f' + a f = g, g held at the boundary point.
+static cplx reconstruct_one(const orc_plan* p, const cplx* f, int nlm, int boun, const double* neu, bool robin,
+                            double a) {
+  const int d = p->d, n = p->N;
+  const int b = boun == 0 ? 0 : n - 1;
+  cplx acc = neu[d - 1] * f[(size_t)b * nlm];
+  for (int k = 1; k <= d - 1; ++k) {
+    const int row = boun == 0 ? d - k : n - 1 - d + k;  // 0-based: point d+1-k, or N-d+k
+    acc = acc + neu[k - 1] * f[(size_t)row * nlm];
+  }
+  if (robin) acc = acc / (a * neu[d - 1] + 1.0);
+  return acc;
+}
+
+extern "C" int orc_neumann_reconstruct(const orc_plan* p, double* spec, int boun, int ord) {
+  if ((boun != 0 && boun != 1) || (ord != 1 && ord != 2) || p->neu[ord - 1].empty()) return 1;
+  cplx* F = reinterpret_cast<cplx*>(spec);
+  const int b = boun == 0 ? 0 : p->N - 1;
+  for (int lm = 0; lm < p->nlm; ++lm)
+    F[(size_t)b * p->nlm + lm] = reconstruct_one(p, F + lm, p->nlm, boun, p->neu[ord - 1].data(), false, 0.0);
+  return 0;
+}
+
+extern "C" int orc_robin_reconstruct(const orc_plan* p, double* spec, int boun, const double* a) {
+  if ((boun != 0 && boun != 1) || p->neu[0].empty()) return 1;
+  cplx* F = reinterpret_cast<cplx*>(spec);
+  const int b = boun == 0 ? 0 : p->N - 1;
+  for (int lm = 0; lm < p->nlm; ++lm)
+    F[(size_t)b * p->nlm + lm] = reconstruct_one(p, F + lm, p->nlm, boun, p->neu[0].data(), true, a[lm]);
+  return 0;
+}
+
+// Boundary kinds per wall (inner, outer): 0 noslip (v_parsebc's only type,
+// vboundary.f90:10-31): Z = W = dW/dr = 0; 1 freeslip (stress-free, no
+// penetration): W = 0, W'' - 2 W'/r = 0, Z' - 2 Z/r = 0 (the toroidal
+// condition by robin_reconstruct, a = +2/rint inside, -2/rext outside, with
+// the outward normal derivative).
+extern "C" int orc_bc_setup_kinds(orc_plan* p, int kint, int kext) {
+  if (kint < 0 || kint > 1 || kext < 0 || kext > 1) return 3;
+  if ((kint == 1 || kext == 1) && p->neu[0].empty()) return 4;
+  p->bck[0] = kint;
+  p->bck[1] = kext;
+  p->bc_ready = 0;
+  return orc_bc_setup(p);
+}
+
 extern "C" int orc_bc_setup(orc_plan* p) {
   const int n = p->N, lmax = p->lmax;
   if (n < 6 || p->C <= 0) return 1;
@@ -743,12 +833,13 @@ extern "C" int orc_bc_setup(orc_plan* p) {
   for (int l = 1; l <= lmax; ++l) {
     std::fill(b.begin(), b.end(), 0.0);
     B(1, 1) = 1.0;
-    for (int j = 1; j <= n; ++j) B(2, j) = D1(1, j);
+    // row 2: W' = 0 (noslip) or W'' - 2 W'/r = 0 (freeslip) at the inner wall
+    for (int j = 1; j <= n; ++j) B(2, j) = p->bck[0] ? D2(1, j) - 2.0 / p->z[0] * D1(1, j) : D1(1, j);
     for (int i = 3; i <= n - 2; ++i) {
       for (int j = 1; j <= n; ++j) B(i, j) = D2(i, j);
       B(i, i) = B(i, i) - (double)(l * (l + 1)) / (p->z[i - 1] * p->z[i - 1]);
     }
-    for (int j = 1; j <= n; ++j) B(n - 1, j) = D1(n, j);
+    for (int j = 1; j <= n; ++j) B(n - 1, j) = p->bck[1] ? D2(n, j) - 2.0 / p->z[n - 1] * D1(n, j) : D1(n, j);
     B(n, n) = 1.0;
     for (int i = 1; i <= n; ++i) {
       double mx = 0;
@@ -798,8 +889,22 @@ extern "C" void orc_invDl(const orc_plan* p, const double* phi, double* w) {
 }
 
 // v_imposebc / v_imposebc_fast (vboundary.f90:59-130)
+// The toroidal condition of each wall: Z = 0 (noslip) or the Robin
+// reconstruction of Z' - 2 Z/r = 0 (freeslip, g = 0).
+static void toroidal_bc(const orc_plan* p, double* tor) {
+  cplx* T = reinterpret_cast<cplx*>(tor);
+  for (int w = 0; w < 2; ++w) {
+    const int b = w == 0 ? 0 : p->N - 1;
+    const double a = w == 0 ? 2.0 / p->z[0] : -2.0 / p->z[p->N - 1];
+    for (int lm = 0; lm < p->nlm; ++lm) {
+      T[(size_t)b * p->nlm + lm] = 0.0;
+      if (p->bck[w]) T[(size_t)b * p->nlm + lm] = reconstruct_one(p, T + lm, p->nlm, w, p->neu[0].data(), true, a);
+    }
+  }
+}
+
 extern "C" void orc_imposebc(const orc_plan* p, double* tor, double* phi, double* pol, int fast) {
-  orc_dirichlet(p, tor);
+  toroidal_bc(p, tor);
   orc_invDl(p, phi, pol);
   if (!fast) { orc_dlr(p, pol, phi); return; }
   const int n = p->N, nlm = p->nlm, nz = p->nz;

@@ -76,6 +76,19 @@ void orc_prodvec(const orc_plan* p, const double* ar, const double* at,
 
 /* Boundary (src/boundary/boundary_mod.f90, vboundary.f90). */
 int orc_bc_setup(orc_plan* p);
+/* load_neumann_tables (src/sphp/fcgram_mod.f90:267-365): neu (d values) for
+ * the reconstruction from the ord-th normal derivative, dx the grid step.
+ * 0 on success. */
+int orc_load_neumann_tables(const char* tdir, int d, int ord, double dx, double* neu);
+void orc_set_neumann(orc_plan* p, const double* neu1, const double* neu2);
+/* neumann_reconstruct / robin_reconstruct (fcgram_mod.f90:368-650) on the
+ * z boundaries of spec (nz x nlm): boun 0 inner (z index 0), 1 outer (N-1);
+ * the boundary row holds g on input, the reconstructed value on output;
+ * a: nlm Robin coefficients.  0 on success. */
+int orc_neumann_reconstruct(const orc_plan* p, double* spec, int boun, int ord);
+int orc_robin_reconstruct(const orc_plan* p, double* spec, int boun, const double* a);
+/* Boundary kinds (inner, outer): 0 noslip, 1 freeslip; then bc_setup. */
+int orc_bc_setup_kinds(orc_plan* p, int kint, int kext);
 void orc_dirichlet(const orc_plan* p, double* a);
 void orc_derivr_mat(const orc_plan* p, int order, double* d /* N x N col-major */);
 void orc_invDl(const orc_plan* p, const double* phi, double* w);

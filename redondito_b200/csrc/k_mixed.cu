@@ -1478,16 +1478,29 @@ int mixed_setup(sph_plan* p, const std::vector<double>& hP, const std::vector<do
       nsyn += (long long)ncb * ntiles_of(lmax, m, par);
     }
   p->Tsynfield = (size_t)nsyn * TILE_HALVES;
-  const size_t nana = ana_tile(lmax, ncb, nkn, SPH_MAX_FIELDS, 0, 0, 0, 0) * TILE_HALVES;
-  const size_t bytes_ana = nana * 2, bytes_syn = (size_t)SPH_MAX_FIELDS * p->Tsynfield * 2;
-  if (rc == SPH_OK && cudaMalloc((void**)&p->Tana, bytes_ana) != cudaSuccess) rc = SPH_ENOMEM;
-  if (rc == SPH_OK && cudaMemset(p->Tana, 0, bytes_ana) != cudaSuccess) rc = SPH_ECUDA;
-  if (rc == SPH_OK && cudaMalloc((void**)&p->Tsyn, std::max<size_t>(16, bytes_syn)) != cudaSuccess) rc = SPH_ENOMEM;
-  if (rc == SPH_OK && cudaMemset(p->Tsyn, 0, std::max<size_t>(16, bytes_syn)) != cudaSuccess) rc = SPH_ECUDA;
   if (rc == SPH_OK && cudaMalloc((void**)&p->d_toff, off.size() * sizeof(long long)) != cudaSuccess) rc = SPH_ENOMEM;
   if (rc == SPH_OK &&
       cudaMemcpy(p->d_toff, off.data(), off.size() * sizeof(long long), cudaMemcpyHostToDevice) != cudaSuccess)
     rc = SPH_ECUDA;
+  if (rc == SPH_OK) rc = mixed_alloc_scratch(p);
+  int dev = 0;
+  if (rc == SPH_OK && (cudaGetDevice(&dev) != cudaSuccess ||
+                       cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess))
+    rc = SPH_ECUDA;
+  return rc;
+}
+
+// The per-plan buffers: analysis and synthesis data tiles, the physically
+// continued planes, the two-pass phi images and the status word.
+int mixed_alloc_scratch(sph_plan* p) {
+  const int lmax = p->lmax, ncb = (p->nz + PLANES - 1) / PLANES;
+  const size_t nana = ana_tile(lmax, ncb, p->nkn, SPH_MAX_FIELDS, 0, 0, 0, 0) * TILE_HALVES;
+  const size_t bytes_ana = nana * 2, bytes_syn = (size_t)SPH_MAX_FIELDS * p->Tsynfield * 2;
+  int rc = SPH_OK;
+  if (rc == SPH_OK && cudaMalloc((void**)&p->Tana, bytes_ana) != cudaSuccess) rc = SPH_ENOMEM;
+  if (rc == SPH_OK && cudaMemset(p->Tana, 0, bytes_ana) != cudaSuccess) rc = SPH_ECUDA;
+  if (rc == SPH_OK && cudaMalloc((void**)&p->Tsyn, std::max<size_t>(16, bytes_syn)) != cudaSuccess) rc = SPH_ENOMEM;
+  if (rc == SPH_OK && cudaMemset(p->Tsyn, 0, std::max<size_t>(16, bytes_syn)) != cudaSuccess) rc = SPH_ECUDA;
   if (rc == SPH_OK && p->C > 0 && p->d <= 32 &&
       cudaMalloc((void**)&p->contg, (size_t)SPH_MAX_FIELDS * p->C * p->nphi * p->nlat * sizeof(double)) !=
           cudaSuccess)
@@ -1501,10 +1514,6 @@ int mixed_setup(sph_plan* p, const std::vector<double>& hP, const std::vector<do
   }
   if (rc == SPH_OK && cudaMalloc((void**)&p->dflag, sizeof(int)) != cudaSuccess) rc = SPH_ENOMEM;
   if (rc == SPH_OK && cudaMemset(p->dflag, 0, sizeof(int)) != cudaSuccess) rc = SPH_ECUDA;
-  int dev = 0;
-  if (rc == SPH_OK && (cudaGetDevice(&dev) != cudaSuccess ||
-                       cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess))
-    rc = SPH_ECUDA;
   return rc;
 }
 
@@ -1524,14 +1533,19 @@ int mixed_retile(sph_plan* p) {
   return build_sets(p, hP, none, none, true, false);
 }
 
-void mixed_free(sph_plan* p) {
+void mixed_free_tables(sph_plan* p) {
   for (TcSet* s : {&p->tcAS, &p->tcAV, &p->tcSS, &p->tcSV}) {
     if (s->items) cudaFree(s->items);
     if (s->blocks) cudaFree(s->blocks);
     s->items = nullptr;
     s->blocks = nullptr;
   }
-  void* ptrs[] = {p->dflag, p->Tana, p->Tsyn, p->d_toff, p->contg, p->phi2};
+  if (p->d_toff) cudaFree(p->d_toff);
+  p->d_toff = nullptr;
+}
+
+void mixed_free_scratch(sph_plan* p) {
+  void* ptrs[] = {p->dflag, p->Tana, p->Tsyn, p->contg, p->phi2};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   p->phi2 = nullptr;
@@ -1540,7 +1554,6 @@ void mixed_free(sph_plan* p) {
   p->dflag = nullptr;
   p->Tana = nullptr;
   p->Tsyn = nullptr;
-  p->d_toff = nullptr;
 }
 
 int mixed_status(const sph_plan* p) {

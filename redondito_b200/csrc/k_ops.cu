@@ -83,6 +83,51 @@ __global__ void dirichlet_kernel(double2* a, int nlm, int N) {
   }
 }
 
+// One wall value of column lm from the d-1 values inside it, the reference's
+// reconstruction loop (fcgram_mod.f90:368-650, z boundaries): acc = neu(d) g
+// + sum_k neu(k) f(interior k), divided by a neu(d) + 1 for Robin.  Rows
+// (0-based) of the interior points: d - k at the inner wall, N - 1 - d + k at
+// the outer one.
+__device__ __forceinline__ double2 reconstruct_col(const double2* f, int lm, int nlm, int N, int d, int boun,
+                                                   const double* neu, bool robin, double a, double2 g) {
+  double2 acc = cscale(g, neu[d - 1]);
+  for (int k = 1; k <= d - 1; ++k) {
+    const int row = boun == 0 ? d - k : N - 1 - d + k;
+    const double2 v = f[(size_t)row * nlm + lm];
+    acc = make_double2(acc.x + neu[k - 1] * v.x, acc.y + neu[k - 1] * v.y);
+  }
+  if (robin) {
+    const double s = a * neu[d - 1] + 1.0;
+    acc = make_double2(acc.x / s, acc.y / s);
+  }
+  return acc;
+}
+
+__global__ void reconstruct_kernel(double2* f, const double* __restrict__ neu, const double* __restrict__ a,
+                                   int nlm, int N, int d, int boun, int robin) {
+  for (int lm = blockIdx.x * blockDim.x + threadIdx.x; lm < nlm; lm += gridDim.x * blockDim.x) {
+    const int b = boun == 0 ? 0 : N - 1;
+    const double2 g = f[(size_t)b * nlm + lm];
+    f[(size_t)b * nlm + lm] = reconstruct_col(f, lm, nlm, N, d, boun, neu, robin != 0, robin ? a[lm] : 0.0, g);
+  }
+}
+
+// the toroidal condition at both walls: Z = 0 (noslip), or Z' - 2 Z/r = 0
+// (freeslip) by the Robin reconstruction with g = 0, a = +2/rint inside and
+// -2/rext outside (outward normal derivatives)
+__global__ void bc_walls_kernel(double2* tor, const double* __restrict__ neu, int nlm, int N, int d, int kin,
+                                int kout, double ain, double aout) {
+  for (int lm = blockIdx.x * blockDim.x + threadIdx.x; lm < nlm; lm += gridDim.x * blockDim.x) {
+    for (int w = 0; w < 2; ++w) {
+      const int b = w == 0 ? 0 : N - 1;
+      const int kind = w == 0 ? kin : kout;
+      double2 v = make_double2(0.0, 0.0);
+      if (kind == 1) v = reconstruct_col(tor, lm, nlm, N, d, w, neu, true, w == 0 ? ain : aout, v);
+      tor[(size_t)b * nlm + lm] = v;
+    }
+  }
+}
+
 // invDl (boundary_mod.f90:244-292): W(1:N) = M_l phi(3:N-2) for all m of one
 // l, the reference's DGEMM with two columns (re, im) per mode.  CTA: one l and
 // up to 32 m; phi rows staged in shared memory, M_l streamed from L2.  The
@@ -255,6 +300,25 @@ int launch_prodvec(const sph_plan* p, const double* const* A, const double* cons
 int launch_dirichlet(const sph_plan* p, double2* a, cudaStream_t st) {
   TimedLaunch tl(p, T_OPS, st);
   dirichlet_kernel<<<ew_blocks(p->nlmv), EW_THREADS, 0, st>>>(a, p->nlmv, p->N);
+  SPH_LAUNCH_OK();
+  return SPH_OK;
+}
+
+int launch_bc_walls(const sph_plan* p, double2* tor, cudaStream_t st) {
+  if ((p->bck[0] || p->bck[1]) && (!p->d_neu || p->neu[0].empty())) return SPH_ENOTREADY;
+  TimedLaunch tl(p, T_OPS, st);
+  bc_walls_kernel<<<ew_blocks(p->nlmv), EW_THREADS, 0, st>>>(tor, p->d_neu, p->nlmv, p->N, p->d, p->bck[0],
+                                                             p->bck[1], 2.0 / p->z[0], -2.0 / p->z[p->N - 1]);
+  SPH_LAUNCH_OK();
+  return SPH_OK;
+}
+
+int launch_reconstruct(const sph_plan* p, double2* f, int boun, int ord, const double* a, cudaStream_t st) {
+  if ((boun != 0 && boun != 1) || (ord != 1 && ord != 2)) return SPH_EINVAL;
+  if (!p->d_neu || p->neu[ord - 1].empty() || p->N < p->d) return SPH_ENOTREADY;
+  TimedLaunch tl(p, T_OPS, st);
+  reconstruct_kernel<<<ew_blocks(p->nlmv), EW_THREADS, 0, st>>>(f, p->d_neu + (size_t)(ord - 1) * p->d, a, p->nlmv,
+                                                               p->N, p->d, boun, a != nullptr);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }

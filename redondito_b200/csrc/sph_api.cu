@@ -162,21 +162,58 @@ static int upload(T** dst, const T* src, size_t n) {
   return SPH_OK;
 }
 
+// the read-only device tables of a plan (shared with its clones)
+static std::vector<void*> table_ptrs(const sph_plan* p) {
+  return {p->P, p->dP, p->mPs, p->wfold, p->wfull, p->d_dir, p->d_z, p->kfac, p->filt, p->zinv2, p->d_ell,
+          p->d_mbase, p->twz, p->twphi, p->twzf, p->twphif, p->revz, p->revphi, p->twpz, p->twpphi, p->twpzf,
+          p->twpphif, p->tw4f, p->tw4d, p->tilesA, p->tilesA32, p->tilesS, p->tilesS32, p->d_bplanes, p->d_toff};
+}
+
+PlanTables::~PlanTables() {
+  for (void* q : dev)
+    if (q) cudaFree(q);
+  for (TcSet& t : tc) {
+    if (t.items) cudaFree(t.items);
+    if (t.blocks) cudaFree(t.blocks);
+  }
+  if (binv) cudaFree(binv);
+  if (d2bor) cudaFree(d2bor);
+}
+
+// Frees a plan's own buffers; its tables go with the last plan that shares
+// them (a plan whose creation failed owns its tables alone).
 static void plan_free(sph_plan* p) {
   for (auto e : p->ev_pool) cudaEventDestroy(e);
-  mixed_free(p);
-  void* ptrs[] = {p->P, p->dP, p->mPs, p->wfold, p->wfull, p->d_dir, p->d_z, p->kfac, p->filt,
-                  p->zinv2, p->d_ell, p->d_mbase, p->twz, p->twphi, p->twzf, p->twphif, p->revz,
-                  p->revphi, p->twpz, p->twpphi, p->twpzf, p->twpphif, p->tw4f, p->tw4d, p->tilesA,
-                  p->tilesA32, p->tilesS, p->tilesS32, p->G, p->binv, p->d2bor, p->energy, p->d_bplanes,
-                  p->spectrum};
-  for (void* q : ptrs)
+  mixed_free_scratch(p);
+  for (void* q : {(void*)p->G, (void*)p->energy, (void*)p->spectrum, (void*)p->d_neu})
     if (q) cudaFree(q);
+  if (p->bc_own) {  // boundary matrices of kinds other than the shared ones
+    if (p->binv) cudaFree(p->binv);
+    if (p->d2bor) cudaFree(p->d2bor);
+    p->binv = p->d2bor = nullptr;
+  }
   for (auto& q : p->sp)
     if (q) cudaFree(q);
   for (auto& q : p->gr)
     if (q) cudaFree(q);
+  if (!p->tables) {
+    mixed_free_tables(p);
+    for (void* q : table_ptrs(p))
+      if (q) cudaFree(q);
+    if (p->binv) cudaFree(p->binv);
+    if (p->d2bor) cudaFree(p->d2bor);
+  }
   delete p;
+}
+
+// hands the plan's tables to a shared owner (after a successful creation)
+static void own_tables(sph_plan* p) {
+  p->tables = std::make_shared<PlanTables>();
+  p->tables->dev = table_ptrs(p);
+  p->tables->tc[0] = p->tcAS;
+  p->tables->tc[1] = p->tcAV;
+  p->tables->tc[2] = p->tcSS;
+  p->tables->tc[3] = p->tcSV;
 }
 
 static std::vector<LegTile> row_tiles(int lmax, int block, bool by_l, int nlat2) {
@@ -392,6 +429,64 @@ extern "C" int sph_plan_create(sph_plan** out, int lmax, int nlat, int nphi, int
     plan_free(p);
     return rc;
   }
+  own_tables(p);
+  *out = p;
+  return SPH_OK;
+}
+
+extern "C" int sph_plan_clone(const sph_plan* src, sph_plan** out) {
+  if (!out) return SPH_EINVAL;
+  *out = nullptr;
+  if (!src || !src->tables) return SPH_EINVAL;
+  sph_plan* p = new sph_plan(*src);  // sizes, host grids, table pointers; one more owner of the tables
+  // its own buffers: nothing of the source's scratch, timers, slab or boundary state
+  p->G = nullptr;
+  for (auto& q : p->sp) q = nullptr;
+  for (auto& q : p->gr) q = nullptr;
+  p->nsp = p->ngr = 0;
+  p->energy = p->spectrum = nullptr;
+  p->dflag = nullptr;
+  p->Tana = p->Tsyn = nullptr;
+  p->contg = nullptr;
+  p->phi2 = nullptr;
+  p->phi2_planes = 0;
+  p->ev_pool.clear();
+  p->ev_class.clear();
+  p->ev_used = 0;
+  p->timing = 0;
+  p->k0 = 0;
+  p->nzv = p->nz;
+  p->lm0 = 0;
+  p->nlmv = p->nlm;
+  p->sel_kz = nullptr;
+  p->sel_n = 0;
+  p->bpass = 0;
+  p->bc_ready = 0;
+  p->bc_own = 0;
+  p->bck[0] = p->bck[1] = 0;
+  p->binv = p->d2bor = nullptr;
+  p->d_neu = nullptr;
+  int rc = SPH_OK;
+  if (!p->neu[0].empty() || !p->neu[1].empty()) {  // the Neumann reconstructors, copied
+    std::vector<double> both((size_t)2 * p->d, 0.0);
+    for (int o = 0; o < 2; ++o)
+      if (!p->neu[o].empty()) std::copy(p->neu[o].begin(), p->neu[o].end(), both.begin() + (size_t)o * p->d);
+    rc = upload(&p->d_neu, both.data(), both.size());
+  }
+  if (rc == SPH_OK && cudaMalloc((void**)&p->G, SPH_MAX_FIELDS * p->Gfield * sizeof(double2)) != cudaSuccess)
+    rc = SPH_ENOMEM;
+  if (rc == SPH_OK && cudaMemset(p->G, 0, SPH_MAX_FIELDS * p->Gfield * sizeof(double2)) != cudaSuccess)
+    rc = SPH_ECUDA;
+  if (rc == SPH_OK && cudaMalloc((void**)&p->energy, sizeof(double)) != cudaSuccess) rc = SPH_ENOMEM;
+  if (rc == SPH_OK && p->precision == SPH_MIXED) rc = mixed_alloc_scratch(p);
+  if (rc == SPH_OK && !p->dflag) {
+    if (cudaMalloc((void**)&p->dflag, sizeof(int)) != cudaSuccess) rc = SPH_ENOMEM;
+    else if (cudaMemset(p->dflag, 0, sizeof(int)) != cudaSuccess) rc = SPH_ECUDA;
+  }
+  if (rc != SPH_OK) {
+    plan_free(p);  // drops its reference to the tables only
+    return rc;
+  }
   *out = p;
   return SPH_OK;
 }
@@ -427,6 +522,56 @@ extern "C" int sph_fcgram_load_tables(const char* tdir, int C, int d, double* di
       dir[i + (size_t)C * j] = s;
     }
   return SPH_OK;
+}
+
+extern "C" int sph_fcgram_load_neumann_tables(const char* tdir, int d, int ord, double dx, double* neu) {
+  if (!tdir || !neu || d < 1 || (ord != 1 && ord != 2) || !(dx > 0.0)) return SPH_EINVAL;
+  std::vector<double> Q((size_t)d * d), Qn((size_t)d * d);
+  char path[4096];
+  snprintf(path, sizeof path, "%s/Q%d.dat", tdir, d);
+  FILE* f = fopen(path, "rb");
+  if (!f) return SPH_EIO;
+  size_t got = fread(Q.data(), sizeof(double), Q.size(), f);
+  fclose(f);
+  if (got != Q.size()) return SPH_EIO;
+  snprintf(path, sizeof path, "%s/Q%dn%d.dat", tdir, ord, d);
+  f = fopen(path, "rb");
+  if (!f) return SPH_EIO;
+  double dxp = 0.0;
+  got = fread(&dxp, sizeof(double), 1, f);
+  got += fread(Qn.data(), sizeof(double), Qn.size(), f);
+  fclose(f);
+  if (got != Qn.size() + 1 || !(dxp > 0.0)) return SPH_EIO;
+  // neu = MATMUL(Q(d,:), TRANSPOSE(Qn)); neu(d) *= (dx/dxp)^ord  (fcgram_mod.f90:357-363)
+  for (int k = 0; k < d; ++k) {
+    double acc = 0.0;
+    for (int j = 0; j < d; ++j) acc += Q[(d - 1) + (size_t)d * j] * Qn[k + (size_t)d * j];
+    neu[k] = acc;
+  }
+  neu[d - 1] *= ord == 1 ? dx / dxp : (dx / dxp) * (dx / dxp);
+  return SPH_OK;
+}
+
+extern "C" int sph_plan_set_neumann(sph_plan* p, const double* neu1, const double* neu2) {
+  if (!p || p->d < 1 || (!neu1 && !neu2)) return SPH_EINVAL;
+  if (neu1) p->neu[0].assign(neu1, neu1 + p->d);
+  if (neu2) p->neu[1].assign(neu2, neu2 + p->d);
+  std::vector<double> both((size_t)2 * p->d, 0.0);
+  for (int o = 0; o < 2; ++o)
+    if (!p->neu[o].empty()) std::copy(p->neu[o].begin(), p->neu[o].end(), both.begin() + (size_t)o * p->d);
+  if (!p->d_neu && cudaMalloc((void**)&p->d_neu, both.size() * sizeof(double)) != cudaSuccess) return SPH_ENOMEM;
+  SPH_CUDA_OK(cudaMemcpy(p->d_neu, both.data(), both.size() * sizeof(double), cudaMemcpyHostToDevice));
+  return SPH_OK;
+}
+
+extern "C" int sph_neumann_reconstruct(sph_plan* p, double* f, int boun, int ord, void* s) {
+  if (!p || !f) return SPH_EINVAL;
+  return launch_reconstruct(p, reinterpret_cast<double2*>(f), boun, ord, nullptr, (cudaStream_t)s);
+}
+
+extern "C" int sph_robin_reconstruct(sph_plan* p, double* f, int boun, const double* a, void* s) {
+  if (!p || !f || !a) return SPH_EINVAL;
+  return launch_reconstruct(p, reinterpret_cast<double2*>(f), boun, 1, a, (cudaStream_t)s);
 }
 
 extern "C" int sph_plan_sizes(const sph_plan* p, int* nlm, long long* ge, long long* se) {
@@ -486,8 +631,15 @@ extern "C" int sph_plan_set_tiles(sph_plan* p, int rows, int ring_pairs, int z_c
   p->tile_np = ring_pairs;
   p->tile_lb = z_cols;
   if (p->precision == SPH_MIXED && rows != p->tile_nr) {
+    // the scalar table tiles are rebuilt: not while clones share them
+    if (p->tables && p->tables.use_count() > 1) return SPH_EINVAL;
     p->tile_nr = rows;
-    return mixed_retile(p);
+    const int rc = mixed_retile(p);
+    if (p->tables) {
+      p->tables->tc[0] = p->tcAS;
+      p->tables->tc[2] = p->tcSS;
+    }
+    return rc;
   }
   return SPH_OK;
 }
@@ -876,18 +1028,39 @@ static int ensure_nl_scratch(sph_plan* p) {
 
 extern "C" int sph_setup_bc(sph_plan* p, const char* bcint, const char* bcext) {
   if (!p) return SPH_EINVAL;
-  // v_parsebc (vboundary.f90:10-31): only 'noslip'
-  auto is_noslip = [](const char* s) {
-    if (!s) return false;
+  // v_parsebc (vboundary.f90:10-31) knows 'noslip' (0); 'freeslip' (1) is
+  // added here: W = 0, W'' - 2 W'/r = 0, Z' - 2 Z/r = 0 at the wall
+  auto parse = [](const char* s) {
+    if (!s) return -1;
     std::string t(s);
     t.erase(0, t.find_first_not_of(" \t"));
     t.erase(t.find_last_not_of(" \t") + 1);
     for (auto& c : t) c = (char)tolower(c);
-    return t == "noslip";
+    return t == "noslip" ? 0 : t == "freeslip" ? 1 : -1;
   };
-  if (!is_noslip(bcint) || !is_noslip(bcext)) return SPH_EINVAL;
+  const int kin = parse(bcint), kout = parse(bcext);
+  if (kin < 0 || kout < 0) return SPH_EINVAL;
   const int n = p->N, lmax = p->lmax;
   if (p->C <= 0 || n < 6) return SPH_EINVAL;
+  if ((kin == 1 || kout == 1) && (p->neu[0].empty() || !p->d_neu)) return SPH_ENOTREADY;
+  const int kinds = kin + 2 * kout;
+  if (p->bc_ready && p->bck[0] == kin && p->bck[1] == kout) return SPH_OK;
+  if (p->bc_own) {
+    if (p->binv) cudaFree(p->binv);
+    if (p->d2bor) cudaFree(p->d2bor);
+    p->bc_own = 0;
+  }
+  p->binv = p->d2bor = nullptr;
+  p->bc_ready = 0;
+  p->bck[0] = kin;
+  p->bck[1] = kout;
+  if (p->tables && p->tables->binv && p->tables->bc_kinds == kinds) {  // built for a plan sharing the tables
+    p->binv = p->tables->binv;
+    p->d2bor = p->tables->d2bor;
+    RC(ensure_nl_scratch(p));
+    p->bc_ready = 1;
+    return SPH_OK;
+  }
   std::vector<double> d1, d2;
   host_derivr_matrix(p, 1, d1);
   host_derivr_matrix(p, 2, d2);
@@ -898,12 +1071,17 @@ extern "C" int sph_setup_bc(sph_plan* p, const char* bcint, const char* bcext) {
     std::fill(b.begin(), b.end(), 0.0);
     auto B = [&](int i, int j) -> double& { return b[(i - 1) + (size_t)n * (j - 1)]; };
     B(1, 1) = 1.0;
-    for (int j = 1; j <= n; ++j) B(2, j) = d1[0 + (size_t)n * (j - 1)];
+    // W' = 0 (noslip) or W'' - 2 W'/r = 0 (freeslip) at the inner wall
+    for (int j = 1; j <= n; ++j)
+      B(2, j) = kin ? d2[0 + (size_t)n * (j - 1)] - 2.0 / p->z[0] * d1[0 + (size_t)n * (j - 1)]
+                    : d1[0 + (size_t)n * (j - 1)];
     for (int i = 3; i <= n - 2; ++i) {
       for (int j = 1; j <= n; ++j) B(i, j) = d2[(i - 1) + (size_t)n * (j - 1)];
       B(i, i) = B(i, i) - (double)(l * (l + 1)) / (p->z[i - 1] * p->z[i - 1]);
     }
-    for (int j = 1; j <= n; ++j) B(n - 1, j) = d1[(n - 1) + (size_t)n * (j - 1)];
+    for (int j = 1; j <= n; ++j)
+      B(n - 1, j) = kout ? d2[(n - 1) + (size_t)n * (j - 1)] - 2.0 / p->z[n - 1] * d1[(n - 1) + (size_t)n * (j - 1)]
+                         : d1[(n - 1) + (size_t)n * (j - 1)];
     B(n, n) = 1.0;
     for (int i = 1; i <= n; ++i) {
       double mx = 0.0;
@@ -925,11 +1103,23 @@ extern "C" int sph_setup_bc(sph_plan* p, const char* bcint, const char* bcext) {
     d2bor[2 + 4 * (size_t)j] = d2[(n - 2) + (size_t)n * j];
     d2bor[3 + 4 * (size_t)j] = d2[(n - 1) + (size_t)n * j];
   }
-  if (p->binv) cudaFree(p->binv);
-  if (p->d2bor) cudaFree(p->d2bor);
-  p->binv = p->d2bor = nullptr;
-  RC(upload(&p->binv, binv.data(), binv.size()));
-  RC(upload(&p->d2bor, d2bor.data(), d2bor.size()));
+  double *db = nullptr, *dd = nullptr;
+  int rc = upload(&db, binv.data(), binv.size());
+  if (rc == SPH_OK) rc = upload(&dd, d2bor.data(), d2bor.size());
+  if (rc != SPH_OK) {
+    if (db) cudaFree(db);
+    if (dd) cudaFree(dd);
+    return rc;
+  }
+  p->binv = db;
+  p->d2bor = dd;
+  if (p->tables && !p->tables->binv) {  // the tables own them from now on
+    p->tables->binv = db;
+    p->tables->d2bor = dd;
+    p->tables->bc_kinds = kinds;
+  } else {
+    p->bc_own = 1;  // other kinds than the shared matrices: this plan's own
+  }
   RC(ensure_nl_scratch(p));
   p->bc_ready = 1;
   return SPH_OK;
@@ -949,7 +1139,7 @@ extern "C" int sph_invDl(sph_plan* p, const double* phi, double* w, void* s) {
 extern "C" int sph_v_imposebc(sph_plan* p, double* tor, double* phi, double* pol, void* s) {
   if (!p || !tor || !phi || !pol) return SPH_EINVAL;
   if (!p->bc_ready) return SPH_ENOTREADY;
-  RC(launch_dirichlet(p, D2(tor), ST(s)));
+  RC(launch_bc_walls(p, D2(tor), ST(s)));
   RC(launch_invDl(p, CD2(phi), D2(pol), ST(s)));
   return launch_zfft(p, Z_DLR, CD2(pol), D2(phi), 2, ST(s));
 }
@@ -957,7 +1147,7 @@ extern "C" int sph_v_imposebc(sph_plan* p, double* tor, double* phi, double* pol
 extern "C" int sph_v_imposebc_fast(sph_plan* p, double* tor, double* phi, double* pol, void* s) {
   if (!p || !tor || !phi || !pol) return SPH_EINVAL;
   if (!p->bc_ready) return SPH_ENOTREADY;
-  RC(launch_dirichlet(p, D2(tor), ST(s)));
+  RC(launch_bc_walls(p, D2(tor), ST(s)));
   RC(launch_invDl(p, CD2(phi), D2(pol), ST(s)));
   return launch_bc_fast_rows(p, D2(phi), CD2(pol), ST(s));
 }

@@ -7,6 +7,7 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -55,6 +56,17 @@ struct TcSet {
   int nitems = 0;
   uint16_t* blocks = nullptr;  // device, bf16 bit patterns
   size_t nhalves = 0;
+};
+
+// Device tables a plan shares with its clones (sph_plan_clone): everything a
+// plan reads but never writes after creation.  Freed with the last plan.
+struct PlanTables {
+  std::vector<void*> dev;      // plain table allocations
+  TcSet tc[4];                 // mixed table tiles (tcAS, tcAV, tcSS, tcSV)
+  double* binv = nullptr;      // boundary tables (sph_setup_bc), shared once built
+  double* d2bor = nullptr;
+  int bc_kinds = -1;           // the wall kinds binv was built for (inner + 2 outer)
+  ~PlanTables();
 };
 
 struct sph_plan {
@@ -111,12 +123,21 @@ struct sph_plan {
   // grid scratch for the NL step (nz*nphi*nlat doubles each)
   double* gr[9] = {nullptr};
   int ngr = 0;
-  // boundary
+  // boundary: kinds at the inner and outer wall (0 noslip, 1 freeslip); the
+  // plan owns binv/d2bor when its kinds differ from the shared tables'
+  int bck[2] = {0, 0};
+  int bc_own = 0;
+  // Neumann reconstructors (sph_plan_set_neumann): host neu[0] first and
+  // neu[1] second normal derivative, d values each (empty: not set); device
+  // copy [2][d]
+  std::vector<double> neu[2];
+  double* d_neu = nullptr;
   int bc_ready = 0;
   double* binv = nullptr;   // [lmax][N-4][N]  M_l column-major per l
   double* d2bor = nullptr;  // [N][4]
   double* energy = nullptr; // device accumulator (1 double)
   double* spectrum = nullptr;  // device [lmax+1][2] per-degree energies (sph_energy_spectrum)
+  std::shared_ptr<PlanTables> tables;  // owner of the read-only tables (shared by clones)
   // mixed precision: bf16 table tiles for the tcgen05 GEMMs, bf16 data tiles
   // (analysis: written by the phi FFT; synthesis: from the spectra), fp32
   // folded coefficients G32 of the synthesis (reusing the G allocation)
@@ -222,6 +243,12 @@ int launch_saxpby(const sph_plan* p, double* z, const double* x, double a, const
 int launch_prodvec(const sph_plan* p, const double* const* A, const double* const* B,
                    double* const* Cout, cudaStream_t st);
 int launch_dirichlet(const sph_plan* p, double2* a, cudaStream_t st);
+// the toroidal condition of each wall by its kind: Z = 0 (noslip) or the
+// Robin reconstruction of Z' - 2Z/r = 0 (freeslip)
+int launch_bc_walls(const sph_plan* p, double2* tor, cudaStream_t st);
+// neumann_reconstruct / robin_reconstruct on a radial boundary (boun 0 inner,
+// 1 outer) of the caller's lm columns; a: device Robin coefficients or null
+int launch_reconstruct(const sph_plan* p, double2* f, int boun, int ord, const double* a, cudaStream_t st);
 int launch_invDl(const sph_plan* p, const double2* phi, double2* w, cudaStream_t st);
 int launch_bc_fast_rows(const sph_plan* p, double2* phi, const double2* w, cudaStream_t st);
 int launch_qst_scale(const sph_plan* p, const double2* in, double2* out, int rpow, int lfac,
@@ -232,7 +259,9 @@ int launch_energy(const sph_plan* p, const double* ur, const double* ut, const d
 // mixed precision (k_mixed.cu)
 int mixed_setup(sph_plan* p, const std::vector<double>& hP, const std::vector<double>& hdP,
                 const std::vector<double>& hmPs);
-void mixed_free(sph_plan* p);
+int mixed_alloc_scratch(sph_plan* p);  // the per-plan buffers of a mixed plan (also for clones)
+void mixed_free_scratch(sph_plan* p);
+void mixed_free_tables(sph_plan* p);
 // grids_hi: planes k >= N of field f come from grids_hi[f] + (k - N) planes
 int launch_phi_fwd32(const sph_plan* p, const double* const* grids, int nfields, cudaStream_t st,
                      const double* const* grids_hi = nullptr);

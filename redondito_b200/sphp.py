@@ -48,7 +48,9 @@ SYMBOLS = (
     "sph_derivr_noalloc", "sph_plan_status", "sph_fftp3d_vec_to_qst", "sph_fftp3d_qst_to_vec",
     "sph_batch_create", "sph_batch_run", "sph_batch_status", "sph_batch_destroy",
     "sph_plan_set_tiles", "sph_plan_set_slab", "sph_range",
-    "sph_read_namelist", "sph_write_grids", "sph_energy_spectrum", "sph_run",
+    "sph_read_namelist", "sph_write_grids", "sph_energy_spectrum", "sph_run", "sph_plan_clone",
+    "sph_fcgram_load_neumann_tables", "sph_plan_set_neumann", "sph_neumann_reconstruct",
+    "sph_robin_reconstruct",
 )
 TIMER_CLASSES = ("phi_fwd", "phi_inv", "leg_analysis", "leg_synthesis", "vec_analysis",
                  "vec_synthesis", "zfft", "ops")
@@ -124,6 +126,11 @@ def lib(build_if_missing=True):
             "sph_write_grids": [P, ctypes.c_char_p],
             "sph_energy_spectrum": [P, Vp, Vp, pD, Vp],
             "sph_run": [P, Vp, Vp, Vp, D, D, I, I, I, I, ctypes.c_char_p, pD, Vp],
+            "sph_plan_clone": [P, ctypes.POINTER(P)],
+            "sph_fcgram_load_neumann_tables": [ctypes.c_char_p, I, I, D, pD],
+            "sph_plan_set_neumann": [P, pD, pD],
+            "sph_neumann_reconstruct": [P, Vp, I, I, Vp],
+            "sph_robin_reconstruct": [P, Vp, I, Vp, Vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -151,6 +158,14 @@ def load_dirichlet_tables(C=25, d=5, tdir=TABLES_DIR):
     """load_dirichlet_tables (src/sphp/fcgram_mod.f90:186-263): dir = A.Q^T."""
     out = (ctypes.c_double * (C * d))()
     _call("sph_fcgram_load_tables", tdir.encode(), C, d, out)
+    return list(out)
+
+
+def load_neumann_tables(d=5, ord=1, dx=1.0, tdir=TABLES_DIR):
+    """load_neumann_tables (src/sphp/fcgram_mod.f90:267-365): the boundary
+    reconstructor from the ord-th normal derivative, scaled for grid step dx."""
+    out = (ctypes.c_double * d)()
+    _call("sph_fcgram_load_neumann_tables", tdir.encode(), int(d), int(ord), float(dx), out)
     return list(out)
 
 
@@ -185,8 +200,27 @@ class Plan:
         self.nlm = (lmax + 1) * (lmax + 2) // 2
         self.N = nz - Cz
         self.k0, self.nzv, self.lm0, self.nlmv = 0, nz, 0, self.nlm
+        self.dz = (rext - rint) / (nz - Cz - 1) if nz - Cz > 1 else 1.0
+        if Cz > 0 and os.path.exists(os.path.join(tdir, f"Q1n{oz}.dat")):
+            # the Neumann reconstructors (fcgram_mod.f90:267-365), for the freeslip walls
+            n1 = (ctypes.c_double * oz)(*load_neumann_tables(oz, 1, self.dz, tdir))
+            n2 = (ctypes.c_double * oz)(*load_neumann_tables(oz, 2, self.dz, tdir))
+            _call("sph_plan_set_neumann", self.h, n1, n2)
         self._grid_arrays()
         self._bc = False
+
+    def clone(self):
+        """A plan of the same sizes sharing this plan's device tables, with
+        scratch of its own (sph_plan_clone)."""
+        c = object.__new__(Plan)
+        c.__dict__.update({k: v for k, v in self.__dict__.items() if k not in ("h", "_bc")})
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            _call("sph_plan_clone", self.h, ctypes.byref(h))
+        c.h = h
+        c._bc = False
+        c.k0, c.nzv, c.lm0, c.nlmv = 0, self.nz, 0, self.nlm
+        return c
 
     def _grid_arrays(self):
         def dbl(n):
@@ -378,6 +412,20 @@ def prodvec(plan, ar, at, ap, br, bt, bp, cr, ct, cp, stream=None):
 def setup_bc(plan, bckind=("noslip", "noslip")):
     _call("sph_setup_bc", plan.h, bckind[0].encode(), bckind[1].encode())
     plan._bc = True
+
+
+def neumann_reconstruct(plan, f, boun, ord=1, stream=None):
+    """The wall row of f (boun 0 inner, 1 outer) from the ord-th outward
+    normal derivative it holds (fcgram_mod.f90:368-520)."""
+    _call("sph_neumann_reconstruct", plan.h, _s(plan, f), int(boun), int(ord), _stream(stream))
+
+
+def robin_reconstruct(plan, f, boun, a, stream=None):
+    """f' + a f = g at the wall (g in the wall row); a: float64 CUDA tensor of
+    nlm coefficients (fcgram_mod.f90:523-650)."""
+    if a.dtype != torch.float64 or a.device.type != "cuda" or a.numel() != plan.nlmv or not a.is_contiguous():
+        raise ValueError("a must be a contiguous float64 CUDA tensor of nlm values")
+    _call("sph_robin_reconstruct", plan.h, _s(plan, f), int(boun), ctypes.c_void_p(a.data_ptr()), _stream(stream))
 
 
 def dirichlet(plan, a, stream=None):

@@ -19,6 +19,18 @@ method (Bruno & Lyon, J. Comput. Phys. 229 (2010); Lyon, SIAM J. Sci. Comput.
   60-digit arithmetic.  A[c, j] = g_j(d + c), c = 0..C-1, the C points that
   follow the matching interval.
 
+* Q1n (d x d) and Q2n (d x d), the Neumann tables of `load_neumann_tables`
+  (fcgram_mod.f90:267-365), which forms the boundary reconstructor
+  ``neu = Q(d,:) . Qn^T``: the value at the boundary point (x = d-1, the
+  last matching point) from the other d-1 values and the first (Q1n) or
+  second (Q2n) derivative there.  With M the d x d matrix whose rows
+  0..d-2 are the Gram basis at x = 0..d-2 and whose last row is the basis'
+  derivative of that order at x = d-1, the Gram coefficients of the
+  interpolant are M^-1 [f_0..f_{d-2}, g], so Qn = (M^-1)^T.  The
+  reconstructor reproduces polynomials of degree < d exactly.  The file
+  starts with the table's grid spacing dxp (1: grid units), as the
+  reference reads it.
+
 The tables are written like the reference reads them: raw stream,
 Fortran column-major float64 (`READ(10) A` on A(C,d), fcgram_mod.f90:234-248).
 
@@ -92,6 +104,24 @@ def continuation_table(d, C, K=16, over=10, cut=mp.mpf("1e-40")):
     return A, Qd
 
 
+def neumann_table(d, order):
+    """Qn = (M^-1)^T for the reconstruction from a derivative of `order`."""
+    Q, R = gram_basis(d)
+    coef = mp.inverse(R)  # p_j(x) = sum_k coef[k, j] x^k
+    x = mp.mpf(d - 1)
+    M = mp.matrix(d, d)
+    for i in range(d - 1):
+        for j in range(d):
+            M[i, j] = Q[i, j]
+    for j in range(d):
+        if order == 1:
+            M[d - 1, j] = mp.fsum(coef[k, j] * k * x ** (k - 1) for k in range(1, d))
+        else:
+            M[d - 1, j] = mp.fsum(coef[k, j] * k * (k - 1) * x ** (k - 2) for k in range(2, d))
+    Mi = mp.inverse(M)
+    return np.array([[float(Mi[j, i]) for j in range(d)] for i in range(d)])
+
+
 def write_tables(outdir, C=25, d=5):
     mp.mp.dps = 60
     A, Q = continuation_table(d, C)
@@ -99,6 +129,11 @@ def write_tables(outdir, C=25, d=5):
     # Fortran column-major raw stream
     A.T.astype("<f8").tofile(os.path.join(outdir, f"A{C}-{d}.dat"))
     Q.T.astype("<f8").tofile(os.path.join(outdir, f"Q{d}.dat"))
+    for order in (1, 2):
+        Qn = neumann_table(d, order)
+        with open(os.path.join(outdir, f"Q{order}n{d}.dat"), "wb") as f:
+            np.array([1.0], "<f8").tofile(f)  # dxp: the tables are in grid units
+            Qn.T.astype("<f8").tofile(f)
     return A, Q
 
 
@@ -109,4 +144,4 @@ if __name__ == "__main__":
     ap.add_argument("--out", default=os.path.dirname(os.path.abspath(__file__)))
     a = ap.parse_args()
     A, Q = write_tables(a.out, a.C, a.d)
-    print(f"wrote A{a.C}-{a.d}.dat ({A.shape}) and Q{a.d}.dat ({Q.shape}) to {a.out}")
+    print(f"wrote A{a.C}-{a.d}.dat ({A.shape}), Q{a.d}.dat ({Q.shape}), Q1n{a.d}.dat and Q2n{a.d}.dat to {a.out}")

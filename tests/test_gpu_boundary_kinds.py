@@ -1,0 +1,101 @@
+"""Neumann and Robin reconstructions (fcgram_mod.f90:267-650) and the
+freeslip wall kind on the GPU against the oracle, on the same inputs."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests._helpers import check, random_spec, rel_l2
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def dev(x):
+    return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+def _pair(lmax=7, nz=128, nlat=None, nphi=None):
+    from redondito_b200 import sphp as S
+    P = O.Plan(lmax, nz, nlat=nlat, nphi=nphi, C=25, d=5, rint=0.5, rext=1.5)
+    G = S.Plan(lmax, nz, nlat=P.nlat, nphi=P.nphi, Cz=25, oz=5, rint=0.5, rext=1.5)
+    return S, P, G
+
+
+@pytest.mark.parametrize("ord", [1, 2])
+def test_neumann_reconstruct(ord):
+    S, P, G = _pair()
+    rng = np.random.default_rng(ord)
+    f = random_spec(P, rng)
+    for boun in (0, 1):
+        ref = P.neumann_reconstruct(f, boun, ord)
+        x = dev(f)
+        S.neumann_reconstruct(G, x, boun, ord)
+        check(rel_l2(x.cpu().numpy(), ref), 1e-15, f"neumann boun={boun} ord={ord}")
+    G.close()
+
+
+def test_robin_reconstruct():
+    S, P, G = _pair()
+    rng = np.random.default_rng(9)
+    f = random_spec(P, rng)
+    a = rng.normal(size=P.nlm)
+    for boun in (0, 1):
+        ref = P.robin_reconstruct(f, boun, a)
+        x = dev(f)
+        S.robin_reconstruct(G, x, boun, dev(a))
+        check(rel_l2(x.cpu().numpy(), ref), 1e-15, f"robin boun={boun}")
+    G.close()
+
+
+@pytest.mark.parametrize("kinds", [("freeslip", "freeslip"), ("freeslip", "noslip"), ("noslip", "freeslip")])
+def test_freeslip_imposebc(kinds):
+    S, P, G = _pair()
+    P.bc_setup(kinds)
+    S.setup_bc(G, kinds)
+    rng = np.random.default_rng(12)
+    tor, phi = random_spec(P, rng), random_spec(P, rng)
+    for fast in (False, True):
+        t_ref, f_ref, w_ref = P.imposebc(tor, phi, fast=fast)
+        T, F, W = dev(tor), dev(phi), G.new_spec()
+        (S.v_imposebc_fast if fast else S.v_imposebc)(G, T, F, W)
+        check(rel_l2(T.cpu().numpy(), t_ref), 1e-15, f"{kinds} tor fast={fast}")
+        check(rel_l2(W.cpu().numpy(), w_ref), TOL, f"{kinds} pol fast={fast}")
+        check(rel_l2(F.cpu().numpy(), f_ref), TOL, f"{kinds} phi fast={fast}")
+    G.close()
+
+
+def test_freeslip_needs_the_reconstructor():
+    from redondito_b200 import sphp as S
+    # a plan built with a continuation operator given directly has no Neumann tables
+    dir_ = S.load_dirichlet_tables(25, 5)
+    G = S.Plan(7, 64, Cz=25, oz=5, rint=0.5, rext=1.5, dir=dir_, tdir="/nonexistent")
+    with pytest.raises(S.SphError) as e:
+        S.setup_bc(G, ("freeslip", "noslip"))
+    assert e.value.code == 4  # SPH_ENOTREADY
+    S.setup_bc(G, ("noslip", "noslip"))
+    G.close()
+
+
+def test_freeslip_nl_step():
+    S, P, G = _pair(lmax=15, nz=64, nlat=24, nphi=48)
+    kinds = ("freeslip", "freeslip")
+    P.bc_setup(kinds)
+    S.setup_bc(G, kinds)
+    rng = np.random.default_rng(3)
+    Z = random_spec(P, rng, power=3.0)
+    W = random_spec(P, rng, power=3.0)
+    Z, phi, W = P.imposebc(Z, P.dlr(W))
+    rz_ref, rf_ref, e_ref = P.nl_rhs(Z, W, phi, 1e-3)
+    rz, rf = G.new_spec(), G.new_spec()
+    e = S.nl_rhs(G, dev(Z), dev(W), dev(phi), 1e-3, rz, rf)
+    check(abs(e - e_ref) / e_ref, TOL, "energy")
+    check(rel_l2(rz.cpu().numpy(), rz_ref), TOL, "rhs_z")
+    check(rel_l2(rf.cpu().numpy(), rf_ref), TOL, "rhs_phi")
+    Zr, Wr, Fr, e_ref = P.rk3_step(Z, W, phi, 1e-3, 1e-4)
+    Zg, Wg, Fg = dev(Z), dev(W), dev(phi)
+    S.rk3_step(G, Zg, Wg, Fg, 1e-3, 1e-4)
+    for name, a, b in (("Z", Zg, Zr), ("W", Wg, Wr), ("phi", Fg, Fr)):
+        check(rel_l2(a.cpu().numpy(), b), TOL, f"RK3 {name}")
+    G.close()

@@ -32,3 +32,14 @@ def test_latency_stats():
     st = serve.latency_stats(rs)
     assert abs(st["p50_ms"] - 50.5) < 0.6 and st["p99_ms"] > 98
     assert st["jobs"] == 100
+
+
+def test_slot_estimates_grow_with_size_and_kind():
+    sizes = (31, 63, 127, 255, 511)
+    for mixed in (False, True):
+        pairs = [serve.estimate_bytes(l, "pair", mixed) for l in sizes]
+        rk3 = [serve.estimate_bytes(l, "rk3", mixed) for l in sizes]
+        assert all(a < b for a, b in zip(pairs, pairs[1:]))
+        assert all(p < r for p, r in zip(pairs, rk3))
+    # an RK3 slot at lmax 511 holds the NL step's 9 grids and 15 spectra: tens of GB
+    assert 25e9 < serve.estimate_bytes(511, "rk3", False) < 60e9
