@@ -138,3 +138,37 @@ def test_slab_operators_and_boundary():
         assert torch.equal(ys, y[:, sl])
     S.set_slab(G, 0, nz, 0, G.nlm)
     G.close()
+
+
+def test_split_3d_pair_one_rank_over_nccl():
+    """The split 3D transforms of redondito_b200/slab.py through an NCCL
+    process group of one rank (the exchange moves every block to itself)
+    equal the unsplit 3D transforms bit for bit.  Several ranks are covered
+    on the CPU (tests/test_slab_gloo.py)."""
+    import socket
+
+    import torch.distributed as dist
+    from redondito_b200 import slab, sphp as S
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            device_id=torch.device("cuda", torch.cuda.current_device()))
+    try:
+        P = O.Plan(31, 64, nlat=48, nphi=96, C=25, d=5)
+        G = S.Plan(31, 64, nlat=48, nphi=96, Cz=25, oz=5)
+        grid = dev(P.sh_synthesis(random_spec(P, np.random.default_rng(8))))
+        ref = G.new_spec()
+        S.fftp3d_real_to_complex(G, grid, ref)
+        spec = G.new_spec()
+        slab.fftp3d_real_to_complex(G, grid, spec)
+        assert torch.equal(spec, ref)
+        g1, g2 = G.new_grid(), G.new_grid()
+        S.set_slab(G, 0, G.nz, 0, G.nlm)
+        S.fftp3d_complex_to_real(G, ref.clone(), g1)
+        slab.fftp3d_complex_to_real(G, spec, g2)
+        assert torch.equal(g1, g2)
+        S.set_slab(G, 0, G.nz, 0, G.nlm)
+        G.close()
+    finally:
+        dist.destroy_process_group()
