@@ -102,3 +102,27 @@ def test_energy_spectrum_against_oracle():
     e = S.nl_rhs(G, dev(Z), dev(W), dev(phi), NU, G.new_spec(), G.new_spec())
     check(abs(sp.sum() - e) / e, TOL, "Parseval")
     G.close()
+
+
+def test_solver_command_line(tmp_path):
+    """python -m redondito_b200.solver: namelist in, grid files, balance and
+    spectra out, the final energy printed."""
+    import json
+    import subprocess
+    import sys
+    nml = tmp_path / "run.nml"
+    nml.write_text("&grid lmax=15, nz=64, Cz=25, oz=5 /\n&boxparams rint=0.5d0, rext=1.5d0 /\n"
+                   "&run dt=1d-4, step=4, tstep=2, sstep=2, nu=1d-3 /\n")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-m", "redondito_b200.solver", str(nml), str(tmp_path / "out"),
+                          "--bc", "freeslip,noslip"], capture_output=True, text=True, timeout=600, cwd=root)
+    assert out.returncode == 0, out.stderr[-2000:]
+    d = json.loads(out.stdout.strip().splitlines()[-1])
+    assert d["steps"] == 4 and d["energy"] > 0
+    bal = np.loadtxt(tmp_path / "out" / "balance.txt")
+    assert bal.shape == (3, 3) and np.array_equal(bal[:, 0], [0, 2, 4])
+    assert abs(bal[-1, 2] - d["energy"]) <= 1e-15 * d["energy"] + 1e-300
+    for i in range(3):
+        assert (tmp_path / "out" / f"lspectrum.{i:04d}.txt").exists()
+    for f in ("theta.txt", "phi.txt", "z.txt"):
+        assert (tmp_path / "out" / f).exists()
