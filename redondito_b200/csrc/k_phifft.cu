@@ -20,6 +20,7 @@
 #include "fft_ct.cuh"
 #include "tc05.cuh"
 #include "tma.cuh"
+#include "cluster.cuh"
 
 namespace {
 
@@ -442,38 +443,6 @@ int phi3d_dispatch_n(const sph_plan* p, const PhiArgs& a, int nfields, cudaStrea
 // step-(A) reads of a half warp (4 ring pairs x 4 rows) spread over the
 // banks; the transform area has an odd row pitch and a ring-pair stride of
 // 2 (mod 8) 16-byte slots.
-__device__ __forceinline__ uint32_t cluster_rank() {
-  uint32_t r;
-  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ void cluster_sync_all() {
-  asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;\n" ::: "memory");
-}
-// shared::cluster address of `p` (a shared-memory location of this CTA) in CTA `rank`
-__device__ __forceinline__ uint32_t cluster_map(const void* p, uint32_t rank) {
-  uint32_t r;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(tc05::smem_u32(p)), "r"(rank));
-  return r;
-}
-__device__ __forceinline__ double ld_cluster_f64(uint32_t addr) {
-  double v;
-  asm volatile("ld.shared::cluster.f64 %0, [%1];\n" : "=d"(v) : "r"(addr) : "memory");
-  return v;
-}
-__device__ __forceinline__ int ld_cluster_s32(uint32_t addr) {
-  int v;
-  asm volatile("ld.shared::cluster.s32 %0, [%1];\n" : "=r"(v) : "r"(addr) : "memory");
-  return v;
-}
-
-constexpr int largest_divisor_le(int n, int cap) {
-  int d = cap < n ? cap : n;
-  while (d > 1 && n % d) --d;
-  return d;
-}
-constexpr size_t round_up(size_t x, size_t q) { return (x + q - 1) / q * q; }
-
 template <int N, int CL>
 struct P3c {
   static constexpr int NPL = 4, NPC = NPL * CL;  // ring pairs per CTA, per cluster tile
@@ -704,11 +673,12 @@ int phi3c_run(const sph_plan* p, const PhiArgs& a, int nfields, cudaStream_t st)
 }
 
 // cluster size: 4 (128-byte runs) where nlat/2 splits into tiles of 16 ring
-// pairs, else 2; ring_pairs tuned to 8 selects 2
+// pairs, else 2; a plan with ring pairs set by sph_plan_set_tiles keeps the
+// single-CTA kernels those settings were tuned on
 template <int N>
 int phi3c_dispatch_n(const sph_plan* p, const PhiArgs& a, int nfields, cudaStream_t st) {
-  if (p->tile_np && p->tile_np != 8) return PHI3C_UNSUPPORTED;
-  if (!p->tile_np && p->nlat2 % 16 == 0) {
+  if (p->tile_np) return PHI3C_UNSUPPORTED;  // tuned ring pairs: the kernels they were tuned on
+  if (p->nlat2 % 16 == 0) {
     const int rc = phi3c_run<N, 4>(p, a, nfields, st);
     if (rc != PHI3C_UNSUPPORTED) return rc;
   }
