@@ -122,3 +122,27 @@ def test_tile_shapes_do_not_change_results(precision):
         S.set_tiles(G, 48, 0, 0)
     with pytest.raises(S.SphError):
         S.set_tiles(G, 0, 3, 0)
+
+
+def test_batch_refuses_a_plan_twice():
+    """A plan's per-field scratch serves one problem: the same plan for two
+    problems of a batch would race on it, so sph_batch_create refuses it."""
+    import ctypes
+    from redondito_b200 import sphp as S
+    G = S.Plan(15, 32, nlat=24, nphi=48, Cz=25, oz=5)
+    bufs = [G.new_spec(), G.new_grid(), G.new_spec(), G.new_spec(), G.new_grid(), G.new_spec()]
+    ph = (ctypes.c_void_p * 2)(G.h.value, G.h.value)
+    nf = (ctypes.c_int * 2)(1, 1)
+    arr = lambda a, b: (ctypes.c_void_p * 2)(a.data_ptr(), b.data_ptr())
+    h = ctypes.c_void_p()
+    rc = S.lib().sph_batch_create(ctypes.byref(h), 2, ph, nf, arr(bufs[0], bufs[3]), arr(bufs[1], bufs[4]),
+                                  arr(bufs[2], bufs[5]))
+    assert rc == 1 and not h.value  # SPH_EINVAL
+    G2 = G.clone()
+    ph2 = (ctypes.c_void_p * 2)(G.h.value, G2.h.value)
+    rc = S.lib().sph_batch_create(ctypes.byref(h), 2, ph2, nf, arr(bufs[0], bufs[3]), arr(bufs[1], bufs[4]),
+                                  arr(bufs[2], bufs[5]))
+    assert rc == 0  # two plans (a clone has scratch of its own)
+    S.lib().sph_batch_destroy(h)
+    G2.close()
+    G.close()
