@@ -8,8 +8,10 @@ def test_candidates_respect_the_entry_point_limits():
         for prec in (0, 1):
             cs = A.candidates(lmax, nz, nlat, 2 * nlat, prec)
             assert cs
+            assert any(c["ring_pairs"] == 0 for c in cs)  # the built-in choice is a candidate
             for c in cs:
-                assert (nlat // 2) % c["ring_pairs"] == 0 and c["ring_pairs"] * 2 * nlat <= 8192
+                rp = c["ring_pairs"]
+                assert rp == 0 or ((nlat // 2) % rp == 0 and rp * 2 * nlat <= 8192)
                 assert c["z_cols"] * nz <= 4096
                 assert (c["rows"] == 0) == (prec == 0)
 
