@@ -69,6 +69,7 @@ def lib():
         L.orc_neumann_reconstruct.argtypes = [P, D, I, I]
         L.orc_robin_reconstruct.argtypes = [P, D, I, D]
         L.orc_bc_setup_kinds.argtypes = [P, I, I]
+        L.orc_bc_set_tables.argtypes = [P, I, I, D, D]
         for name in ("orc_plan_destroy", "orc_set_threads", "orc_grid", "orc_sh_analysis",
                      "orc_sh_synthesis", "orc_qst_analysis", "orc_qst_synthesis", "orc_z_forward",
                      "orc_z_inverse", "orc_3d_forward", "orc_3d_inverse", "orc_laplang",
@@ -297,15 +298,27 @@ class Plan:
         lib().orc_dirichlet(self.h, _p(s.view(np.float64)))
         return s
 
-    def bc_setup(self, kinds=None):
+    def bc_setup(self, kinds=None, tables=None):
         """Boundary kinds at the inner and outer wall: noslip or freeslip
-        (None: keep the kinds set up, noslip if none)."""
+        (None: keep the kinds set up, noslip if none).  tables = (binv,
+        d2bor) in bc_tables()'s layouts replaces the matrices invDl_setup
+        builds (e.g. extended.bc_tables(), evaluated in long double)."""
         code = {"noslip": 0, "freeslip": 1}
         if kinds is None:
             if self._bc:
                 return
             kinds = ("noslip", "noslip")
         k = (code[kinds[0]], code[kinds[1]])
+        if tables is not None:
+            binv = np.ascontiguousarray(tables[0], dtype=np.float64).ravel()
+            d2bor = np.ascontiguousarray(tables[1], dtype=np.float64).ravel()
+            assert binv.size == self.N * (self.N - 4) * max(self.lmax, 1) and d2bor.size == 4 * self.N
+            rc = lib().orc_bc_set_tables(self.h, *k, _p(binv), _p(d2bor))
+            if rc:
+                raise ValueError(f"bc_set_tables failed ({rc})")
+            self._bc = True
+            self._bck = k
+            return
         if not self._bc or getattr(self, "_bck", (0, 0)) != k:
             rc = lib().orc_bc_setup_kinds(self.h, *k)
             if rc:

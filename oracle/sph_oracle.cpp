@@ -863,6 +863,23 @@ extern "C" int orc_bc_setup(orc_plan* p) {
   return 0;
 }
 
+// The boundary tables given directly (binv: N x (N-4) per l = 1..lmax;
+// d2bor: 4 x N), for the wall kinds kint / kext: the operators of
+// v_imposebc then run on tables built elsewhere (an extended-precision
+// evaluation of invDl_setup's matrices).  0 on success.
+extern "C" int orc_bc_set_tables(orc_plan* p, int kint, int kext, const double* binv, const double* d2bor) {
+  if (kint < 0 || kint > 1 || kext < 0 || kext > 1 || !binv || !d2bor) return 3;
+  if ((kint == 1 || kext == 1) && p->neu[0].empty()) return 4;
+  const int n = p->N;
+  if (n < 6 || p->C <= 0) return 1;
+  p->bck[0] = kint;
+  p->bck[1] = kext;
+  p->binv.assign(binv, binv + (size_t)n * (n - 4) * std::max(p->lmax, 1));
+  p->d2bor.assign(d2bor, d2bor + (size_t)4 * n);
+  p->bc_ready = 1;
+  return 0;
+}
+
 extern "C" void orc_bc_tables(const orc_plan* p, double* binv, double* d2bor) {
   if (binv) std::copy(p->binv.begin(), p->binv.end(), binv);
   if (d2bor) std::copy(p->d2bor.begin(), p->d2bor.end(), d2bor);

@@ -95,6 +95,7 @@ void orc_invDl(const orc_plan* p, const double* phi, double* w);
 void orc_imposebc(const orc_plan* p, double* tor, double* phi, double* pol, int fast);
 /* binv (N x (N-4) x lmax, column-major per l) and d2bor (4 x N). */
 void orc_bc_tables(const orc_plan* p, double* binv, double* d2bor);
+int orc_bc_set_tables(orc_plan* p, int kint, int kext, const double* binv, const double* d2bor);
 
 /* Nonlinear term and RK3 (composed from the reference's building blocks):
  * state = (Z, W, phi) spectra (nz x nlm each), phi = D_l W.

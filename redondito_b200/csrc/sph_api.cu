@@ -927,84 +927,95 @@ extern "C" int sph_prodvec(sph_plan* p, const double* ar, const double* at, cons
 }
 
 // ---------------------------------------------------------------- boundary
-// Host FP64 pieces of invDl_setup (src/boundary/boundary_mod.f90:140-241).
+// Host pieces of invDl_setup (src/boundary/boundary_mod.f90:140-241), in
+// extended precision.  The reference builds the derivative matrices by
+// probing its FFT derivative with unit vectors (derivr_mat,
+// boundary_mod.f90:96-137) and factors B_l in FP64; both round at the
+// level of the largest matrix entries (about 1e-13 of them at nz = 128),
+// and B_l^-1 and the second derivative that phi = D_l W takes afterwards
+// amplify that to 1e-11 (no slip) and 1e-10 (free slip) in phi.  Here the
+// matrices come from a direct DFT with long double twiddles and sums, the
+// LU and the solve run in long double, and only binv and the four d2 rows
+// are rounded to FP64: W = binv phi is then correct to a few ulp.
 
-// One column of the FC-Gram radial derivative of order `order` applied to a
-// unit vector e_j, done on the host in FP64 with a direct DFT (setup only;
-// derivr_mat probes derivr the same way, boundary_mod.f90:122-133).
-static void host_derivr_matrix(const sph_plan* p, int order, std::vector<double>& D) {
+// Columns of the FC-Gram radial derivatives of orders 1 and 2 applied to the
+// unit vectors e_j on the N physical points: continuation (the z transform's
+// summation order), forward DFT / nz, (i kz)^order, inverse DFT, real part.
+static void host_derivr_matrices(const sph_plan* p, std::vector<ld>& D1, std::vector<ld>& D2) {
   const int nz = p->nz, n = p->N, C = p->C, d = p->d;
-  D.assign((size_t)n * n, 0.0);
-  std::vector<double> cs(nz * nz), sn(nz * nz);
+  D1.assign((size_t)n * n, 0.0L);
+  D2.assign((size_t)n * n, 0.0L);
+  std::vector<ld> cs((size_t)nz * nz), sn((size_t)nz * nz);
   for (int k = 0; k < nz; ++k)
     for (int j = 0; j < nz; ++j) {
-      ld a = -2.0L * kPi * (ld)((long)k * j % nz) / nz;
-      cs[(size_t)k * nz + j] = (double)cosl(a);
-      sn[(size_t)k * nz + j] = (double)sinl(a);
+      const ld a = -2.0L * kPi * (ld)((long)k * j % nz) / nz;
+      cs[(size_t)k * nz + j] = cosl(a);
+      sn[(size_t)k * nz + j] = sinl(a);
     }
-  std::vector<double> f(nz), Fr(nz), Fi(nz);
+  std::vector<ld> f(nz), Fr(nz), Fi(nz), R1(nz), I1(nz), R2(nz), I2(nz);
   for (int j = 0; j < n; ++j) {
-    std::fill(f.begin(), f.end(), 0.0);
-    f[j] = 1.0;
+    std::fill(f.begin(), f.end(), 0.0L);
+    f[j] = 1.0L;
     for (int ii = 0; ii < C; ++ii) {
-      double acc = p->dir[ii] * f[n - d] + p->dir[C - 1 - ii] * f[d - 1];
+      ld acc = (ld)p->dir[ii] * f[n - d] + (ld)p->dir[C - 1 - ii] * f[d - 1];
       for (int jj = 1; jj < d; ++jj)
-        acc = (acc + p->dir[ii + (size_t)C * jj] * f[n - d + jj]) + p->dir[(C - 1 - ii) + (size_t)C * jj] * f[d - 1 - jj];
+        acc = (acc + (ld)p->dir[ii + (size_t)C * jj] * f[n - d + jj]) +
+              (ld)p->dir[(C - 1 - ii) + (size_t)C * jj] * f[d - 1 - jj];
       f[n + ii] = acc;
     }
     for (int k = 0; k < nz; ++k) {
-      double sr = 0, si = 0;
+      ld sr = 0, si = 0;
       for (int q = 0; q < nz; ++q) {
         sr += cs[(size_t)k * nz + q] * f[q];
         si += sn[(size_t)k * nz + q] * f[q];
       }
-      // (i kz)^order / nz
-      double kp = 1.0;
-      for (int o = 0; o < order; ++o) kp *= p->kz[k];
-      double re = sr / nz, im = si / nz;
-      double r2 = re, i2 = im;
-      for (int o = 0; o < order; ++o) {
-        double t = -i2;
-        i2 = r2;
-        r2 = t;
-      }
-      Fr[k] = r2 * kp;
-      Fi[k] = i2 * kp;
+      const ld re = sr / nz, im = si / nz, kz = (ld)p->kz[k];
+      R1[k] = -kz * im;  // (i kz) (re + i im)
+      I1[k] = kz * re;
+      R2[k] = -kz * kz * re;  // (i kz)^2 (re + i im)
+      I2[k] = -kz * kz * im;
     }
     for (int i = 0; i < n; ++i) {
-      double sr = 0;
-      for (int k = 0; k < nz; ++k) sr += cs[(size_t)k * nz + i] * Fr[k] + sn[(size_t)k * nz + i] * Fi[k];
-      D[i + (size_t)n * j] = sr;  // real part of the inverse DFT (sign +1)
+      ld s1 = 0, s2 = 0;
+      for (int k = 0; k < nz; ++k) {  // real part of the inverse DFT (sign +1)
+        const ld c = cs[(size_t)k * nz + i], sv = sn[(size_t)k * nz + i];
+        s1 += c * R1[k] + sv * I1[k];
+        s2 += c * R2[k] + sv * I2[k];
+      }
+      D1[i + (size_t)n * j] = s1;
+      D2[i + (size_t)n * j] = s2;
     }
   }
 }
 
-static int lu_decompose(int n, std::vector<double>& a, std::vector<int>& piv) {
+// LU with partial pivoting (DGETRF's steps), column-major, in long double
+static int lu_decompose(int n, std::vector<ld>& a, std::vector<int>& piv) {
   piv.resize(n);
   for (int k = 0; k < n; ++k) {
     int pr = k;
-    double best = fabs(a[k + (size_t)n * k]);
+    ld best = fabsl(a[k + (size_t)n * k]);
     for (int i = k + 1; i < n; ++i)
-      if (fabs(a[i + (size_t)n * k]) > best) {
-        best = fabs(a[i + (size_t)n * k]);
+      if (fabsl(a[i + (size_t)n * k]) > best) {
+        best = fabsl(a[i + (size_t)n * k]);
         pr = i;
       }
     piv[k] = pr;
-    if (best == 0.0) return 1;
+    if (best == 0.0L) return 1;
     if (pr != k)
       for (int j = 0; j < n; ++j) std::swap(a[k + (size_t)n * j], a[pr + (size_t)n * j]);
-    double inv = 1.0 / a[k + (size_t)n * k];
+    const ld inv = 1.0L / a[k + (size_t)n * k];
     for (int i = k + 1; i < n; ++i) a[i + (size_t)n * k] *= inv;
     for (int j = k + 1; j < n; ++j) {
-      double f = a[k + (size_t)n * j];
-      if (f != 0.0)
+      const ld f = a[k + (size_t)n * j];
+      if (f != 0.0L)
         for (int i = k + 1; i < n; ++i) a[i + (size_t)n * j] -= a[i + (size_t)n * k] * f;
     }
   }
   return 0;
 }
 
-static void lu_apply(int n, const std::vector<double>& a, const std::vector<int>& piv, double* x) {
+// solve with the factors (DGETRS's steps), one right-hand side
+static void lu_apply(int n, const std::vector<ld>& a, const std::vector<int>& piv, ld* x) {
   for (int k = 0; k < n; ++k) std::swap(x[k], x[piv[k]]);
   for (int k = 0; k < n; ++k)
     for (int i = k + 1; i < n; ++i) x[i] -= a[i + (size_t)n * k] * x[k];
@@ -1012,6 +1023,60 @@ static void lu_apply(int n, const std::vector<double>& a, const std::vector<int>
     x[k] /= a[k + (size_t)n * k];
     for (int i = 0; i < k; ++i) x[i] -= a[i + (size_t)n * k] * x[k];
   }
+}
+
+// binv(:, :, l) for l = 1..lmax: columns 3..N-2 of B_l^-1 (invDl_setup's M_l),
+// the l spread over host threads
+static int host_binv(const sph_plan* p, int kin, int kout, const std::vector<ld>& d1, const std::vector<ld>& d2,
+                     std::vector<double>& binv) {
+  const int n = p->N, lmax = p->lmax;
+  binv.assign((size_t)std::max(lmax, 1) * n * (n - 4), 0.0);
+  const int nth = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  std::vector<int> failed(nth, 0);
+  std::vector<std::thread> th;
+  for (int t = 0; t < nth; ++t)
+    th.emplace_back([&, t]() {
+      std::vector<ld> b((size_t)n * n), esc(n), x(n);
+      std::vector<int> piv;
+      for (int l = 1 + t; l <= lmax; l += nth) {
+        std::fill(b.begin(), b.end(), 0.0L);
+        auto B = [&](int i, int j) -> ld& { return b[(i - 1) + (size_t)n * (j - 1)]; };
+        auto DM1 = [&](int i, int j) { return d1[(i - 1) + (size_t)n * (j - 1)]; };
+        auto DM2 = [&](int i, int j) { return d2[(i - 1) + (size_t)n * (j - 1)]; };
+        B(1, 1) = 1.0L;
+        // W' = 0 (noslip) or W'' - 2 W'/r = 0 (freeslip) at the inner wall
+        for (int j = 1; j <= n; ++j) B(2, j) = kin ? DM2(1, j) - 2.0L / (ld)p->z[0] * DM1(1, j) : DM1(1, j);
+        for (int i = 3; i <= n - 2; ++i) {
+          for (int j = 1; j <= n; ++j) B(i, j) = DM2(i, j);
+          const ld zi = (ld)p->z[i - 1];
+          B(i, i) = B(i, i) - (ld)(l * (l + 1)) / (zi * zi);
+        }
+        for (int j = 1; j <= n; ++j)
+          B(n - 1, j) = kout ? DM2(n, j) - 2.0L / (ld)p->z[n - 1] * DM1(n, j) : DM1(n, j);
+        B(n, n) = 1.0L;
+        for (int i = 1; i <= n; ++i) {  // rows scaled by their largest entry, as the reference does
+          ld mx = 0.0L;
+          for (int j = 1; j <= n; ++j) mx = std::max(mx, fabsl(B(i, j)));
+          esc[i - 1] = mx;
+          for (int j = 1; j <= n; ++j) B(i, j) /= mx;
+        }
+        if (lu_decompose(n, b, piv)) {
+          failed[t] = 1;
+          return;
+        }
+        double* M = &binv[(size_t)(l - 1) * n * (n - 4)];
+        for (int j = 0; j < n - 4; ++j) {
+          std::fill(x.begin(), x.end(), 0.0L);
+          x[j + 2] = 1.0L / esc[j + 2];
+          lu_apply(n, b, piv, x.data());
+          for (int i = 0; i < n; ++i) M[i + (size_t)n * j] = (double)x[i];
+        }
+      }
+    });
+  for (auto& x : th) x.join();
+  for (int f : failed)
+    if (f) return SPH_EINVAL;
+  return SPH_OK;
 }
 
 static int ensure_nl_scratch(sph_plan* p) {
@@ -1061,47 +1126,16 @@ extern "C" int sph_setup_bc(sph_plan* p, const char* bcint, const char* bcext) {
     p->bc_ready = 1;
     return SPH_OK;
   }
-  std::vector<double> d1, d2;
-  host_derivr_matrix(p, 1, d1);
-  host_derivr_matrix(p, 2, d2);
-  std::vector<double> binv((size_t)std::max(lmax, 1) * n * (n - 4), 0.0);
-  std::vector<double> b((size_t)n * n), esc(n);
-  std::vector<int> piv;
-  for (int l = 1; l <= lmax; ++l) {
-    std::fill(b.begin(), b.end(), 0.0);
-    auto B = [&](int i, int j) -> double& { return b[(i - 1) + (size_t)n * (j - 1)]; };
-    B(1, 1) = 1.0;
-    // W' = 0 (noslip) or W'' - 2 W'/r = 0 (freeslip) at the inner wall
-    for (int j = 1; j <= n; ++j)
-      B(2, j) = kin ? d2[0 + (size_t)n * (j - 1)] - 2.0 / p->z[0] * d1[0 + (size_t)n * (j - 1)]
-                    : d1[0 + (size_t)n * (j - 1)];
-    for (int i = 3; i <= n - 2; ++i) {
-      for (int j = 1; j <= n; ++j) B(i, j) = d2[(i - 1) + (size_t)n * (j - 1)];
-      B(i, i) = B(i, i) - (double)(l * (l + 1)) / (p->z[i - 1] * p->z[i - 1]);
-    }
-    for (int j = 1; j <= n; ++j)
-      B(n - 1, j) = kout ? d2[(n - 1) + (size_t)n * (j - 1)] - 2.0 / p->z[n - 1] * d1[(n - 1) + (size_t)n * (j - 1)]
-                         : d1[(n - 1) + (size_t)n * (j - 1)];
-    B(n, n) = 1.0;
-    for (int i = 1; i <= n; ++i) {
-      double mx = 0.0;
-      for (int j = 1; j <= n; ++j) mx = std::max(mx, fabs(B(i, j)));
-      esc[i - 1] = mx;
-      for (int j = 1; j <= n; ++j) B(i, j) /= mx;
-    }
-    if (lu_decompose(n, b, piv)) return SPH_EINVAL;
-    double* M = &binv[(size_t)(l - 1) * n * (n - 4)];
-    for (int j = 0; j < n - 4; ++j) {
-      M[(j + 2) + (size_t)n * j] = 1.0 / esc[j + 2];
-      lu_apply(n, b, piv, M + (size_t)n * j);
-    }
-  }
+  std::vector<ld> d1, d2;
+  host_derivr_matrices(p, d1, d2);
+  std::vector<double> binv;
+  RC(host_binv(p, kin, kout, d1, d2, binv));
   std::vector<double> d2bor((size_t)4 * n);
   for (int j = 0; j < n; ++j) {
-    d2bor[0 + 4 * (size_t)j] = d2[0 + (size_t)n * j];
-    d2bor[1 + 4 * (size_t)j] = d2[1 + (size_t)n * j];
-    d2bor[2 + 4 * (size_t)j] = d2[(n - 2) + (size_t)n * j];
-    d2bor[3 + 4 * (size_t)j] = d2[(n - 1) + (size_t)n * j];
+    d2bor[0 + 4 * (size_t)j] = (double)d2[0 + (size_t)n * j];
+    d2bor[1 + 4 * (size_t)j] = (double)d2[1 + (size_t)n * j];
+    d2bor[2 + 4 * (size_t)j] = (double)d2[(n - 2) + (size_t)n * j];
+    d2bor[3 + 4 * (size_t)j] = (double)d2[(n - 1) + (size_t)n * j];
   }
   double *db = nullptr, *dd = nullptr;
   int rc = upload(&db, binv.data(), binv.size());

@@ -258,6 +258,11 @@ class Server:
                 launch(s, r)
                 running.append(s)
             waiting = still_waiting
+            if waiting and not running:
+                # nothing runs and every idle slot of another size was released:
+                # the first waiting request is larger than the budget
+                raise MemoryError(f"request {waiting[0].rid} (lmax {waiting[0].lmax}, {waiting[0].kind}) "
+                                  f"does not fit an HBM budget of {self.budget / 1e9:.1f} GB")
             still = []
             for s in running:  # completions
                 if s.event.query():
@@ -271,10 +276,6 @@ class Server:
                 else:
                     still.append(s)
             running = still
-            if waiting and not running and not pending:
-                # nothing runs and nothing can be admitted: a request larger than the budget
-                raise MemoryError(f"request {waiting[0].rid} (lmax {waiting[0].lmax}, {waiting[0].kind}) "
-                                  f"does not fit an HBM budget of {self.budget / 1e9:.1f} GB")
         self.torch.cuda.synchronize()
         return requests
 

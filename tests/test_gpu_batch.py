@@ -7,15 +7,12 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from tests._helpers import check, rel_l2, random_spec
+from tests._helpers import check, check_derivative, rel_l2, random_spec
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
-TOL_CONT = 1e-11
-# the derivative of a z-inverted input passes through two FC-Gram continued
-# transforms, each amplifying round-off by the continuation operator
-TOL_DERIV = 1e-10
+TOL = 1e-12
 
 # (lmax, nz, nfields): the C4 ensemble's shapes at small sizes (nlat = 3(lmax+1)/2, nphi = 2 nlat)
 PROBLEMS = [(15, 32, 1), (31, 64, 3), (31, 32, 2), (63, 96, 1), (15, 64, 2), (63, 32, 3)]
@@ -71,9 +68,11 @@ def test_batch_equals_single_plan_calls(precision):
             if precision == "fp64":
                 P = orcs[p]
                 sr = P.z_inverse(x)
-                check(rel_l2(host(g), P.sh_synthesis(sr)), TOL_CONT)
-                check(rel_l2(host(d), P.derivr(sr, 1)), TOL_DERIV)
-                check(rel_l2(host(out), P.forward_3d(P.sh_synthesis(sr))), TOL_CONT)
+                check(rel_l2(host(s), sr), TOL, "z inverse")
+                check(rel_l2(host(g), P.sh_synthesis(sr)), TOL, "synthesis")
+                # the derivative of the same (device) input on both sides
+                check_derivative(host(d), P, host(s), 1, f"problem {p}")
+                check(rel_l2(host(out), P.forward_3d(P.sh_synthesis(sr))), TOL, "3D forward")
 
 
 def test_batch_replays():
@@ -114,7 +113,11 @@ def test_tile_shapes_do_not_change_results(precision):
     g1, o1 = run()
     S.set_tiles(G, 32 if prec else 0, 4, 32)
     g2, o2 = run()
-    tol = 1e-13 if precision == "fp64" else 1e-9
+    # FP64: the built-in shape takes the cluster forward phi kernel, the set
+    # ring pairs the single-CTA kernels, whose FFTs factor the length
+    # differently (rounding differs; the continuation of the forward 3D
+    # transform amplifies it); mixed: the MMA rows change the fp32 sums
+    tol = 1e-12 if precision == "fp64" else 1e-9
     for g, o in ((g1, o1), (g2, o2)):
         check(rel_l2(g, g0), tol)
         check(rel_l2(o, o0), tol)

@@ -1,8 +1,12 @@
-"""Neumann and Robin reconstructions (fcgram_mod.f90:267-650) and the
-freeslip wall kind on the GPU against the oracle, on the same inputs."""
+"""Neumann and Robin reconstructions (fcgram_mod.f90:267-650), the wall
+kinds of v_imposebc (vboundary.f90:59-130, noslip and freeslip) and the NL
+step with free-slip walls on the GPU, against the oracle on the same inputs
+and, for the boundary solve, against its extended-precision evaluation
+(oracle/extended.py)."""
 import numpy as np
 import pytest
 
+from oracle import extended as X
 from oracle import oracle as O
 from tests._helpers import check, random_spec, rel_l2
 
@@ -49,20 +53,44 @@ def test_robin_reconstruct():
     G.close()
 
 
-@pytest.mark.parametrize("kinds", [("freeslip", "freeslip"), ("freeslip", "noslip"), ("noslip", "freeslip")])
-def test_freeslip_imposebc(kinds):
+KINDS = [("noslip", "noslip"), ("freeslip", "freeslip"), ("freeslip", "noslip"), ("noslip", "freeslip")]
+TOL_W = 1e-14  # W = binv phi: binv correct to rounding, one FP64 product
+
+
+@pytest.mark.parametrize("kinds", KINDS)
+def test_imposebc_kinds(kinds):
+    """v_imposebc and v_imposebc_fast for each pair of wall kinds:
+    * against the oracle run on the extended-precision boundary tables (the
+      same steps on the same matrices, to rounding): whole arrays, 1e-12;
+    * against the extended-precision values on the physical rows: W within
+      1e-14, phi = D_l W within 1e-12;
+    * against the oracle's own restatement of invDl_setup (FP64 matrices
+      built by probing the FFT derivative): within that restatement's error
+      against the extended values, printed."""
     S, P, G = _pair()
+    Px = O.Plan(P.lmax, P.nz, C=25, d=5, rint=0.5, rext=1.5)
     P.bc_setup(kinds)
+    Px.bc_setup(kinds, tables=X.bc_tables(Px, kinds))
     S.setup_bc(G, kinds)
     rng = np.random.default_rng(12)
     tor, phi = random_spec(P, rng), random_spec(P, rng)
+    n = P.N
+    w_x, f_x = X.imposebc_rows(P, kinds, phi)
     for fast in (False, True):
-        t_ref, f_ref, w_ref = P.imposebc(tor, phi, fast=fast)
+        t_ref, f_ref, w_ref = Px.imposebc(tor, phi, fast=fast)
         T, F, W = dev(tor), dev(phi), G.new_spec()
         (S.v_imposebc_fast if fast else S.v_imposebc)(G, T, F, W)
-        check(rel_l2(T.cpu().numpy(), t_ref), 1e-15, f"{kinds} tor fast={fast}")
-        check(rel_l2(W.cpu().numpy(), w_ref), TOL, f"{kinds} pol fast={fast}")
-        check(rel_l2(F.cpu().numpy(), f_ref), TOL, f"{kinds} phi fast={fast}")
+        t, f, w = T.cpu().numpy(), F.cpu().numpy(), W.cpu().numpy()
+        check(rel_l2(t, t_ref), 1e-15, f"{kinds} tor fast={fast}")
+        check(rel_l2(w, w_ref), TOL, f"{kinds} W vs oracle(extended tables) fast={fast}")
+        check(rel_l2(f, f_ref), TOL, f"{kinds} phi vs oracle(extended tables) fast={fast}")
+        check(X.rel_l2(w[:n], w_x), TOL_W, f"{kinds} W vs extended fast={fast}")
+        check(X.rel_l2(f[:n], f_x), TOL, f"{kinds} phi vs extended fast={fast}")
+        _, f_o, w_o = P.imposebc(tor, phi, fast=fast)
+        ew, ef = X.rel_l2(w_o[:n], w_x), X.rel_l2(f_o[:n], f_x)
+        print(f"reference setup (oracle, FP64 matrices) vs extended: W {ew:.2e} phi {ef:.2e}")
+        check(rel_l2(w[:n], w_o[:n]), 2 * ew + TOL, f"{kinds} W vs oracle fast={fast}")
+        check(rel_l2(f[:n], f_o[:n]), 2 * ef + TOL, f"{kinds} phi vs oracle fast={fast}")
     G.close()
 
 
@@ -79,9 +107,11 @@ def test_freeslip_needs_the_reconstructor():
 
 
 def test_freeslip_nl_step():
+    """NL term and one RK3 step with free-slip walls, against the oracle on
+    the extended-precision boundary tables."""
     S, P, G = _pair(lmax=15, nz=64, nlat=24, nphi=48)
     kinds = ("freeslip", "freeslip")
-    P.bc_setup(kinds)
+    P.bc_setup(kinds, tables=X.bc_tables(P, kinds))
     S.setup_bc(G, kinds)
     rng = np.random.default_rng(3)
     Z = random_spec(P, rng, power=3.0)

@@ -13,7 +13,10 @@ mixed form to 1e-6 per output.
 
 C2: the vector nonlinear step at lmax 255, 384 x 768, nz 128, with the
 no-slip rows imposed by v_imposebc (src/boundary/vboundary.f90:59-87):
-the right-hand sides and the FP64 energy, and one RK3 step.
+the right-hand sides and the FP64 energy, and one RK3 step.  The oracle runs
+here on the boundary matrices evaluated in long double (oracle/extended.py),
+as the CUDA path builds them; the boundary solve is also compared with the
+extended-precision values themselves.
 
 The oracle runs on every host core (about a minute in all on 16 cores).
 """
@@ -23,6 +26,7 @@ import sys
 import numpy as np
 import pytest
 
+from oracle import extended as X
 from oracle import oracle as O
 from tests._helpers import check, random_spec
 
@@ -117,16 +121,19 @@ def test_c3_mixed_pair_against_oracle(c3):
 @pytest.fixture(scope="module")
 def c2():
     """C2: Z, W ~ N(0,1)(l+1)^-3 times a smooth radial profile, phi = D_l W,
-    the no-slip rows imposed by the oracle's v_imposebc."""
+    the no-slip rows imposed by the oracle's v_imposebc on the
+    extended-precision boundary tables (the CUDA path builds its matrices in
+    long double too; the reference's FP64 setup is compared separately)."""
     lmax, nz, nlat, nphi = 255, 128, 384, 768
     P = O.Plan(lmax, nz, nlat=nlat, nphi=nphi, C=25, d=5, rint=0.35, rext=1.0)
-    P.bc_setup()
+    P.bc_setup(("noslip", "noslip"), tables=X.bc_tables(P, ("noslip", "noslip")))
     rng = np.random.default_rng(20261203 + 2)
     Z0 = random_spec(P, rng, power=3.0)
     W0 = random_spec(P, rng, power=3.0)
     Z, phi, W = P.imposebc(Z0, P.dlr(W0))
     rz, rf, e = P.nl_rhs(Z, W, phi, 1e-3)
-    return dict(P=P, raw=(Z0, P.dlr(W0)), state=(Z, W, phi), nl=(rz, rf, e))
+    return dict(P=P, raw=(Z0, P.dlr(W0)), state=(Z, W, phi), nl=(rz, rf, e),
+                exact=X.imposebc_rows(P, ("noslip", "noslip"), P.dlr(W0)))
 
 
 def _gpu_plan(prec):
@@ -146,6 +153,10 @@ def test_c2_imposebc_fp64(c2):
     check(rel_dev(T, Z), TOL, "C2 tor")
     check(rel_dev(Wg, W), TOL, "C2 pol")
     check(rel_dev(F, phi), TOL, "C2 phi")
+    n = c2["P"].N
+    w_x, f_x = c2["exact"]
+    check(X.rel_l2(Wg.cpu().numpy()[:n], w_x), 1e-14, "C2 pol vs extended")
+    check(X.rel_l2(F.cpu().numpy()[:n], f_x), TOL, "C2 phi vs extended")
     G.close()
 
 

@@ -1,21 +1,23 @@
 """CUDA path vs the CPU oracle on identical seeded inputs (prueba_gpu.f90's
 design: same entry point, CPU oracle against the device path).  FP64
-transforms must agree to relative L2 <= 1e-12; outputs that pass through
-the FC-Gram continuation (which amplifies round-off by |A| ~ 5e3) and
-second radial derivatives are held to 1e-11."""
+transforms must agree to relative L2 <= 1e-12.  Radial derivatives are held
+against the extended-precision operator (oracle/extended.py) within the
+oracle's own error for the same field, at least 1e-12 (check_derivative);
+the boundary solve runs on the extended-precision tables on both sides."""
 import numpy as np
 import pytest
 
+from oracle import extended as X
 from oracle import oracle as O
-from tests._helpers import check, rel_l2, random_spec
+from tests._helpers import check, check_derivative, rel_l2, random_spec
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
+# also for the outputs through the FC-Gram continuation (3D forward
+# transforms), whose weights (up to 3.7e3) amplify the independent FP64
+# rounding of the two sides: measured up to 8e-13
 TOL = 1e-12
-TOL_CONT = 1e-11
-# second radial derivatives multiply the continuation's round-off by kz^2
-TOL_D2 = 1e-10
 
 
 def _pair(lmax, nz, C=0, d=0, nlat=None, nphi=None, rint=0.35, rext=1.0):
@@ -83,9 +85,9 @@ def test_z_transforms(nz, C, d):
     t = dev(f)
     S.fftp1d_real_to_complex_z(G, t)
     ref = P.z_forward(f)
-    check(rel_l2(host(t), ref), (TOL_CONT if C else TOL))
+    check(rel_l2(host(t), ref), TOL)
     S.fftp1d_complex_to_real_z(G, t)
-    check(rel_l2(host(t), P.z_inverse(ref)), (TOL_CONT if C else TOL))
+    check(rel_l2(host(t), P.z_inverse(ref)), TOL)
 
 
 @pytest.mark.parametrize("nz", [33, 58])
@@ -97,7 +99,6 @@ def test_config1_round_trip_and_derivative(nz):
     spec = random_spec(P, rng)
     grid_ref = P.sh_synthesis(spec)
     back_ref = P.sh_analysis(grid_ref)
-    der_ref = P.derivr(back_ref, 1)
     g = G.new_grid()
     s = G.new_spec()
     d = G.new_spec()
@@ -106,7 +107,7 @@ def test_config1_round_trip_and_derivative(nz):
     S.derivr(G, s, d, 1, "r")
     check(rel_l2(host(g), grid_ref), TOL)
     check(rel_l2(host(s), back_ref), TOL)
-    check(rel_l2(host(d), der_ref), TOL_CONT)
+    check_derivative(host(d), P, back_ref, 1, f"config 1 nz {nz}")
 
 
 def test_3d_pair():
@@ -117,7 +118,7 @@ def test_3d_pair():
     ref = P.forward_3d(grid)
     s = G.new_spec()
     S.fftp3d_real_to_complex(G, dev(grid), s)
-    check(rel_l2(host(s), ref), TOL_CONT)
+    check(rel_l2(host(s), ref), TOL)
     g = G.new_grid()
     back_ref = P.inverse_3d(ref)
     S.fftp3d_complex_to_real(G, dev(ref), g)
@@ -135,17 +136,32 @@ def pseudo():
 
 def test_derivr_ops(pseudo):
     S, P, G, a = pseudo
-    for order, tol in ((1, TOL_CONT), (2, TOL_D2)):
+    for order in (1, 2, 3, 4):
         b = G.new_spec()
         S.derivr(G, dev(a), b, order, "r")
-        check(rel_l2(host(b), P.derivr(a, order)), tol)
+        check_derivative(host(b), P, a, order, "derivr")
     ak = P.z_forward(a)
     b = G.new_spec()
     S.derivr(G, dev(ak), b, 1, "k")
     check(rel_l2(host(b), P.derivr(ak, 1, "k")), TOL)
     b = G.new_spec()
     S.dlr(G, dev(a), b)
-    check(rel_l2(host(b), P.dlr(a)), TOL_D2)
+    check_derivative(host(b), P, a, "dlr", "dlr")
+
+
+@pytest.mark.parametrize("nz", [33, 58, 64, 256])
+def test_derivr_sizes(nz):
+    """derivr orders 1-4 and dlr at radix-2/3 and generic lengths."""
+    from redondito_b200 import sphp as S
+    P, G = _pair(15, nz, C=25, d=5, nlat=24, nphi=48, rint=0.5, rext=1.5)
+    a = random_spec(P, np.random.default_rng(nz + 1))
+    for order in (1, 2, 3, 4):
+        b = G.new_spec()
+        S.derivr(G, dev(a), b, order, "r")
+        check_derivative(host(b), P, a, order, f"nz {nz}")
+    b = G.new_spec()
+    S.dlr(G, dev(a), b)
+    check_derivative(host(b), P, a, "dlr", f"nz {nz}")
 
 
 def test_pointwise_ops(pseudo):
@@ -163,7 +179,7 @@ def test_pointwise_ops(pseudo):
     check(rel_l2(host(c), P.saxpby_c(a, 2.0, y, -3.0)), 1e-15)
     f = dev(a)
     S.fc_filter(G, f, "r")
-    check(rel_l2(host(f), P.fc_filter(a)), TOL_CONT)
+    check(rel_l2(host(f), P.fc_filter(a)), TOL)
     ak = P.z_forward(a)
     f = dev(ak)
     S.fc_filter(G, f, "k")
@@ -185,32 +201,37 @@ def test_prodvec(pseudo):
 
 
 def test_boundary(pseudo):
+    """invDl and v_imposebc(_fast) with no-slip walls against the oracle on
+    the extended-precision boundary tables, which the CUDA path's long double
+    setup reproduces to rounding (the comparison with the extended values
+    themselves and with the oracle's own FP64 setup is in
+    test_gpu_boundary_kinds.py)."""
     S, P, G, a = pseudo
     S.setup_bc(G)
-    P.bc_setup()
+    P.bc_setup(("noslip", "noslip"), tables=X.bc_tables(P, ("noslip", "noslip")))
     rng = np.random.default_rng(11)
     tor = random_spec(P, rng)
     phi = random_spec(P, rng)
     w = G.new_spec()
     S.invDl(G, dev(phi), w)
-    check(rel_l2(host(w), P.invDl(phi)), TOL_CONT)
+    check(rel_l2(host(w), P.invDl(phi)), TOL)
     t_ref, f_ref, w_ref = P.imposebc(tor, phi)
     T, F, W = dev(tor), dev(phi), G.new_spec()
     S.v_imposebc(G, T, F, W)
     assert rel_l2(host(T), t_ref) == 0.0
-    check(rel_l2(host(W), w_ref), TOL_CONT)
-    check(rel_l2(host(F), f_ref), TOL_D2)
+    check(rel_l2(host(W), w_ref), TOL)
+    check(rel_l2(host(F), f_ref), TOL)
     t_ref, f_ref, w_ref = P.imposebc(tor, phi, fast=True)
     T, F, W = dev(tor), dev(phi), G.new_spec()
     S.v_imposebc_fast(G, T, F, W)
-    check(rel_l2(host(W), w_ref), TOL_CONT)
-    check(rel_l2(host(F), f_ref), TOL_D2)
+    check(rel_l2(host(W), w_ref), TOL)
+    check(rel_l2(host(F), f_ref), TOL)
 
 
 def test_nl_rhs_and_rk3():
     from redondito_b200 import sphp as S
     P, G = _pair(15, 64, C=25, d=5, nlat=24, nphi=48, rint=0.5, rext=1.5)
-    P.bc_setup()
+    P.bc_setup(("noslip", "noslip"), tables=X.bc_tables(P, ("noslip", "noslip")))
     S.setup_bc(G)
     rng = np.random.default_rng(3)
     Z = random_spec(P, rng, power=3.0)
@@ -220,15 +241,15 @@ def test_nl_rhs_and_rk3():
     rz, rf = G.new_spec(), G.new_spec()
     e = S.nl_rhs(G, dev(Z), dev(W), dev(phi), 1e-3, rz, rf)
     check(abs(e - e_ref) / e_ref, 1e-12)
-    check(rel_l2(host(rz), rz_ref), TOL_D2)
-    check(rel_l2(host(rf), rf_ref), TOL_D2)
+    check(rel_l2(host(rz), rz_ref), TOL)
+    check(rel_l2(host(rf), rf_ref), TOL)
     Zr, Wr, Fr, e_ref = P.rk3_step(Z, W, phi, 1e-3, 1e-4)
     Zg, Wg, Fg = dev(Z), dev(W), dev(phi)
     e = S.rk3_step(G, Zg, Wg, Fg, 1e-3, 1e-4)
     check(abs(e - e_ref) / e_ref, 1e-12)
-    check(rel_l2(host(Zg), Zr), TOL_D2)
-    check(rel_l2(host(Wg), Wr), TOL_D2)
-    check(rel_l2(host(Fg), Fr), TOL_D2)
+    check(rel_l2(host(Zg), Zr), TOL)
+    check(rel_l2(host(Wg), Wr), TOL)
+    check(rel_l2(host(Fg), Fr), TOL)
 
 
 @pytest.mark.parametrize("lmax,nlat,nphi", [(255, 384, 768), (511, 768, 1536)])
@@ -274,9 +295,9 @@ def test_3d_vector_pair():
     g = [G.new_grid() for _ in range(3)]
     S.fftp3d_qst_to_vec(G, *d, *g)
     for a, b in zip(g, ref_grids):
-        check(rel_l2(host(a), b), TOL_CONT)
+        check(rel_l2(host(a), b), TOL)
     ref = [P.z_forward(x) for x in P.qst_analysis(*ref_grids)]
     out = [G.new_spec() for _ in range(3)]
     S.fftp3d_vec_to_qst(G, *(dev(x) for x in ref_grids), *out)
     for a, b in zip(out, ref):
-        check(rel_l2(host(a), b), TOL_CONT)
+        check(rel_l2(host(a), b), TOL)

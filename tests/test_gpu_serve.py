@@ -45,8 +45,14 @@ def test_budget_releases_idle_slots_and_rejects_oversize():
     held never pass the budget, and a request larger than the budget is an
     error instead of a wait that never ends."""
     from redondito_b200 import serve
-    one = serve.estimate_bytes(127, "rk3", False) * 2
-    srv = _server("fp64", budget=1.6 * one)
+    probe = _server("fp64")
+    probe.warm([(127, "rk3"), (63, "rk3")])
+    measured = dict(probe.measured)
+    probe.close()
+    b127, b63 = measured[(127, "rk3", True)], measured[(63, "rk3", True)]
+    assert b127 > b63 > 0
+    srv = _server("fp64", budget=b127 + 0.5 * b63)  # one slot of either size, not both
+    srv.measured.update(measured)
     reqs = [serve.Request(i, 0.0005 * i, (127, 63)[i % 2], "rk3", 1) for i in range(6)]
     srv.serve(reqs)
     assert all(r.t_done is not None for r in reqs)

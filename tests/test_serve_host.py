@@ -43,3 +43,94 @@ def test_slot_estimates_grow_with_size_and_kind():
         assert all(p < r for p, r in zip(pairs, rk3))
     # an RK3 slot at lmax 511 holds the NL step's 9 grids and 15 spectra: tens of GB
     assert 25e9 < serve.estimate_bytes(511, "rk3", False) < 60e9
+
+
+# ---------------------------------------------------------------- admission, on fake slots
+import itertools
+import types
+
+import pytest
+
+
+class _FakeEvent:
+    def __init__(self):
+        self.polls = 0
+
+    def query(self):  # completes on the third poll after its launch
+        self.polls -= 1
+        return self.polls < 0
+
+
+class _FakeSlot:
+    live = 0
+
+    def __init__(self, S, torch, lmax, kind, precision, source=None):
+        self.lmax, self.kind, self.fresh = lmax, kind, source is None
+        self.plan = ("plan", lmax)
+        self.bytes = serve.estimate_bytes(lmax, kind, False) * (2 if self.fresh else 1)
+        self.event = _FakeEvent()
+        self.req, self.last_used = None, 0.0
+        _FakeSlot.live += 1
+
+    def close(self):
+        _FakeSlot.live -= 1
+
+
+def _fake_launch(slot, req):
+    slot.event.polls = 2
+
+
+@pytest.fixture
+def fake_server(monkeypatch):
+    monkeypatch.setattr(serve, "Slot", _FakeSlot)
+    monkeypatch.setattr(serve, "launch", _fake_launch)
+    S = types.SimpleNamespace(SPH_FP64=0, SPH_MIXED=1)
+    torch = types.SimpleNamespace(cuda=types.SimpleNamespace(synchronize=lambda: None))
+    _FakeSlot.live = 0
+
+    def make(budget):
+        tick = itertools.count()
+        return serve.Server(S, torch, S.SPH_FP64, budget, clock=lambda: next(tick) * 1e-4)
+    return make
+
+
+def _fresh(lmax, kind="rk3"):
+    return serve.estimate_bytes(lmax, kind, False) * 2
+
+
+def test_admission_waits_for_a_running_slot_instead_of_failing(fake_server):
+    """A request that does not fit while another runs waits; once that one
+    completes, its idle slot is released and the waiting request starts."""
+    srv = fake_server(_fresh(127) + 0.5 * _fresh(63))
+    reqs = [serve.Request(0, 0.0, 127, "rk3", 1), serve.Request(1, 0.0, 63, "rk3", 1)]
+    srv.serve(reqs)
+    assert all(r.t_done is not None for r in reqs)
+    assert reqs[1].t_admit >= reqs[0].t_done
+    assert srv.released == 1 and srv.peak_bytes <= srv.budget
+
+
+def test_admission_alternating_sizes_within_budget(fake_server):
+    srv = fake_server(_fresh(127) + 0.5 * _fresh(63))
+    reqs = [serve.Request(i, 2e-4 * i, (127, 63)[i % 2], "rk3", 1) for i in range(8)]
+    srv.serve(reqs)
+    assert all(r.t_done >= r.t_admit >= r.arrival for r in reqs)
+    assert srv.released >= 3 and srv.peak_bytes <= srv.budget
+    srv.close()
+    assert _FakeSlot.live == 0
+
+
+def test_admission_rejects_a_request_larger_than_the_budget(fake_server):
+    srv = fake_server(0.5 * _fresh(127))
+    with pytest.raises(MemoryError):
+        srv.serve([serve.Request(0, 0.0, 127, "rk3", 1), serve.Request(1, 1.0, 63, "pair")])
+
+
+def test_slots_of_one_size_are_reused_and_cloned(fake_server):
+    srv = fake_server(10 * _fresh(63))
+    reqs = [serve.Request(i, 0.0, 63, "pair") for i in range(3)]
+    srv.serve(reqs)
+    ss = srv.slots[(63, "pair")]
+    assert len(ss) == 3 and [s.fresh for s in ss] == [True, False, False]
+    more = [serve.Request(10 + i, 0.0, 63, "pair") for i in range(3)]
+    srv.serve(more)
+    assert srv.created == 3  # the idle slots took the second wave
