@@ -54,7 +54,8 @@ def save_table(table, path):
 def candidates(lmax, nz, nlat, nphi, precision):
     """Tile shapes that sph_plan_set_tiles accepts for this size."""
     rows = ROWS if precision else (0,)
-    # 0: the built-in choice (the cluster forward phi kernels where they tile nlat/2)
+    # 0: the built-in choice (FP64: the cluster forward phi kernel where its
+    # tiles divide nlat/2; mixed: the kernels chosen by the transform length)
     pairs = [0] + [r for r in RING_PAIRS if (nlat // 2) % r == 0 and r * nphi <= 8192]
     cols = [c for c in Z_COLS if c * nz <= 4096]
     return [dict(rows=r, ring_pairs=p, z_cols=c) for r, p, c in itertools.product(rows, pairs, cols)]

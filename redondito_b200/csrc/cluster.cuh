@@ -16,6 +16,18 @@ __device__ __forceinline__ uint32_t cluster_rank() {
 __device__ __forceinline__ void cluster_sync_all() {
   asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
+// the cluster barrier with this warp's arrival either releasing (what the
+// warp wrote or observed becomes visible to the cluster; its pending global
+// stores drain first) or relaxed (no ordering: for warps whose only pending
+// writes are global stores nobody in the cluster reads); `dep` is a value the
+// arrival waits for (a result of loads that must have completed first)
+__device__ __forceinline__ void cluster_sync_split(bool release, double dep = 0.0) {
+  if (release)
+    asm volatile("barrier.cluster.arrive.release.aligned;\n" ::"d"(dep) : "memory");
+  else
+    asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::"d"(dep) : "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
 // shared::cluster address of `p` (a shared-memory location of this CTA) in CTA `rank`
 __device__ __forceinline__ uint32_t cluster_map(const void* p, uint32_t rank) {
   uint32_t r;
@@ -25,6 +37,11 @@ __device__ __forceinline__ uint32_t cluster_map(const void* p, uint32_t rank) {
 __device__ __forceinline__ double ld_cluster_f64(uint32_t addr) {
   double v;
   asm volatile("ld.shared::cluster.f64 %0, [%1];\n" : "=d"(v) : "r"(addr) : "memory");
+  return v;
+}
+__device__ __forceinline__ double2 ld_cluster_f64x2(uint32_t addr) {  // addr 16-byte aligned
+  double2 v;
+  asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];\n" : "=d"(v.x), "=d"(v.y) : "r"(addr) : "memory");
   return v;
 }
 __device__ __forceinline__ int ld_cluster_s32(uint32_t addr) {

@@ -5,7 +5,8 @@
 // in natural order.  Lengths 2, 3, 4, 8 use the butterflies of fft_ct.cuh;
 // 6, 12, 16, 24 are four-step compositions R = R1 R2 whose twiddles are
 // constants computed by the compiler (Taylor series of cos and sin of the
-// reduced angle, exact at multiples of pi/2), so no table is read.
+// angle reduced to the first octant, exact at multiples of pi/2), so no
+// table is read.
 #pragma once
 #include <type_traits>
 
@@ -15,9 +16,11 @@ namespace ct {
 
 constexpr double kPi3 = 3.14159265358979323846264338327950288;
 
+// Taylor series of cos and sin for |x| <= pi/4, where every term is below
+// 0.31 in magnitude: the sums are within about one ulp
 __host__ __device__ constexpr double taylor_cos(double x) {
   double term = 1.0, sum = 1.0;
-  for (int n = 1; n < 26; ++n) {
+  for (int n = 1; n < 14; ++n) {
     term *= -x * x / ((2.0 * n - 1.0) * (2.0 * n));
     sum += term;
   }
@@ -25,20 +28,33 @@ __host__ __device__ constexpr double taylor_cos(double x) {
 }
 __host__ __device__ constexpr double taylor_sin(double x) {
   double term = x, sum = x;
-  for (int n = 1; n < 26; ++n) {
+  for (int n = 1; n < 14; ++n) {
     term *= -x * x / ((2.0 * n) * (2.0 * n + 1.0));
     sum += term;
   }
   return sum;
 }
-// cos and sin of 2 pi e / R, the angle reduced to (-pi, pi]
-__host__ __device__ constexpr int reduce_e(int e, int R) {
-  e %= R;
-  if (e < 0) e += R;
-  return 2 * e > R ? e - R : e;
+// cos (c = true) or sin of 2 pi e / R: the angle is brought to the first
+// octant with integer arithmetic, 8 e = o R + r, theta = (pi/4)(o + r/R) =
+// q pi/2 + s t with t = (pi/4) r/R (o even, s = +1) or (pi/4)(R - r)/R (o
+// odd, s = -1) and q = (o + (o odd)) / 2; then cos(q pi/2 + s t) and
+// sin(q pi/2 + s t) are +-cos t or +-sin t
+__host__ __device__ constexpr double cs2pi(int e, int R, bool c) {
+  long k = 8L * (((long)e % R + R) % R);
+  const int o = (int)(k / R);
+  const long r = k - (long)o * R;
+  const bool odd = o % 2 != 0;
+  const double t = (kPi3 / 4.0) * ((double)(odd ? R - r : r) / (double)R);
+  const double ct = taylor_cos(t), st = odd ? -taylor_sin(t) : taylor_sin(t);
+  switch (((o + (odd ? 1 : 0)) / 2) % 4) {
+    case 0: return c ? ct : st;
+    case 1: return c ? -st : ct;
+    case 2: return c ? -ct : -st;
+    default: return c ? st : -ct;
+  }
 }
-__host__ __device__ constexpr double cos2pi(int e, int R) { return taylor_cos(2.0 * kPi3 * reduce_e(e, R) / R); }
-__host__ __device__ constexpr double sin2pi(int e, int R) { return taylor_sin(2.0 * kPi3 * reduce_e(e, R) / R); }
+__host__ __device__ constexpr double cos2pi(int e, int R) { return cs2pi(e, R, true); }
+__host__ __device__ constexpr double sin2pi(int e, int R) { return cs2pi(e, R, false); }
 
 // compile-time loop: f(std::integral_constant<int, I>) for I in [B, E)
 template <int B, int E, typename F>

@@ -43,7 +43,6 @@
 #include "fft_ct.cuh"
 #include "tc05.cuh"
 #include "tma.cuh"
-#include "cluster.cuh"
 
 namespace {
 
@@ -1157,201 +1156,6 @@ __global__ void __launch_bounds__(PHI2_T, 2) phi2b_fwd32(Phi32Args a, const floa
   }
 }
 
-// ---------------------------------------------------------------- cluster three-step forward (fp32)
-// The forward transform with the tile of NPC = 4 CL ring pairs shared by a
-// cluster of CL CTAs, as the FP64 kernel phi3c_fwd64 (k_phifft.cu) does it:
-// CTA rank r stages by TMA the rows [r N/CL, (r+1) N/CL) of all NPC rings
-// and mirrors (runs of 8 NPC bytes), double buffered and swizzled, and
-// transforms ring pairs 4r..4r+3 from samples read across the cluster in
-// step (A); two cluster barriers per tile.  Here the transform runs in
-// fp32 and the fold writes the analysis tiles (bf16 x 3) like phi3_fwd32;
-// planes k >= ksplit come from the continued planes (the hi maps).
-template <int N, int CL>
-struct P3cf {
-  static constexpr int NPL = 4, NPC = NPL * CL;
-  static constexpr int A = 16, M = N / A, B = ct::pow2_part_cap16(M), C = M / B;
-  static constexpr int ROWS = N / CL, BR = largest_divisor_le(ROWS, 256), ROWB = NPC * 8;
-  static constexpr int SWB = CL == 4 ? 3 : 2;
-  static constexpr int ITEMS_A = NPL * M, ITEMS_B = NPL * A * C, ITEMS_C = NPL * A * B;
-  static constexpr int THREADS = ITEMS_A <= 64 ? 64 : (ITEMS_A + 31) / 32 * 32;
-  static constexpr int PR = M | 1;
-  static constexpr int SB = up_mod16(A * PR, 16 / NPL);  // half warps: 4 pairs x 4 rows, distinct 8-byte slots
-  static constexpr size_t XBYTES = (size_t)NPL * SB * sizeof(float2);
-  static constexpr size_t TILE_BYTES = (size_t)2 * ROWS * ROWB;
-  static constexpr size_t STAGE = round_up(XBYTES > TILE_BYTES ? XBYTES : TILE_BYTES, 1024);
-  static constexpr size_t SMEM = 2 * STAGE + (size_t)N * sizeof(float2) + 64;
-  static __device__ __forceinline__ uint32_t off(int row, int col) {
-    const uint32_t o = (uint32_t)(row * ROWB + col * 8);
-    return o ^ (((o >> 7) & ((1u << SWB) - 1)) << 4);
-  }
-};
-
-template <int N, int CL>
-constexpr bool phi3cf_ok() {
-  if constexpr (N % 16 != 0 || N < 48 || (CL != 2 && CL != 4)) {
-    return false;
-  } else {
-    using G = P3cf<N, CL>;
-    return G::THREADS <= 1024 && ((size_t)G::ROWS * G::ROWB) % 1024 == 0 && (G::BR * G::ROWB) % 1024 == 0 &&
-           G::SMEM <= 227 * 1024;
-  }
-}
-
-struct Phi3cMaps {
-  CUtensorMap lo[SPH_MAX_FIELDS], hi[SPH_MAX_FIELDS];
-};
-
-template <int N, int CL>
-__global__ void __launch_bounds__(P3cf<N, CL>::THREADS, 1)
-    phi3c_fwd32(Phi32Args a, int ntiles, const __grid_constant__ Phi3cMaps maps) {
-  using G = P3cf<N, CL>;
-  constexpr int A = G::A, M = G::M, B = G::B, C = G::C, T = G::THREADS, NPL = G::NPL, NPC = G::NPC;
-  constexpr int ROWS = G::ROWS, BR = G::BR;
-  extern __shared__ __align__(1024) unsigned char smc[];
-  float2* tw = reinterpret_cast<float2*>(smc + 2 * G::STAGE);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smc + 2 * G::STAGE + (size_t)N * sizeof(float2));
-  int* bad = reinterpret_cast<int*>(full + 2);  // this CTA's last wait gave up (read by the cluster)
-  const int t = threadIdx.x;
-  const uint32_t rank = cluster_rank();
-  const int cid = blockIdx.x / CL, ncl = gridDim.x / CL;
-  const int nlat = a.nlat, ngroups = nlat / 2 / NPC;
-  for (int i = t; i < N; i += T) tw[i] = __ldg(a.twN + i);
-  if (t == 0) {
-    tc05::mbar_init(&full[0], 1);
-    tc05::mbar_init(&full[1], 1);
-    *bad = 0;
-    tc05::mbar_fence_init();
-  }
-  __syncthreads();
-  cluster_sync_all();  // every CTA of the cluster runs before any reads another's shared memory
-  auto stage = [&](int w) { return smc + (size_t)w * G::STAGE; };
-  auto issue = [&](int tile, int w) {  // one thread: this CTA's rows of a tile, rings then mirrors
-    const int g = tile % ngroups, r = tile / ngroups, k = r % a.nz, f = r / a.nz;
-    const bool lo = k < a.ksplit;
-    const CUtensorMap* map = lo ? &maps.lo[f] : &maps.hi[f];
-    const int y0 = (lo ? k : k - a.ksplit) * N + (int)rank * ROWS;
-    unsigned char* st = stage(w);
-    tma::expect_tx(&full[w], (uint32_t)G::TILE_BYTES);
-#pragma unroll 1
-    for (int i = 0; i < ROWS / BR; ++i) {
-      tma::load_2d(st + (size_t)i * BR * G::ROWB, map, g * NPC, y0 + i * BR, &full[w]);
-      tma::load_2d(st + (size_t)(ROWS + i * BR) * G::ROWB, map, nlat - g * NPC - NPC, y0 + i * BR, &full[w]);
-    }
-  };
-  int tile = cid;
-  if (t == 0 && tile < ntiles) issue(tile, 0);
-  int s = 0;
-  uint32_t phase = 0;
-  bool gave_up = false;
-  for (; tile < ntiles; tile += ncl, s ^= 1) {
-    const bool ok = tc05::mbar_wait(&full[s], (phase >> s) & 1);
-    const int mine = __syncthreads_or(!ok);
-    if (t == 0) *bad = mine;
-    cluster_sync_all();  // (1) every CTA's rows of this tile have landed, or a wait gave up
-    int any = 0;
-#pragma unroll
-    for (int r = 0; r < CL; ++r) any |= ld_cluster_s32(cluster_map(bad, r));
-    if (any) {  // every CTA of the cluster leaves here, on the same tile
-      gave_up = mine != 0;
-      break;
-    }
-    phase ^= 1u << s;
-    if (t == 0 && tile + ncl < ntiles) {
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      issue(tile + ncl, s ^ 1);
-    }
-    const int g = tile % ngroups, rr = tile / ngroups, k = rr % a.nz, f = rr / a.nz;
-    const int p0 = g * NPC + (int)rank * NPL;
-    const bool act = t < G::ITEMS_A;
-    const int b = t % NPL, nm = t / NPL;
-    float2 v[A];
-    if (act) {  // (A) samples x[nm + M n1] of local ring pair b
-      const int col = (int)rank * NPL + b;
-      uint32_t base[CL];
-#pragma unroll
-      for (int o = 0; o < CL; ++o) base[o] = cluster_map(stage(s), o);
-#pragma unroll
-      for (int n1 = 0; n1 < A; ++n1) {
-        constexpr int PER = A / CL;
-        const int o = n1 / PER, jr = nm + M * (n1 - o * PER);
-        v[n1] = make_float2((float)ld_cluster_f64(base[o] + G::off(jr, col)),
-                            (float)ld_cluster_f64(base[o] + (uint32_t)(ROWS * G::ROWB) + G::off(jr, NPC - 1 - col)));
-      }
-    }
-    cluster_sync_all();  // (2) no CTA reads this stage of another any more
-    float2* X = reinterpret_cast<float2*>(stage(s));
-    if (act) {
-      ct::RD<float2, A, -1>::run(v);
-      float2* xo = X + b * G::SB + nm;
-#pragma unroll
-      for (int ka = 0; ka < A; ++ka) xo[ka * G::PR] = ka ? ct::mul(v[ka], tw[nm * ka]) : v[ka];
-    }
-    __syncthreads();
-    if constexpr (B > 1) {  // (B)
-      for (int it = t; it < G::ITEMS_B; it += T) {
-        const int ka = it % A, r2 = it / A, c = r2 % C, bb = r2 / C;
-        float2* row = X + bb * G::SB + ka * G::PR + c;
-        float2 w[B];
-#pragma unroll
-        for (int nb = 0; nb < B; ++nb) w[nb] = row[C * nb];
-        ct::RD<float2, B, -1>::run(w);
-#pragma unroll
-        for (int kb = 0; kb < B; ++kb) row[C * kb] = (kb && c) ? ct::mul(w[kb], tw[A * c * kb]) : w[kb];
-      }
-      __syncthreads();
-    }
-    if constexpr (C > 1) {  // (C)
-      for (int it = t; it < G::ITEMS_C; it += T) {
-        const int ka = it % A, r2 = it / A, kb = r2 % B, bb = r2 / B;
-        float2* row = X + bb * G::SB + ka * G::PR + C * kb;
-        float2 u[C];
-#pragma unroll
-        for (int c = 0; c < C; ++c) u[c] = row[c];
-        ct::RD<float2, C, -1>::run(u);
-#pragma unroll
-        for (int kc = 0; kc < C; ++kc) row[kc] = u[kc];
-      }
-      __syncthreads();
-    }
-    // fold both parities of the NPL ring pairs, weight, split, write tile rows (as phi3_fwd32)
-    float W[NPL];
-#pragma unroll
-    for (int q = 0; q < NPL; ++q) W[q] = (float)__ldg(a.wfold + p0 + q);
-    const int cb = k / PLANES, row = 2 * (k % PLANES), kt = p0 / TK, kk0 = p0 % TK;
-    auto zpos = [&](int m) {
-      const int q = m / A;
-      return (m % A) * G::PR + C * (q % B) + q / B;
-    };
-    for (int m = t; m <= a.lmax; m += T) {
-      const int pz = zpos(m), pc = zpos(m == 0 ? 0 : N - m);
-      float er[NPL], ei[NPL], orr[NPL], oi[NPL];
-#pragma unroll
-      for (int q = 0; q < NPL; ++q) {
-        const float2 Z = X[q * G::SB + pz], Zc = X[q * G::SB + pc];
-        // F(ring) = (Z + conj Z(-m))/2, F(mirror) = -i (Z - conj Z(-m))/2
-        const float fir = 0.5f * (Z.x + Zc.x), fii = 0.5f * (Z.y - Zc.y);
-        const float fmr = 0.5f * (Z.y + Zc.y), fmi = -0.5f * (Z.x - Zc.x);
-        er[q] = (fir + fmr) * W[q];
-        ei[q] = (fii + fmi) * W[q];
-        orr[q] = (fir - fmr) * W[q];
-        oi[q] = (fii - fmi) * W[q];
-      }
-      __nv_bfloat16* t0 = a.tiles + ana_tile(a.lmax, a.ncb, a.nkn, f, m, 0, cb, kt) * TILE_HALVES;
-      __nv_bfloat16* t1 = a.tiles + ana_tile(a.lmax, a.ncb, a.nkn, f, m, 1, cb, kt) * TILE_HALVES;
-      store_tile_row<NPL>(t0, row, kk0, er);
-      store_tile_row<NPL>(t0, row + 1, kk0, ei);
-      store_tile_row<NPL>(t1, row, kk0, orr);
-      store_tile_row<NPL>(t1, row + 1, kk0, oi);
-    }
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-  }
-  if (gave_up && t == 0) {  // report, and let the copy still in flight land before leaving
-    atomicExch(a.flag, 1);
-    tc05::mbar_wait(&full[s], (phase >> s) & 1);
-  }
-  cluster_sync_all();  // no CTA leaves while another may still read its shared memory
-}
-
 // FC-Gram continuation of physical planes (FP64), one grid point per
 // thread: out(ii) = sum_jj dir(ii,jj) f(N-d+jj) + dir(C-1-ii,jj) f(d-1-jj),
 // the same operator the z transform applies to spectral planes
@@ -1939,80 +1743,6 @@ int phi3_run(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st
   }
 }
 
-template <int N, int CL>
-int phi3cf_run(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st) {
-  if constexpr (!phi3cf_ok<N, CL>()) {
-    return PHI3_UNSUPPORTED;
-  } else {
-    using G = P3cf<N, CL>;
-    if (p->nlat2 % G::NPC || !a.flag) return PHI3_UNSUPPORTED;
-    const long long ntiles = (long long)(p->nlat2 / G::NPC) * p->nz * nfields;
-    if (ntiles == 0) return SPH_OK;
-    if (ntiles > (1ll << 30) || (long long)N * p->nz > (1ll << 31) - 1) return PHI3_UNSUPPORTED;
-    Phi3cMaps maps;
-    const CUtensorMapSwizzle swz = CL == 4 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
-    const bool hi = a.ksplit < p->nz;
-    for (int f = 0; f < nfields; ++f) {
-      if (!tma::grid_map(&maps.lo[f], a.gin[f], p->nlat, (long long)N * a.ksplit, G::NPC, G::BR,
-                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, swz))
-        return PHI3_UNSUPPORTED;
-      if (!tma::grid_map(&maps.hi[f], hi ? a.gin_hi[f] : a.gin[f], p->nlat,
-                         (long long)N * (hi ? p->nz - a.ksplit : a.ksplit), G::NPC, G::BR,
-                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, swz))
-        return PHI3_UNSUPPORTED;
-    }
-    for (int f = nfields; f < SPH_MAX_FIELDS; ++f) maps.lo[f] = maps.hi[f] = maps.lo[0];
-    auto kern = phi3c_fwd32<N, CL>;
-    static DeviceOnce once;
-    if (!once.run([] {
-          return cudaFuncSetAttribute(phi3c_fwd32<N, CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)G::SMEM) == cudaSuccess &&
-                 cudaFuncSetAttribute(phi3c_fwd32<N, CL>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) ==
-                     cudaSuccess;
-        }))
-      return SPH_ECUDA;
-    cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = CL;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.blockDim = dim3(G::THREADS);
-    cfg.dynamicSmemBytes = G::SMEM;
-    cfg.stream = st;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cfg.gridDim = dim3(CL);
-    int nclusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg) != cudaSuccess || nclusters < 1)
-      return PHI3_UNSUPPORTED;
-    const long long ncl = std::min<long long>(nclusters, ntiles);
-    cfg.gridDim = dim3((unsigned)(ncl * CL));
-    if (cudaLaunchKernelEx(&cfg, kern, a, (int)ntiles, maps) != cudaSuccess) return SPH_ECUDA;
-    return SPH_OK;
-  }
-}
-
-// cluster size 4 where nlat/2 splits into tiles of 16 ring pairs, else 2;
-// a plan with ring pairs set by sph_plan_set_tiles keeps the kernels those
-// settings were tuned on
-int phi3cf_dispatch(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st) {
-  if (p->tile_np) return PHI3_UNSUPPORTED;
-  switch (p->nphi) {
-#define CASE(n)                                                  \
-  case n:                                                        \
-    if (p->nlat2 % 16 == 0) {                                    \
-      const int rc = phi3cf_run<n, 4>(p, a, nfields, st);        \
-      if (rc != PHI3_UNSUPPORTED) return rc;                     \
-    }                                                            \
-    if (p->nlat2 % 8 == 0) return phi3cf_run<n, 2>(p, a, nfields, st); \
-    return PHI3_UNSUPPORTED;
-    PHI32_SIZES(CASE)
-#undef CASE
-  }
-  return PHI3_UNSUPPORTED;
-}
-
 // two-pass forward: lengths whose 8-ring-pair tile fits shared memory only once
 template <int N>
 constexpr bool phi2_ok() {
@@ -2170,10 +1900,6 @@ int launch_phi_fwd32(const sph_plan* p, const double* const* grids, int nfields,
   for (int f = 0; f < nfields; ++f)
     aligned = aligned && reinterpret_cast<uintptr_t>(a.gin[f]) % 16 == 0 &&
               (!grids_hi || reinterpret_cast<uintptr_t>(a.gin_hi[f]) % 16 == 0);
-  if (aligned) {
-    const int rc = phi3cf_dispatch(p, a, nfields, st);
-    if (rc != PHI3_UNSUPPORTED) return rc;
-  }
   {
     const int rc = phi2_dispatch(p, a, nfields, st);
     if (rc != PHI3_UNSUPPORTED) return rc;

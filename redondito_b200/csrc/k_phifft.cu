@@ -433,12 +433,17 @@ int phi3d_dispatch_n(const sph_plan* p, const PhiArgs& a, int nfields, cudaStrea
 // of all NPC rings and mirrors (runs of 8 NPC bytes: 64 B for CL = 2, 128 B
 // for CL = 4), double buffered, and transforms ring pairs 4r .. 4r+3, whose
 // samples it reads across the cluster from distributed shared memory in
-// step (A).  Two cluster barriers per tile: (1) every CTA's rows have landed
-// (or a bounded wait gave up, which every CTA then sees), (2) no CTA reads
-// another's staged rows any more, so each overwrites its own with its
-// transform area.  Steps (A), (B), (C) and the fold are those of the
-// three-step inverse run forwards (sign -1); the fold writes the folded
-// coefficients G[m][parity][k][node] like phi_fwd_ct.  The staged rows are
+// step (A).  Three cluster barriers per tile: (1) every CTA's rows have
+// landed (or a bounded wait gave up, which every CTA then sees), (2) no CTA
+// reads another's staged rows any more, so each overwrites its own with its
+// transform area, (3) every CTA's spectra are complete.  Steps (A), (B), (C)
+// are those of the three-step inverse run forwards (sign -1).  The fold runs
+// across the cluster: each warp folds a few m for all NPC ring pairs, reading
+// the spectra where they were transformed, so that the folded coefficients
+// G[m][parity][k][node] go out in runs of 8 NPC bytes.  Only warp 0, which
+// stores nothing to global memory, arrives at the barriers with release
+// semantics; the folding warps arrive relaxed, so their stores are not
+// drained at every barrier.  The staged rows are
 // swizzled by the TMA (16-byte chunk index XOR 128-byte row index), so the
 // step-(A) reads of a half warp (4 ring pairs x 4 rows) spread over the
 // banks; the transform area has an odd row pitch and a ring-pair stride of
@@ -492,7 +497,7 @@ __global__ void __launch_bounds__(P3c<N, CL>::THREADS, 1)
   double2* tw = reinterpret_cast<double2*>(sm3c + 2 * G::STAGE);
   uint64_t* full = reinterpret_cast<uint64_t*>(sm3c + 2 * G::STAGE + (size_t)N * sizeof(double2));
   int* bad = reinterpret_cast<int*>(full + 2);  // this CTA's last wait gave up (read by the cluster)
-  const int t = threadIdx.x;
+  const int t = threadIdx.x, warp = t / 32;
   const uint32_t rank = cluster_rank();
   const int cid = blockIdx.x / CL, ncl = gridDim.x / CL;
   const int nlat = a.nlat, ngroups = nlat / 2 / NPC;
@@ -528,7 +533,11 @@ __global__ void __launch_bounds__(P3c<N, CL>::THREADS, 1)
     const bool ok = tc05::mbar_wait(&full[s], (phase >> s) & 1);
     const int mine = __syncthreads_or(!ok);
     if (t == 0) *bad = mine;
-    cluster_sync_all();  // (1)
+    // (1) every CTA's rows of this tile have landed, or a wait gave up; warp 0
+    // (which observed the copies' completion and wrote `bad`, and holds no
+    // global stores) releases, the folding warps arrive relaxed so that their
+    // stores of the last tile do not drain here
+    cluster_sync_split(warp == 0);
     int any = 0;
 #pragma unroll
     for (int r = 0; r < CL; ++r) any |= ld_cluster_s32(cluster_map(bad, r));
@@ -542,7 +551,6 @@ __global__ void __launch_bounds__(P3c<N, CL>::THREADS, 1)
       issue(tile + ncl, s ^ 1);
     }
     const int g = tile % ngroups, rr = tile / ngroups, k = rr % a.nz, f = rr / a.nz;
-    const int p0 = g * NPC + (int)rank * NPL;
     // (A) the samples x[nm + M n1] of local ring pair b (ring: real part, mirror: imaginary part)
     const bool act = t < G::ITEMS_A;
     const int b = t % NPL, nm = t / NPL;
@@ -559,11 +567,13 @@ __global__ void __launch_bounds__(P3c<N, CL>::THREADS, 1)
         v[n1] = make_double2(ld_cluster_f64(base[o] + G::off(jr, col)),
                              ld_cluster_f64(base[o] + (uint32_t)(ROWS * G::ROWB) + G::off(jr, NPC - 1 - col)));
       }
+      ct::RD<double2, A, -1>::run(v);
     }
-    cluster_sync_all();  // (2)
+    // (2) no CTA reads another's staged rows any more: every sample has been
+    // loaded (the arrival waits for v[0] = the sum of all of them)
+    cluster_sync_split(false, act ? v[0].x + v[0].y : 0.0);
     double2* X = reinterpret_cast<double2*>(stage(s));
     if (act) {
-      ct::RD<double2, A, -1>::run(v);
       double2* xo = X + b * G::SB + nm;
 #pragma unroll
       for (int ka = 0; ka < A; ++ka) xo[ka * G::PR] = ka ? ct::mul(v[ka], tw[nm * ka]) : v[ka];
@@ -595,22 +605,38 @@ __global__ void __launch_bounds__(P3c<N, CL>::THREADS, 1)
       }
       __syncthreads();
     }
-    // fold both parities of one (m, pair) from Z(m), Z(-m), as phi_fwd_ct
-    double2* Gp = a.G + (size_t)f * a.Gfield + (size_t)k * a.ldn + p0;
-    const size_t mstride = (size_t)2 * a.nz * a.ldn, pstride = (size_t)a.nz * a.ldn;
-    const double W = __ldg(a.wfold + p0 + b);
-    auto zpos = [&](int m) {
-      const int q = m / A;
-      return (m % A) * G::PR + C * (q % B) + q / B;
-    };
-    for (int m = t / NPL; m <= a.lmax; m += T / NPL) {
-      const double2 Z = X[b * G::SB + zpos(m)];
-      const double2 Zc = X[b * G::SB + zpos(m == 0 ? 0 : N - m)];
-      // F(i) = (Z + conj Z(-m))/2, F(mirror) = -i (Z - conj Z(-m))/2
-      double2 Fi = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y - Zc.y));
-      double2 Fm = make_double2(0.5 * (Z.y + Zc.y), -0.5 * (Z.x - Zc.x));
-      Gp[m * mstride + b] = cscale(cadd(Fi, Fm), W);
-      Gp[m * mstride + pstride + b] = cscale(csub(Fi, Fm), W);
+    // (3) every CTA's spectra of the tile are in its stage: warp 0 releases
+    // them for the cluster (the __syncthreads above ordered the CTA's writes
+    // before it)
+    cluster_sync_split(warp == 0);
+    // fold across the cluster: a warp takes 32 / NPC values of m and all NPC
+    // ring pairs of the tile (their spectra in the CTAs that transformed
+    // them), so that each (m, parity) row of NPC nodes is one 8 NPC-byte run
+    // (256 bytes for CL = 4); CTA rank r takes every CL-th group of m, and
+    // warp 0 none: it holds no global stores at the releasing barriers
+    if (warp > 0) {
+      constexpr int MW = 32 / NPC;  // m values per warp step
+      const int lane = t % 32, q = lane % NPC, mi = lane / NPC;
+      const uint32_t xb = cluster_map(X, (uint32_t)(q / NPL)) + (uint32_t)((q % NPL) * G::SB) * 16u;
+      double2* Gp = a.G + (size_t)f * a.Gfield + (size_t)k * a.ldn + g * NPC + q;
+      const size_t mstride = (size_t)2 * a.nz * a.ldn, pstride = (size_t)a.nz * a.ldn;
+      const double W = __ldg(a.wfold + g * NPC + q);
+      auto zpos = [&](int m) {
+        const int qq = m / A;
+        return (m % A) * G::PR + C * (qq % B) + qq / B;
+      };
+      const int nw = T / 32 - 1;
+      for (int grp = (int)rank + CL * (warp - 1); grp * MW <= a.lmax; grp += CL * nw) {
+        const int m = grp * MW + mi;
+        if (m > a.lmax) continue;
+        const double2 Z = ld_cluster_f64x2(xb + (uint32_t)zpos(m) * 16u);
+        const double2 Zc = ld_cluster_f64x2(xb + (uint32_t)zpos(m == 0 ? 0 : N - m) * 16u);
+        // F(i) = (Z + conj Z(-m))/2, F(mirror) = -i (Z - conj Z(-m))/2
+        double2 Fi = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y - Zc.y));
+        double2 Fm = make_double2(0.5 * (Z.y + Zc.y), -0.5 * (Z.x - Zc.x));
+        Gp[m * mstride] = cscale(cadd(Fi, Fm), W);
+        Gp[m * mstride + pstride] = cscale(csub(Fi, Fm), W);
+      }
     }
     // this stage is refilled by TMA (async proxy) after the next barrier
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
