@@ -1019,7 +1019,12 @@ __global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB_INV) phi3_
 // in shared memory ([b][ka][nm], pitches PR and SB), one contiguous image per
 // (plane, tile).  Pass 2 bulk-copies an image into shared memory (double
 // buffered) and finishes steps (B), (C), the fold and the tile rows.
-constexpr int PHI2_PB = 16, PHI2_NMC = 16, PHI2_NP = 8, PHI2_BATCH = 64;
+// The passes alternate over batches of PHI2_BATCH plane-fields, whose images
+// (77 MB at nphi 1536) stay in the 126 MB L2 between the passes: pass 1
+// streams the grid past L2 (loads marked evict-first) and pass 2 drops each
+// image's lines once it has read them (discard, no write-back), so the
+// images need not reach HBM at all.
+constexpr int PHI2_PB = 16, PHI2_NMC = 16, PHI2_NP = 8, PHI2_BATCH = 16;
 
 template <int N>
 __global__ void __launch_bounds__(PHI2_PB* PHI2_NMC, 2) phi2a_fwd32(Phi32Args a, float2* img, int q0) {
@@ -1036,7 +1041,7 @@ __global__ void __launch_bounds__(PHI2_PB* PHI2_NMC, 2) phi2a_fwd32(Phi32Args a,
 #pragma unroll
   for (int n1 = 0; n1 < A; ++n1) {
     const double* row = pl + (size_t)(nm + M * n1) * nlat;
-    v[n1] = make_float2((float)__ldg(row + pair), (float)__ldg(row + (nlat - 1 - pair)));
+    v[n1] = make_float2((float)__ldcs(row + pair), (float)__ldcs(row + (nlat - 1 - pair)));
   }
   ct::RD<float2, A, -1>::run(v);
 #pragma unroll
@@ -1100,6 +1105,13 @@ __global__ void __launch_bounds__(PHI2_T, 2) phi2b_fwd32(Phi32Args a, const floa
         tc05::mbar_wait(full, phase);
       }
       return;
+    }
+    {  // the image has landed and is not read again: drop its L2 lines without
+       // writing them back (the lines it shares with a neighbouring image stay)
+      const uintptr_t b0 = reinterpret_cast<uintptr_t>(img + ((size_t)ql * ngroups + g) * XF);
+      const uintptr_t lo = (b0 + 127) & ~(uintptr_t)127, hi = (b0 + G::XBYTES) & ~(uintptr_t)127;
+      for (uintptr_t o = lo + (uintptr_t)t * 128; o < hi; o += (uintptr_t)T * 128)
+        asm volatile("discard.global.L2 [%0], 128;\n" ::"l"(o) : "memory");
     }
     if constexpr (B > 1) {  // (B)
       for (int it = t; it < G::ITEMS_B; it += T) {
