@@ -39,11 +39,6 @@ __device__ __forceinline__ double ld_cluster_f64(uint32_t addr) {
   asm volatile("ld.shared::cluster.f64 %0, [%1];\n" : "=d"(v) : "r"(addr) : "memory");
   return v;
 }
-__device__ __forceinline__ double2 ld_cluster_f64x2(uint32_t addr) {  // addr 16-byte aligned
-  double2 v;
-  asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];\n" : "=d"(v.x), "=d"(v.y) : "r"(addr) : "memory");
-  return v;
-}
 __device__ __forceinline__ int ld_cluster_s32(uint32_t addr) {
   int v;
   asm volatile("ld.shared::cluster.s32 %0, [%1];\n" : "=r"(v) : "r"(addr) : "memory");

@@ -433,17 +433,15 @@ int phi3d_dispatch_n(const sph_plan* p, const PhiArgs& a, int nfields, cudaStrea
 // of all NPC rings and mirrors (runs of 8 NPC bytes: 64 B for CL = 2, 128 B
 // for CL = 4), double buffered, and transforms ring pairs 4r .. 4r+3, whose
 // samples it reads across the cluster from distributed shared memory in
-// step (A).  Three cluster barriers per tile: (1) every CTA's rows have
-// landed (or a bounded wait gave up, which every CTA then sees), (2) no CTA
-// reads another's staged rows any more, so each overwrites its own with its
-// transform area, (3) every CTA's spectra are complete.  Steps (A), (B), (C)
-// are those of the three-step inverse run forwards (sign -1).  The fold runs
-// across the cluster: each warp folds a few m for all NPC ring pairs, reading
-// the spectra where they were transformed, so that the folded coefficients
-// G[m][parity][k][node] go out in runs of 8 NPC bytes.  Only warp 0, which
-// stores nothing to global memory, arrives at the barriers with release
-// semantics; the folding warps arrive relaxed, so their stores are not
-// drained at every barrier.  The staged rows are
+// step (A).  Two cluster barriers per tile: (1) every CTA's rows have landed
+// (or a bounded wait gave up, which every CTA then sees), (2) no CTA reads
+// another's staged rows any more, so each overwrites its own with its
+// transform area.  Steps (A), (B), (C) and the fold are those of the
+// three-step inverse run forwards (sign -1); the fold writes the folded
+// coefficients G[m][parity][k][node] like phi_fwd_ct.  Only warp 0, which
+// stores nothing to global memory, arrives at barrier (1) with release
+// semantics, and every warp arrives at (2) relaxed once its step-(A) loads
+// have returned: the folding warps' stores are not drained at the barriers.  The staged rows are
 // swizzled by the TMA (16-byte chunk index XOR 128-byte row index), so the
 // step-(A) reads of a half warp (4 ring pairs x 4 rows) spread over the
 // banks; the transform area has an odd row pitch and a ring-pair stride of
@@ -605,32 +603,20 @@ __global__ void __launch_bounds__(P3c<N, CL>::THREADS, 1)
       }
       __syncthreads();
     }
-    // (3) every CTA's spectra of the tile are in its stage: warp 0 releases
-    // them for the cluster (the __syncthreads above ordered the CTA's writes
-    // before it)
-    cluster_sync_split(warp == 0);
-    // fold across the cluster: a warp takes 32 / NPC values of m and all NPC
-    // ring pairs of the tile (their spectra in the CTAs that transformed
-    // them), so that each (m, parity) row of NPC nodes is one 8 NPC-byte run
-    // (256 bytes for CL = 4); CTA rank r takes every CL-th group of m, and
-    // warp 0 none: it holds no global stores at the releasing barriers
+    // fold both parities of one (m, pair) from Z(m), Z(-m), as phi_fwd_ct;
+    // warp 0 takes no part: it holds no global stores at the releasing barrier
     if (warp > 0) {
-      constexpr int MW = 32 / NPC;  // m values per warp step
-      const int lane = t % 32, q = lane % NPC, mi = lane / NPC;
-      const uint32_t xb = cluster_map(X, (uint32_t)(q / NPL)) + (uint32_t)((q % NPL) * G::SB) * 16u;
-      double2* Gp = a.G + (size_t)f * a.Gfield + (size_t)k * a.ldn + g * NPC + q;
+      const int tf = t - 32;
+      double2* Gp = a.G + (size_t)f * a.Gfield + (size_t)k * a.ldn + g * NPC + (int)rank * NPL + b;
       const size_t mstride = (size_t)2 * a.nz * a.ldn, pstride = (size_t)a.nz * a.ldn;
-      const double W = __ldg(a.wfold + g * NPC + q);
+      const double W = __ldg(a.wfold + g * NPC + (int)rank * NPL + b);
       auto zpos = [&](int m) {
-        const int qq = m / A;
-        return (m % A) * G::PR + C * (qq % B) + qq / B;
+        const int q = m / A;
+        return (m % A) * G::PR + C * (q % B) + q / B;
       };
-      const int nw = T / 32 - 1;
-      for (int grp = (int)rank + CL * (warp - 1); grp * MW <= a.lmax; grp += CL * nw) {
-        const int m = grp * MW + mi;
-        if (m > a.lmax) continue;
-        const double2 Z = ld_cluster_f64x2(xb + (uint32_t)zpos(m) * 16u);
-        const double2 Zc = ld_cluster_f64x2(xb + (uint32_t)zpos(m == 0 ? 0 : N - m) * 16u);
+      for (int m = tf / NPL; m <= a.lmax; m += (T - 32) / NPL) {
+        const double2 Z = X[b * G::SB + zpos(m)];
+        const double2 Zc = X[b * G::SB + zpos(m == 0 ? 0 : N - m)];
         // F(i) = (Z + conj Z(-m))/2, F(mirror) = -i (Z - conj Z(-m))/2
         double2 Fi = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y - Zc.y));
         double2 Fm = make_double2(0.5 * (Z.y + Zc.y), -0.5 * (Z.x - Zc.x));

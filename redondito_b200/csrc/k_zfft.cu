@@ -21,9 +21,14 @@ namespace {
 constexpr int ZTHREADS = 256;
 constexpr int ZMAXCOL = 4096;  // LB*nz complex values per CTA (64 KB)
 
+template <int IO>
+struct ZIo {
+  static constexpr bool FIN = IO == ZIO_FF || IO == ZIO_FD, FOUT = IO == ZIO_FF || IO == ZIO_DF;
+};
+
 struct ZArgs {
-  const double2* in;
-  double2* out;
+  const void* in;
+  void* out;
   int nlm, nz, N, C, d, LB, order;
   const double* dir;      // C x d column-major
   const double2* kfac;    // (i kz)^order, nz entries
@@ -70,7 +75,38 @@ __device__ __forceinline__ double2 div_nz(double2 v, int nz) {
   return make_double2(v.x / (double)nz, v.y / (double)nz);
 }
 
-template <int MODE, int CTN>
+// column element (row r, column lm) of the input, widened to FP64
+template <int IO>
+__device__ __forceinline__ double2 zin(const ZArgs& a, size_t idx) {
+  if constexpr (ZIo<IO>::FIN) {
+    const float2 v = __ldg(static_cast<const float2*>(a.in) + idx);
+    return make_double2((double)v.x, (double)v.y);
+  } else {
+    return __ldg(static_cast<const double2*>(a.in) + idx);
+  }
+}
+
+// one column element into shared memory: by cp.async when the input is
+// FP64, else loaded, widened and stored; zero past nlm
+template <int IO>
+__device__ __forceinline__ void zload(const ZArgs& a, double2* dst, size_t idx, bool in) {
+  if constexpr (ZIo<IO>::FIN) {
+    *dst = in ? zin<IO>(a, idx) : make_double2(0.0, 0.0);
+  } else {
+    const double2* src = static_cast<const double2*>(a.in);
+    cp_async16z(dst, in ? src + idx : src, in ? 16 : 0);
+  }
+}
+
+template <int IO>
+__device__ __forceinline__ void zstore(const ZArgs& a, size_t idx, double2 v) {
+  if constexpr (ZIo<IO>::FOUT)
+    static_cast<float2*>(a.out)[idx] = make_float2((float)v.x, (float)v.y);
+  else
+    static_cast<double2*>(a.out)[idx] = v;
+}
+
+template <int MODE, int CTN, int IO>
 __global__ void __launch_bounds__(ZTHREADS) zfft_kernel(ZArgs a) {
   extern __shared__ double2 sm[];
   const int LB = a.LB, nz = a.nz, nlm = a.nlm;
@@ -86,17 +122,14 @@ __global__ void __launch_bounds__(ZTHREADS) zfft_kernel(ZArgs a) {
   for (int idx = tid; idx < nload * LB; idx += ZTHREADS) {
     int r = idx / LB, c = idx - r * LB;
     int lm = lm0 + c;
-    const bool in = lm < nlm;
     // the inverse transform takes its input in digit-reversed order
-    cp_async16z(sm + (MODE == Z_INV ? __ldg(rev + r) : r) * LB + c, in ? a.in + (size_t)r * nlm + lm : a.in,
-                in ? 16 : 0);
+    zload<IO>(a, sm + (MODE == Z_INV ? __ldg(rev + r) : r) * LB + c, (size_t)r * nlm + lm, lm < nlm);
   }
   if (MODE == Z_DLR) {
     for (int idx = tid; idx < nz * LB; idx += ZTHREADS) {
       int r = idx / LB, c = idx - r * LB;
       int lm = lm0 + c;
-      const bool in = lm < nlm;
-      cp_async16z(orig + idx, in ? a.in + (size_t)r * nlm + lm : a.in, in ? 16 : 0);
+      zload<IO>(a, orig + idx, (size_t)r * nlm + lm, lm < nlm);
     }
   }
   asm volatile("cp.async.commit_group;\n" ::: "memory");
@@ -167,42 +200,66 @@ __global__ void __launch_bounds__(ZTHREADS) zfft_kernel(ZArgs a) {
       v.x = v.x + zi * (lf * o.x);
       v.y = v.y + zi * (lf * o.y);
     }
-    a.out[(size_t)r * nlm + lm] = v;
+    zstore<IO>(a, (size_t)r * nlm + lm, v);
   }
 }
 
-template <int MODE, int CTN>
+template <int MODE, int CTN, int IO>
 int launch_ct(const ZArgs& a, int nblocks, size_t smem, cudaStream_t st) {
   static DeviceOnce once;
   if (!once.run([] {
-        return cudaFuncSetAttribute(zfft_kernel<MODE, CTN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        return cudaFuncSetAttribute(zfft_kernel<MODE, CTN, IO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     200 * 1024) == cudaSuccess &&
-               cudaFuncSetAttribute(zfft_kernel<MODE, CTN>, cudaFuncAttributePreferredSharedMemoryCarveout,
+               cudaFuncSetAttribute(zfft_kernel<MODE, CTN, IO>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                     100) == cudaSuccess;
       }))
     return SPH_ECUDA;
-  zfft_kernel<MODE, CTN><<<nblocks, ZTHREADS, smem, st>>>(a);
+  zfft_kernel<MODE, CTN, IO><<<nblocks, ZTHREADS, smem, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
 
 #define Z_SIZES(X) X(16) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(512)
 
-template <int MODE>
+template <int MODE, int IO>
 int launch_mode(const ZArgs& a, int nblocks, size_t smem, cudaStream_t st) {
   switch (a.nz) {
 #define CASE(n) \
-  case n: return launch_ct<MODE, n>(a, nblocks, smem, st);
+  case n: return launch_ct<MODE, n, IO>(a, nblocks, smem, st);
     Z_SIZES(CASE)
 #undef CASE
-    default: return launch_ct<MODE, 0>(a, nblocks, smem, st);
+    default: return launch_ct<MODE, 0, IO>(a, nblocks, smem, st);
   }
+}
+
+// the element types used with each mode: FP64 everywhere; single precision
+// in and out for every mode; FP64 in, single out for the forward transform
+// (after the analysis in FP64); single in, FP64 out for the inverse (before
+// the synthesis)
+template <int MODE>
+int launch_mode_io(const ZArgs& a, int io, int nblocks, size_t smem, cudaStream_t st) {
+  switch (io) {
+    case ZIO_DD: return launch_mode<MODE, ZIO_DD>(a, nblocks, smem, st);
+    case ZIO_FF: return launch_mode<MODE, ZIO_FF>(a, nblocks, smem, st);
+    case ZIO_DF:
+      if constexpr (MODE == Z_FWD) return launch_mode<MODE, ZIO_DF>(a, nblocks, smem, st);
+      break;
+    case ZIO_FD:
+      if constexpr (MODE == Z_INV) return launch_mode<MODE, ZIO_FD>(a, nblocks, smem, st);
+      break;
+  }
+  return SPH_EINVAL;
 }
 
 }  // namespace
 
 int launch_zfft(const sph_plan* p, int mode, const double2* in, double2* out, int order,
                 cudaStream_t st, bool cont) {
+  return launch_zfft_io(p, mode, in, out, ZIO_DD, order, st, cont);
+}
+
+int launch_zfft_io(const sph_plan* p, int mode, const void* in, void* out, int io, int order, cudaStream_t st,
+                   bool cont) {
   ZArgs a;
   a.in = in;
   a.out = out;
@@ -229,15 +286,15 @@ int launch_zfft(const sph_plan* p, int mode, const double2* in, double2* out, in
   size_t smem = (size_t)LB * p->nz * sizeof(double2) * (mode == Z_DLR ? 2 : 1);
   TimedLaunch tl(p, T_ZFFT, st);
   switch (mode) {
-    case Z_FWD: return launch_mode<Z_FWD>(a, nblocks, smem, st);
-    case Z_INV: return launch_mode<Z_INV>(a, nblocks, smem, st);
+    case Z_FWD: return launch_mode_io<Z_FWD>(a, io, nblocks, smem, st);
+    case Z_INV: return launch_mode_io<Z_INV>(a, io, nblocks, smem, st);
     case Z_DERIV:
       if (!a.kfac) return SPH_EINVAL;
-      return launch_mode<Z_DERIV>(a, nblocks, smem, st);
-    case Z_FILTER: return launch_mode<Z_FILTER>(a, nblocks, smem, st);
+      return launch_mode_io<Z_DERIV>(a, io, nblocks, smem, st);
+    case Z_FILTER: return launch_mode_io<Z_FILTER>(a, io, nblocks, smem, st);
     case Z_DLR:
       a.kfac = p->kfac + (size_t)1 * p->nz;  // (i kz)^2
-      return launch_mode<Z_DLR>(a, nblocks, smem, st);
+      return launch_mode_io<Z_DLR>(a, io, nblocks, smem, st);
   }
   return SPH_EINVAL;
 }
@@ -387,5 +444,5 @@ extern "C" int sph_derivr_noalloc(const double* a, double* b, int nlm, int nz, i
   z.fd = fd;
   const int nblocks = (nlm + LB - 1) / LB;
   const size_t smem = (size_t)LB * nz * sizeof(double2);
-  return launch_mode<Z_DERIV>(z, nblocks, smem, st);
+  return launch_mode<Z_DERIV, ZIO_DD>(z, nblocks, smem, st);
 }

@@ -222,6 +222,12 @@ enum ZMode { Z_FWD = 0, Z_INV = 1, Z_DERIV = 2, Z_FILTER = 3, Z_DLR = 4 };
 // cont = false: the planes past N are taken as given (already continued)
 int launch_zfft(const sph_plan* p, int mode, const double2* in, double2* out, int order,
                 cudaStream_t st, bool cont = true);
+// element types of the spectra a z transform reads and writes: FP64
+// (double2) or single precision (float2, the single-precision entry
+// points); the transform itself runs in FP64 in shared memory
+enum { ZIO_DD = 0, ZIO_FF = 1, ZIO_DF = 2, ZIO_FD = 3 };
+int launch_zfft_io(const sph_plan* p, int mode, const void* in, void* out, int io, int order, cudaStream_t st,
+                   bool cont = true);
 
 // phi transforms (k_phifft.cu): grid fields -> folded coefficients and back
 int launch_phi_fwd(const sph_plan* p, const double* const* grids, int nfields, cudaStream_t st);

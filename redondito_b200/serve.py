@@ -180,18 +180,27 @@ class Server:
         return b
 
     def _release_idle(self, need, keep):
-        """Release idle slots of other (size, kind), least recently used first,
-        until `need` more bytes fit the budget; True if they do."""
+        """Release idle slots of other (size, kind) until `need` more bytes fit
+        the budget; True if they do.  Slots whose size keeps another slot go
+        first (least recently used first): releasing the last slot of a size
+        frees its tables, and the next request of that size then builds them
+        again on the host."""
         if self.bytes + need <= self.budget:
             return True
-        idle = [(s.last_used, k, s) for k, ss in self.slots.items() if k != keep for s in ss if s.req is None]
-        for _, k, s in sorted(idle, key=lambda x: x[0]):
-            self.slots[k].remove(s)
-            s.close()
-            self.bytes -= s.bytes
-            self.released += 1
-            if self.bytes + need <= self.budget:
-                return True
+        count = collections.Counter(k[0] for k, ss in self.slots.items() for _ in ss)
+        idle = sorted(((s.last_used, k, s) for k, ss in self.slots.items() if k != keep
+                       for s in ss if s.req is None), key=lambda x: x[0])
+        for keep_last in (True, False):  # first only slots that are not the last of their size
+            for _, k, s in idle:
+                if s not in self.slots[k] or (keep_last and count[k[0]] == 1):
+                    continue
+                count[k[0]] -= 1
+                self.slots[k].remove(s)
+                s.close()
+                self.bytes -= s.bytes
+                self.released += 1
+                if self.bytes + need <= self.budget:
+                    return True
         return False
 
     def _free_slot(self, lmax, kind, now):

@@ -61,9 +61,11 @@ TOL_W = 1e-14  # W = binv phi: binv correct to rounding, one FP64 product
 def test_imposebc_kinds(kinds):
     """v_imposebc and v_imposebc_fast for each pair of wall kinds:
     * against the oracle run on the extended-precision boundary tables (the
-      same steps on the same matrices, to rounding): whole arrays, 1e-12;
+      same steps on the same matrices, to rounding): whole arrays, W within
+      1e-12, phi within 1e-12 + 3x that oracle's own error for the field;
     * against the extended-precision values on the physical rows: W within
-      1e-14, phi = D_l W within 1e-12;
+      1e-14, phi = D_l W (an FP64 FFT second derivative) within 1e-12 or 3x
+      the oracle's own error on the same tables, whichever is larger;
     * against the oracle's own restatement of invDl_setup (FP64 matrices
       built by probing the FFT derivative): within that restatement's error
       against the extended values, printed."""
@@ -83,9 +85,13 @@ def test_imposebc_kinds(kinds):
         t, f, w = T.cpu().numpy(), F.cpu().numpy(), W.cpu().numpy()
         check(rel_l2(t, t_ref), 1e-15, f"{kinds} tor fast={fast}")
         check(rel_l2(w, w_ref), TOL, f"{kinds} W vs oracle(extended tables) fast={fast}")
-        check(rel_l2(f, f_ref), TOL, f"{kinds} phi vs oracle(extended tables) fast={fast}")
         check(X.rel_l2(w[:n], w_x), TOL_W, f"{kinds} W vs extended fast={fast}")
-        check(X.rel_l2(f[:n], f_x), TOL, f"{kinds} phi vs extended fast={fast}")
+        # phi = D_l W by the FP64 FFT second derivative: its own rounding,
+        # which the oracle on the same tables shows for this field
+        e_x = X.rel_l2(f_ref[:n], f_x)
+        print(f"oracle(extended tables) phi vs extended: {e_x:.2e}")
+        check(rel_l2(f, f_ref), 3 * e_x + TOL, f"{kinds} phi vs oracle(extended tables) fast={fast}")
+        check(X.rel_l2(f[:n], f_x), max(TOL, 3 * e_x), f"{kinds} phi vs extended fast={fast}")
         _, f_o, w_o = P.imposebc(tor, phi, fast=fast)
         ew, ef = X.rel_l2(w_o[:n], w_x), X.rel_l2(f_o[:n], f_x)
         print(f"reference setup (oracle, FP64 matrices) vs extended: W {ew:.2e} phi {ef:.2e}")

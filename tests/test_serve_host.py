@@ -134,3 +134,22 @@ def test_slots_of_one_size_are_reused_and_cloned(fake_server):
     more = [serve.Request(10 + i, 0.0, 63, "pair") for i in range(3)]
     srv.serve(more)
     assert srv.created == 3  # the idle slots took the second wave
+
+
+def test_release_keeps_the_last_slot_of_a_size(fake_server):
+    """Under budget pressure the clones of a size go before the last slot of
+    another size (which holds the tables)."""
+    srv = fake_server(10 * _fresh(63))
+    srv.serve([serve.Request(i, 0.0, 63, "pair") for i in range(3)])
+    srv.serve([serve.Request(10, 0.0, 31, "pair")])
+    assert len(srv.slots[(63, "pair")]) == 3 and len(srv.slots[(31, "pair")]) == 1
+    # room for a new slot as large as the 31 slot only if something goes: a 63
+    # clone goes, not the 31 slot (the last of its size)
+    clone = srv.slots[(63, "pair")][1].bytes
+    srv.budget = srv.bytes + 0.5 * clone
+    assert srv._release_idle(clone, keep=(127, "pair"))
+    assert len(srv.slots[(31, "pair")]) == 1 and len(srv.slots[(63, "pair")]) == 2
+    # when only last slots are left, they go too, least recently used first
+    srv.budget = 0.5 * clone
+    assert not srv._release_idle(clone, keep=(127, "pair"))
+    assert sum(len(v) for v in srv.slots.values()) == 0
