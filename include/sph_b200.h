@@ -332,6 +332,34 @@ int sph_energy_spectrum(sph_plan* plan, const double* Z, const double* W, double
 int sph_run(sph_plan* plan, double* Z, double* W, double* phi, double nu, double dt, int nsteps, int tstep,
             int sstep, int filter, const char* outdir, double* energy_out, void* stream);
 
+/* ---------------------------------------------------------------- single precision
+ * The arrays of a GSINGLE_PRECISION build of the reference
+ * (src/sphp/fprecision_mod.F90:13-18: REAL(KIND=GP), COMPLEX(KIND=GP) with
+ * GP = 4): each routine below is its FP64 counterpart above with float
+ * arrays (grids: float[nz][nphi][nlat]; spectra: float pairs [nz][nlm]), on
+ * an SPH_MIXED plan over whole fields (SPH_EINVAL otherwise).  The mixed
+ * engine reads and writes the float grids in its phi FFTs and the float
+ * spectra in its z transforms directly; results agree with the FP64 path to
+ * the mixed form's accuracy and float rounding.  The inverse transforms
+ * preserve their input. */
+int sph_fftp2d_real_to_complex_xy_f32(sph_plan* plan, const float* in, float* out, void* stream);
+int sph_fftp2d_complex_to_real_xy_f32(sph_plan* plan, const float* in, float* out, void* stream);
+int sph_fftp1d_real_to_complex_z_f32(sph_plan* plan, float* inout, void* stream);
+int sph_fftp1d_complex_to_real_z_f32(sph_plan* plan, float* inout, void* stream);
+int sph_fftp3d_real_to_complex_f32(sph_plan* plan, const float* in, float* out, void* stream);
+int sph_fftp3d_complex_to_real_f32(sph_plan* plan, const float* in, float* out, void* stream);
+int sph_fftp2d_vec_to_qst_f32(sph_plan* plan, const float* vr, const float* vt, const float* vp, float* q,
+                              float* s, float* t, void* stream);
+int sph_fftp2d_qst_to_vec_f32(sph_plan* plan, const float* q, const float* s, const float* t, float* vr,
+                              float* vt, float* vp, void* stream);
+int sph_fftp3d_vec_to_qst_f32(sph_plan* plan, const float* vr, const float* vt, const float* vp, float* q,
+                              float* s, float* t, void* stream);
+int sph_fftp3d_qst_to_vec_f32(sph_plan* plan, const float* q, const float* s, const float* t, float* vr,
+                              float* vt, float* vp, void* stream);
+int sph_derivr_f32(sph_plan* plan, const float* a, float* b, int p, char esp, void* stream);
+int sph_dlr_f32(sph_plan* plan, const float* a, float* b, void* stream);
+int sph_fc_filter_f32(sph_plan* plan, float* a, char esp, void* stream);
+
 /* ---------------------------------------------------------------- timers
  * The reference accumulates wall time per stage in gtimer handles
  * (src/sphp/sphp_mod.F90:36-41: comtime, ffttime, conttime, tottime;

@@ -495,10 +495,12 @@ __host__ __device__ inline int seq_stride(int nphi) {
 }
 
 struct Phi32Args {
-  const double* gin[SPH_MAX_FIELDS];
-  const double* gin_hi[SPH_MAX_FIELDS];  // planes k >= ksplit (continued planes)
+  // grids: double, or float for the single-precision entry points (the
+  // kernels' GT template parameter says which)
+  const void* gin[SPH_MAX_FIELDS];
+  const void* gin_hi[SPH_MAX_FIELDS];  // planes k >= ksplit (continued planes)
   int ksplit;
-  double* gout[SPH_MAX_FIELDS];
+  void* gout[SPH_MAX_FIELDS];
   __nv_bfloat16* tiles;  // analysis data tiles (forward output)
   const float2* G32c;    // folded coefficients (inverse input)
   size_t G32field;
@@ -510,6 +512,14 @@ struct Phi32Args {
   const float2* twN;
   int* flag;  // set when a bounded wait gives up (three-step forward)
 };
+
+// plane k of field f of the forward input: from the grid below ksplit, from
+// the continued planes above
+template <typename GT>
+__device__ __forceinline__ const GT* in_plane(const Phi32Args& a, int f, int k, int N) {
+  return k < a.ksplit ? static_cast<const GT*>(a.gin[f]) + (size_t)k * N * a.nlat
+                      : static_cast<const GT*>(a.gin_hi[f]) + (size_t)(k - a.ksplit) * N * a.nlat;
+}
 
 // Four-step forward phi FFT geometry (N = N1 N2, NP ring pairs per CTA),
 // the register-staged fallback for grids whose rows cannot be staged by TMA
@@ -534,7 +544,7 @@ struct P4 {
 // k1 giving Z(k1 + N1 k2), written back over the row; (3) thread m folds
 // both parities of the NP nodes from Z(m), Z(-m) and writes them, split, as
 // row chunks of the analysis tiles.
-template <int N, int NP>
+template <int N, int NP, typename GT>
 __global__ void __launch_bounds__(P4<N, NP>::THREADS, 2) phi4_fwd32(Phi32Args a) {
   using C = P4<N, NP>;
   constexpr int N1 = C::N1, N2 = C::N2;
@@ -542,12 +552,11 @@ __global__ void __launch_bounds__(P4<N, NP>::THREADS, 2) phi4_fwd32(Phi32Args a)
   const int nlat = a.nlat;
   const int p0 = blockIdx.x * NP, k = blockIdx.y, f = blockIdx.z;
   const int t = threadIdx.x;
-  const double* plane =
-      k < a.ksplit ? a.gin[f] + (size_t)k * N * nlat : a.gin_hi[f] + (size_t)(k - a.ksplit) * N * nlat;
+  const GT* plane = in_plane<GT>(a, f, k, N);
   for (int it = t; it < NP * N2; it += C::THREADS) {
     const int b = it % NP, n2 = it / NP;
-    const double* pr = plane + p0 + b;               // ring p0 + b (real part)
-    const double* pm = plane + (nlat - 1 - p0 - b);  // its mirror (imaginary part)
+    const GT* pr = plane + p0 + b;               // ring p0 + b (real part)
+    const GT* pm = plane + (nlat - 1 - p0 - b);  // its mirror (imaginary part)
     float2 v[N1];
 #pragma unroll
     for (int n1 = 0; n1 < N1; ++n1) {
@@ -610,15 +619,14 @@ __global__ void __launch_bounds__(P4<N, NP>::THREADS, 2) phi4_fwd32(Phi32Args a)
 // thread of degree m then reads Z(m), Z(-m) of its NP ring pairs from
 // consecutive addresses, folds both parities and writes them, split, as row
 // chunks of the analysis tiles.
-template <int N, int NP>
+template <int N, int NP, typename GT>
 __global__ void __launch_bounds__(PTHREADS, 2) phi_fwd32(Phi32Args a) {
   extern __shared__ float2 sf[];
   constexpr int Q = 2 * NP, JSTEP = PTHREADS / Q;
   const int nlat = a.nlat;
   const int p0 = blockIdx.x * NP, k = blockIdx.y, f = blockIdx.z;
   const int tid = threadIdx.x;
-  const double* plane =
-      k < a.ksplit ? a.gin[f] + (size_t)k * N * nlat : a.gin_hi[f] + (size_t)(k - a.ksplit) * N * nlat;
+  const GT* plane = in_plane<GT>(a, f, k, N);
   const ct::Geo<N, 1, true> g{NP, seq_stride(N), 1};
   float* smf = reinterpret_cast<float*>(sf);
   {
@@ -631,11 +639,11 @@ __global__ void __launch_bounds__(PTHREADS, 2) phi_fwd32(Phi32Args a) {
     constexpr int U = 8;
 #pragma unroll
     for (int u0 = 0; u0 < NJ; u0 += U) {
-      double v[U];
+      GT v[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         int j = j0 + (u0 + u) * JSTEP;
-        v[u] = (u0 + u < NJ && j < N) ? __ldg(plane + (size_t)j * nlat + ring) : 0.0;
+        v[u] = (u0 + u < NJ && j < N) ? __ldg(plane + (size_t)j * nlat + ring) : GT(0);
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
@@ -674,7 +682,7 @@ __global__ void __launch_bounds__(PTHREADS, 2) phi_fwd32(Phi32Args a) {
   }
 }
 
-template <int N, int NP>
+template <int N, int NP, typename GT>
 __global__ void __launch_bounds__(PTHREADS, 2) phi_inv32(Phi32Args a) {
   extern __shared__ float2 sf[];
   constexpr int Q = 2 * NP, JSTEP = PTHREADS / Q;
@@ -702,13 +710,13 @@ __global__ void __launch_bounds__(PTHREADS, 2) phi_inv32(Phi32Args a) {
   }
   __syncthreads();
   ct::dit<float2, N, N>(sf, g, a.twp, +1);
-  double* plane = a.gout[f] + (size_t)k * N * nlat;
+  GT* plane = static_cast<GT*>(a.gout[f]) + (size_t)k * N * nlat;
   const float* smf = reinterpret_cast<const float*>(sf);
   const int q = tid % Q, j0 = tid / Q;
   const int b = q < NP ? q : 2 * NP - 1 - q;
   const int ring = q < NP ? p0 + q : nlat - 1 - (p0 + b);
   const int half = q < NP ? 0 : 1;
-  for (int j = j0; j < N; j += JSTEP) plane[(size_t)j * nlat + ring] = (double)smf[2 * g.addr(b, j) + half];
+  for (int j = j0; j < N; j += JSTEP) plane[(size_t)j * nlat + ring] = (GT)smf[2 * g.addr(b, j) + half];
 }
 
 // ---------------------------------------------------------------- three-step phi FFTs
@@ -784,7 +792,7 @@ __host__ __device__ constexpr int phi3_box_rows() {
   return N <= 256 ? N : (N % 256 == 0 ? 256 : 192);
 }
 
-template <int N, int NP>
+template <int N, int NP, typename GT>
 __global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB)
     phi3_fwd32(Phi32Args a, int ntiles, const __grid_constant__ Phi3Maps maps) {
   using G = P3<N, NP>;
@@ -803,15 +811,16 @@ __global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB)
     tc05::mbar_fence_init();
   }
   __syncthreads();
-  auto stage = [&](int which) { return reinterpret_cast<double*>(sm3 + which * G::STAGE_F); };
+  // a stage holds an FP64 tile (float grids use the first half of it)
+  auto stage = [&](int which) { return reinterpret_cast<GT*>(sm3 + which * G::STAGE_F); };
   // one thread: the 2 N / BR boxes of a tile (its NP rings and their NP mirrors, all N samples)
   auto issue = [&](int tile, int which) {
     const int g = tile % ngroups, r = tile / ngroups, k = r % a.nz, f = r / a.nz;
     const bool lo = k < a.ksplit;
     const CUtensorMap* map = lo ? &maps.lo[f] : &maps.hi[f];
     const int y0 = (lo ? k : k - a.ksplit) * N;
-    double* st = stage(which);
-    mbar_arrive_tx(&full[which], (uint32_t)(2 * N * NP * sizeof(double)));
+    GT* st = stage(which);
+    mbar_arrive_tx(&full[which], (uint32_t)(2 * N * NP * sizeof(GT)));
 #pragma unroll 1
     for (int i = 0; i < N / BR; ++i) {
       tma_load_2d(st + (size_t)i * BR * NP, map, g * NP, y0 + i * BR, &full[which]);
@@ -836,8 +845,8 @@ __global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB)
       issue(tile + gridDim.x, s ^ 1);
     }
     const int g = tile % ngroups, r = tile / ngroups, k = r % a.nz, f = r / a.nz, p0 = g * NP;
-    const double* ring = stage(s);
-    const double* mir = ring + (size_t)N * NP;
+    const GT* ring = stage(s);
+    const GT* mir = ring + (size_t)N * NP;
     float2* X = reinterpret_cast<float2*>(stage(s));
     // (A) the samples x[nm + M n1] of ring pair bA (ring: real part, mirror: imaginary part)
     const bool act = t < G::ITEMS_A;
@@ -919,7 +928,7 @@ __global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB)
   }
 }
 
-template <int N, int NP>
+template <int N, int NP, typename GT>
 __global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB_INV) phi3_inv32(Phi32Args a, int ntiles) {
   using G = P3<N, NP>;
   constexpr int A = G::A, M = G::M, B = G::B, C = G::C, T = G::THREADS;
@@ -996,14 +1005,14 @@ __global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB_INV) phi3_
 #pragma unroll
       for (int ka = 0; ka < A; ++ka) v[ka] = ka ? ct::mul(xi[ka * G::PR], conj2(tw[nm * ka])) : xi[0];
       ct::RD<float2, A, 1>::run(v);
-      double* plane = a.gout[f] + (size_t)k * N * nlat;
-      double* pr = plane + p0 + b;
-      double* pm = plane + (nlat - 1 - p0 - b);
+      GT* plane = static_cast<GT*>(a.gout[f]) + (size_t)k * N * nlat;
+      GT* pr = plane + p0 + b;
+      GT* pm = plane + (nlat - 1 - p0 - b);
 #pragma unroll
       for (int n1 = 0; n1 < A; ++n1) {
         const size_t j = (size_t)(nm + M * n1) * nlat;
-        pr[j] = (double)v[n1].x;
-        pm[j] = (double)v[n1].y;
+        pr[j] = (GT)v[n1].x;
+        pm[j] = (GT)v[n1].y;
       }
     }
   }
@@ -1019,14 +1028,15 @@ __global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB_INV) phi3_
 // in shared memory ([b][ka][nm], pitches PR and SB), one contiguous image per
 // (plane, tile).  Pass 2 bulk-copies an image into shared memory (double
 // buffered) and finishes steps (B), (C), the fold and the tile rows.
-// The passes alternate over batches of PHI2_BATCH plane-fields, whose images
-// (77 MB at nphi 1536) stay in the 126 MB L2 between the passes: pass 1
-// streams the grid past L2 (loads marked evict-first) and pass 2 drops each
-// image's lines once it has read them (discard, no write-back), so the
-// images need not reach HBM at all.
-constexpr int PHI2_PB = 16, PHI2_NMC = 16, PHI2_NP = 8, PHI2_BATCH = 16;
+// The passes alternate over batches of PHI2_BATCH plane-fields; pass 1
+// streams the grid (loads marked evict-first: each value is read once).
+// Batches of 16 plane-fields, whose images (77 MB at nphi 1536) stay in L2
+// between the passes, were measured slower on the B200 (6.5 against 5.1 ms
+// per pair): four times the launches, and a pass 2 of 768 tiles on 296 CTAs
+// leaves 14% of its last wave idle.
+constexpr int PHI2_PB = 16, PHI2_NMC = 16, PHI2_NP = 8, PHI2_BATCH = 64;
 
-template <int N>
+template <int N, typename GT>
 __global__ void __launch_bounds__(PHI2_PB* PHI2_NMC, 2) phi2a_fwd32(Phi32Args a, float2* img, int q0) {
   using G = P3<N, PHI2_NP>;
   constexpr int A = G::A, M = G::M, PB = PHI2_PB, NMC = PHI2_NMC, SPB = A * NMC + 1;
@@ -1035,12 +1045,11 @@ __global__ void __launch_bounds__(PHI2_PB* PHI2_NMC, 2) phi2a_fwd32(Phi32Args a,
   const int t = threadIdx.x, b = t % PB, nmi = t / PB;
   const int nlat = a.nlat, pair = blockIdx.x * PB + b, nm0 = blockIdx.y * NMC, nm = nm0 + nmi;
   const int q = q0 + blockIdx.z, k = q % a.nz, f = q / a.nz;
-  const double* pl =
-      k < a.ksplit ? a.gin[f] + (size_t)k * N * nlat : a.gin_hi[f] + (size_t)(k - a.ksplit) * N * nlat;
+  const GT* pl = in_plane<GT>(a, f, k, N);
   float2 v[A];
 #pragma unroll
   for (int n1 = 0; n1 < A; ++n1) {
-    const double* row = pl + (size_t)(nm + M * n1) * nlat;
+    const GT* row = pl + (size_t)(nm + M * n1) * nlat;
     v[n1] = make_float2((float)__ldcs(row + pair), (float)__ldcs(row + (nlat - 1 - pair)));
   }
   ct::RD<float2, A, -1>::run(v);
@@ -1106,13 +1115,6 @@ __global__ void __launch_bounds__(PHI2_T, 2) phi2b_fwd32(Phi32Args a, const floa
       }
       return;
     }
-    {  // the image has landed and is not read again: drop its L2 lines without
-       // writing them back (the lines it shares with a neighbouring image stay)
-      const uintptr_t b0 = reinterpret_cast<uintptr_t>(img + ((size_t)ql * ngroups + g) * XF);
-      const uintptr_t lo = (b0 + 127) & ~(uintptr_t)127, hi = (b0 + G::XBYTES) & ~(uintptr_t)127;
-      for (uintptr_t o = lo + (uintptr_t)t * 128; o < hi; o += (uintptr_t)T * 128)
-        asm volatile("discard.global.L2 [%0], 128;\n" ::"l"(o) : "memory");
-    }
     if constexpr (B > 1) {  // (B)
       for (int it = t; it < G::ITEMS_B; it += T) {
         const int ka = it % A, rr = it / A, c = rr % C, b = rr / C;
@@ -1173,24 +1175,24 @@ __global__ void __launch_bounds__(PHI2_T, 2) phi2b_fwd32(Phi32Args a, const floa
 // the same operator the z transform applies to spectral planes
 // (fcgram_mod.f90 / pseudospec continuation step), here before the
 // analysis so that its round-off is not amplified.
-__global__ void cont_phys_kernel(const double* __restrict__ f0, const double* __restrict__ f1,
-                                 const double* __restrict__ f2, double* out, const double* __restrict__ dir, int C,
-                                 int d, int N, size_t npts) {
+template <typename GT>
+__global__ void cont_phys_kernel(const GT* __restrict__ f0, const GT* __restrict__ f1, const GT* __restrict__ f2,
+                                 GT* out, const double* __restrict__ dir, int C, int d, int N, size_t npts) {
   const int f = blockIdx.y;
-  const double* in = f == 0 ? f0 : (f == 1 ? f1 : f2);
-  double* o = out + (size_t)f * C * npts;
+  const GT* in = f == 0 ? f0 : (f == 1 ? f1 : f2);
+  GT* o = out + (size_t)f * C * npts;
   for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < npts; x += (size_t)gridDim.x * blockDim.x) {
     double hi[32], lo[32];
 #pragma unroll 8
     for (int jj = 0; jj < d; ++jj) {
-      hi[jj] = __ldg(in + (size_t)(N - d + jj) * npts + x);
-      lo[jj] = __ldg(in + (size_t)(d - 1 - jj) * npts + x);
+      hi[jj] = (double)__ldg(in + (size_t)(N - d + jj) * npts + x);
+      lo[jj] = (double)__ldg(in + (size_t)(d - 1 - jj) * npts + x);
     }
     for (int ii = 0; ii < C; ++ii) {
       double acc = 0.0;
       for (int jj = 0; jj < d; ++jj)
         acc = (acc + __ldg(dir + ii + C * jj) * hi[jj]) + __ldg(dir + (C - 1 - ii) + C * jj) * lo[jj];
-      o[(size_t)ii * npts + x] = acc;
+      o[(size_t)ii * npts + x] = (GT)acc;
     }
   }
 }
@@ -1199,16 +1201,16 @@ __global__ void cont_phys_kernel(const double* __restrict__ f0, const double* __
 // in shared memory (read as a broadcast), the 2 d input values of each point
 // in registers, two points per thread (each matrix entry read once for both);
 // every output is summed in the same order as above.
-template <int D>
-__global__ void __launch_bounds__(256) cont_phys_d(const double* __restrict__ f0, const double* __restrict__ f1,
-                                                   const double* __restrict__ f2, double* out,
+template <int D, typename GT>
+__global__ void __launch_bounds__(256) cont_phys_d(const GT* __restrict__ f0, const GT* __restrict__ f1,
+                                                   const GT* __restrict__ f2, GT* out,
                                                    const double* __restrict__ dir, int C, int N, size_t npts) {
   extern __shared__ double sdir[];  // dir(ii, jj) at ii + C jj
   for (int i = threadIdx.x; i < C * D; i += blockDim.x) sdir[i] = __ldg(dir + i);
   __syncthreads();
   const int f = blockIdx.y;
-  const double* in = f == 0 ? f0 : (f == 1 ? f1 : f2);
-  double* o = out + (size_t)f * C * npts;
+  const GT* in = f == 0 ? f0 : (f == 1 ? f1 : f2);
+  GT* o = out + (size_t)f * C * npts;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < npts; x += 2 * stride) {
     const size_t x2 = x + stride;
@@ -1216,10 +1218,10 @@ __global__ void __launch_bounds__(256) cont_phys_d(const double* __restrict__ f0
     double hi0[D], lo0[D], hi1[D], lo1[D];
 #pragma unroll
     for (int jj = 0; jj < D; ++jj) {
-      hi0[jj] = __ldg(in + (size_t)(N - D + jj) * npts + x);
-      lo0[jj] = __ldg(in + (size_t)(D - 1 - jj) * npts + x);
-      hi1[jj] = two ? __ldg(in + (size_t)(N - D + jj) * npts + x2) : 0.0;
-      lo1[jj] = two ? __ldg(in + (size_t)(D - 1 - jj) * npts + x2) : 0.0;
+      hi0[jj] = (double)__ldg(in + (size_t)(N - D + jj) * npts + x);
+      lo0[jj] = (double)__ldg(in + (size_t)(D - 1 - jj) * npts + x);
+      hi1[jj] = two ? (double)__ldg(in + (size_t)(N - D + jj) * npts + x2) : 0.0;
+      lo1[jj] = two ? (double)__ldg(in + (size_t)(D - 1 - jj) * npts + x2) : 0.0;
     }
     for (int ii = 0; ii < C; ++ii) {
       double a0 = 0.0, a1 = 0.0;
@@ -1229,8 +1231,8 @@ __global__ void __launch_bounds__(256) cont_phys_d(const double* __restrict__ f0
         a0 = (a0 + w1 * hi0[jj]) + w2 * lo0[jj];
         a1 = (a1 + w1 * hi1[jj]) + w2 * lo1[jj];
       }
-      o[(size_t)ii * npts + x] = a0;
-      if (two) o[(size_t)ii * npts + x2] = a1;
+      o[(size_t)ii * npts + x] = (GT)a0;
+      if (two) o[(size_t)ii * npts + x2] = (GT)a1;
     }
   }
 }
@@ -1648,47 +1650,50 @@ int run_phi4(K kernel, const Phi32Args& a, dim3 grid, int threads, size_t smem, 
   return SPH_OK;
 }
 
-template <int N, int NP, bool FWD>
+template <int N, int NP, bool FWD, typename GT>
 int phi4_np(const Phi32Args& a, dim3 grid, cudaStream_t st) {
   static_assert(FWD, "the four-step form is forward only");
   using C = P4<N, NP>;
-  return run_phi4(phi4_fwd32<N, NP>, a, grid, C::THREADS, C::SMEM_FWD, st);
+  return run_phi4(phi4_fwd32<N, NP, GT>, a, grid, C::THREADS, C::SMEM_FWD, st);
 }
 
-template <int N, bool FWD>
+template <int N, bool FWD, typename GT>
 int phi32_n(const Phi32Args& a, dim3 grid, size_t smem, cudaStream_t st) {
   // the four-step form for the forward transform; the inverse keeps the
   // shared-memory passes (more resident warps hide its grid stores better)
   if constexpr (FWD && N <= 1536) {
     if (a.tw1 && a.tw2) {
       switch (a.NP) {
-        case 8: return phi4_np<N, 8, FWD>(a, grid, st);
-        case 4: return phi4_np<N, 4, FWD>(a, grid, st);
-        case 2: return phi4_np<N, 2, FWD>(a, grid, st);
-        case 1: return phi4_np<N, 1, FWD>(a, grid, st);
+        case 8: return phi4_np<N, 8, FWD, GT>(a, grid, st);
+        case 4: return phi4_np<N, 4, FWD, GT>(a, grid, st);
+        case 2: return phi4_np<N, 2, FWD, GT>(a, grid, st);
+        case 1: return phi4_np<N, 1, FWD, GT>(a, grid, st);
       }
     }
   }
   switch (a.NP) {
     case 8:
-      if constexpr (8 * N <= PMAXC) return run_phi(FWD ? phi_fwd32<N, 8> : phi_inv32<N, 8>, a, grid, smem, st);
+      if constexpr (8 * N <= PMAXC)
+        return run_phi(FWD ? phi_fwd32<N, 8, GT> : phi_inv32<N, 8, GT>, a, grid, smem, st);
       break;
     case 4:
-      if constexpr (4 * N <= PMAXC) return run_phi(FWD ? phi_fwd32<N, 4> : phi_inv32<N, 4>, a, grid, smem, st);
+      if constexpr (4 * N <= PMAXC)
+        return run_phi(FWD ? phi_fwd32<N, 4, GT> : phi_inv32<N, 4, GT>, a, grid, smem, st);
       break;
     case 2:
-      if constexpr (2 * N <= PMAXC) return run_phi(FWD ? phi_fwd32<N, 2> : phi_inv32<N, 2>, a, grid, smem, st);
+      if constexpr (2 * N <= PMAXC)
+        return run_phi(FWD ? phi_fwd32<N, 2, GT> : phi_inv32<N, 2, GT>, a, grid, smem, st);
       break;
-    case 1: return run_phi(FWD ? phi_fwd32<N, 1> : phi_inv32<N, 1>, a, grid, smem, st);
+    case 1: return run_phi(FWD ? phi_fwd32<N, 1, GT> : phi_inv32<N, 1, GT>, a, grid, smem, st);
   }
   return SPH_EINVAL;
 }
 
-template <bool FWD>
+template <bool FWD, typename GT>
 int phi32_dispatch(const sph_plan* p, const Phi32Args& a, dim3 grid, size_t smem, cudaStream_t st) {
   switch (p->nphi) {
 #define CASE(n) \
-  case n: return phi32_n<n, FWD>(a, grid, smem, st);
+  case n: return phi32_n<n, FWD, GT>(a, grid, smem, st);
     PHI32_SIZES(CASE)
 #undef CASE
   }
@@ -1696,9 +1701,11 @@ int phi32_dispatch(const sph_plan* p, const Phi32Args& a, dim3 grid, size_t smem
 }
 
 constexpr int PHI3_UNSUPPORTED = 1000;
-// 2D fp64 view [rows][nlat] of a grid array, box NP x box_rows
-int phi3_map(CUtensorMap* map, const double* base, int nlat, int rows, int np, int box_rows) {
-  return tma::grid_map(map, base, nlat, rows, np, box_rows) ? SPH_OK : PHI3_UNSUPPORTED;
+// 2D view [rows][nlat] of a grid array (FP64 or float), box NP x box_rows;
+// unsupported where a box row is not a multiple of 16 bytes (float: NP < 4)
+template <typename GT>
+int phi3_map(CUtensorMap* map, const void* base, int nlat, int rows, int np, int box_rows) {
+  return tma::grid_map(map, static_cast<const GT*>(base), nlat, rows, np, box_rows) ? SPH_OK : PHI3_UNSUPPORTED;
 }
 
 // three-step kernels: which (N, NP) fit (one step-A item per thread, both
@@ -1710,7 +1717,7 @@ constexpr bool phi3_ok() {
          (size_t)2 * N * 2 * NP * sizeof(double) + (size_t)N * sizeof(float2) <= PHI3_SMEM_MAX;
 }
 
-template <int N, int NP, bool FWD>
+template <int N, int NP, bool FWD, typename GT>
 int phi3_run(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st) {
   if constexpr (!phi3_ok<N, NP>()) {
     return PHI3_UNSUPPORTED;
@@ -1726,15 +1733,15 @@ int phi3_run(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st
       Phi3Maps maps;
       if (!a.flag) return PHI3_UNSUPPORTED;
       for (int f = 0; f < nfields; ++f) {
-        const int rc = phi3_map(&maps.lo[f], a.gin[f], p->nlat, N * a.ksplit, NP, phi3_box_rows<N>());
+        const int rc = phi3_map<GT>(&maps.lo[f], a.gin[f], p->nlat, N * a.ksplit, NP, phi3_box_rows<N>());
         if (rc != SPH_OK) return rc;
         const bool hi = a.ksplit < p->nz;
-        const int rc2 = phi3_map(&maps.hi[f], hi ? a.gin_hi[f] : a.gin[f], p->nlat,
-                                 N * (hi ? p->nz - a.ksplit : a.ksplit), NP, phi3_box_rows<N>());
+        const int rc2 = phi3_map<GT>(&maps.hi[f], hi ? a.gin_hi[f] : a.gin[f], p->nlat,
+                                     N * (hi ? p->nz - a.ksplit : a.ksplit), NP, phi3_box_rows<N>());
         if (rc2 != SPH_OK) return rc2;
       }
       for (int f = nfields; f < SPH_MAX_FIELDS; ++f) maps.lo[f] = maps.hi[f] = maps.lo[0];
-      auto kern = phi3_fwd32<N, NP>;
+      auto kern = phi3_fwd32<N, NP, GT>;
       if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
           cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess ||
           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, G::THREADS, smem) != cudaSuccess)
@@ -1742,7 +1749,7 @@ int phi3_run(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st
       const int grid = (int)std::min<long long>(ntiles, (long long)std::max(1, occ) * std::max(1, p->nsm));
       kern<<<grid, G::THREADS, smem, st>>>(a, (int)ntiles, maps);
     } else {
-      auto kern = phi3_inv32<N, NP>;
+      auto kern = phi3_inv32<N, NP, GT>;
       if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
           cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess ||
           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, G::THREADS, smem) != cudaSuccess)
@@ -1765,7 +1772,7 @@ constexpr bool phi2_ok() {
   }
 }
 
-template <int N>
+template <int N, typename GT>
 int phi2_run(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st) {
   if constexpr (!phi2_ok<N>()) {
     return PHI3_UNSUPPORTED;
@@ -1783,7 +1790,8 @@ int phi2_run(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st
     const int nq = p->nz * nfields, ngroups = p->nlat2 / PHI2_NP;
     for (int q0 = 0; q0 < nq; q0 += p->phi2_planes) {
       const int nb = std::min(p->phi2_planes, nq - q0);
-      phi2a_fwd32<N><<<dim3(p->nlat2 / PHI2_PB, G::M / PHI2_NMC, nb), PHI2_PB * PHI2_NMC, 0, st>>>(a, p->phi2, q0);
+      phi2a_fwd32<N, GT><<<dim3(p->nlat2 / PHI2_PB, G::M / PHI2_NMC, nb), PHI2_PB * PHI2_NMC, 0, st>>>(a, p->phi2,
+                                                                                                      q0);
       SPH_LAUNCH_OK();
       const int ntiles = nb * ngroups;
       const int grid = std::min(ntiles, std::max(1, occ) * std::max(1, p->nsm));
@@ -1794,10 +1802,11 @@ int phi2_run(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st
   }
 }
 
+template <typename GT>
 int phi2_dispatch(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st) {
   switch (p->nphi) {
 #define CASE(n) \
-  case n: return phi2_run<n>(p, a, nfields, st);
+  case n: return phi2_run<n, GT>(p, a, nfields, st);
     PHI32_SIZES(CASE)
 #undef CASE
   }
@@ -1834,15 +1843,15 @@ int phi3_pairs(const sph_plan* p) {
   return 0;
 }
 
-template <bool FWD>
+template <bool FWD, typename GT>
 int phi3_dispatch(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st) {
   switch (p->nphi) {
 #define CASE(n)                                                  \
   case n:                                                        \
     switch (phi3_pairs<n>(p)) {                                  \
-      case 8: return phi3_run<n, 8, FWD>(p, a, nfields, st);     \
-      case 4: return phi3_run<n, 4, FWD>(p, a, nfields, st);     \
-      case 2: return phi3_run<n, 2, FWD>(p, a, nfields, st);     \
+      case 8: return phi3_run<n, 8, FWD, GT>(p, a, nfields, st); \
+      case 4: return phi3_run<n, 4, FWD, GT>(p, a, nfields, st); \
+      case 2: return phi3_run<n, 2, FWD, GT>(p, a, nfields, st); \
     }                                                            \
     return PHI3_UNSUPPORTED;
     PHI32_SIZES(CASE)
@@ -1875,31 +1884,36 @@ Phi32Args phi32_args(const sph_plan* p) {
 
 }  // namespace
 
-int launch_cont_phys(const sph_plan* p, const double* const* grids, int nfields, cudaStream_t st) {
-  if (!p->contg || p->C <= 0 || p->d > 32 || nfields < 1 || nfields > SPH_MAX_FIELDS) return SPH_EINVAL;
+namespace {
+
+template <typename GT>
+int cont_phys_t(const sph_plan* p, const void* const* grids, int nfields, cudaStream_t st) {
   const size_t npts = (size_t)p->nphi * p->nlat;
-  const double* f[SPH_MAX_FIELDS] = {grids[0], nfields > 1 ? grids[1] : grids[0], nfields > 2 ? grids[2] : grids[0]};
+  const GT* f[SPH_MAX_FIELDS];
+  for (int i = 0; i < SPH_MAX_FIELDS; ++i) f[i] = static_cast<const GT*>(grids[i < nfields ? i : 0]);
+  GT* out = reinterpret_cast<GT*>(p->contg);  // float planes use the first half of the FP64 buffer
   TimedLaunch tl(p, T_OPS, st);
   const int blocks = (int)std::min<size_t>((npts + 255) / 256, 148 * 8);
   const size_t smem = (size_t)p->C * p->d * sizeof(double);
   switch (p->d) {
-#define CASE(D)                                                                                                  \
-  case D:                                                                                                        \
-    cont_phys_d<D><<<dim3(blocks, nfields), 256, smem, st>>>(f[0], f[1], f[2], p->contg, p->d_dir, p->C, p->N, \
-                                                              npts);                                             \
+#define CASE(D)                                                                                               \
+  case D:                                                                                                     \
+    cont_phys_d<D, GT><<<dim3(blocks, nfields), 256, smem, st>>>(f[0], f[1], f[2], out, p->d_dir, p->C, p->N, \
+                                                                  npts);                                     \
     break;
     CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
 #undef CASE
     default:
-      cont_phys_kernel<<<dim3(blocks, nfields), 256, 0, st>>>(f[0], f[1], f[2], p->contg, p->d_dir, p->C, p->d,
-                                                            p->N, npts);
+      cont_phys_kernel<GT><<<dim3(blocks, nfields), 256, 0, st>>>(f[0], f[1], f[2], out, p->d_dir, p->C, p->d,
+                                                                  p->N, npts);
   }
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
 
-int launch_phi_fwd32(const sph_plan* p, const double* const* grids, int nfields, cudaStream_t st,
-                     const double* const* grids_hi) {
+template <typename GT>
+int phi_fwd32_t(const sph_plan* p, const void* const* grids, int nfields, cudaStream_t st,
+                const void* const* grids_hi) {
   Phi32Args a = phi32_args(p);
   for (int f = 0; f < nfields; ++f) a.gin[f] = grids[f];
   a.ksplit = p->nz;
@@ -1908,32 +1922,73 @@ int launch_phi_fwd32(const sph_plan* p, const double* const* grids, int nfields,
     for (int f = 0; f < nfields; ++f) a.gin_hi[f] = grids_hi[f];
   }
   TimedLaunch tl(p, T_PHI_FWD, st);
-  bool aligned = p->nlat % 2 == 0;
+  bool aligned = (p->nlat * sizeof(GT)) % 16 == 0;
   for (int f = 0; f < nfields; ++f)
     aligned = aligned && reinterpret_cast<uintptr_t>(a.gin[f]) % 16 == 0 &&
               (!grids_hi || reinterpret_cast<uintptr_t>(a.gin_hi[f]) % 16 == 0);
   {
-    const int rc = phi2_dispatch(p, a, nfields, st);
+    const int rc = phi2_dispatch<GT>(p, a, nfields, st);
     if (rc != PHI3_UNSUPPORTED) return rc;
   }
   if (aligned) {
-    const int rc = phi3_dispatch<true>(p, a, nfields, st);
+    const int rc = phi3_dispatch<true, GT>(p, a, nfields, st);
     if (rc != PHI3_UNSUPPORTED) return rc;
   }
   dim3 grid(p->nlat2 / a.NP, p->nz, nfields);
   const size_t smem = (size_t)a.NP * seq_stride(p->nphi) * sizeof(float2);
-  return phi32_dispatch<true>(p, a, grid, smem, st);
+  return phi32_dispatch<true, GT>(p, a, grid, smem, st);
 }
 
-int launch_phi_inv32(const sph_plan* p, double* const* grids, int nfields, cudaStream_t st) {
+template <typename GT>
+int phi_inv32_t(const sph_plan* p, void* const* grids, int nfields, cudaStream_t st) {
   Phi32Args a = phi32_args(p);
   for (int f = 0; f < nfields; ++f) a.gout[f] = grids[f];
   TimedLaunch tl(p, T_PHI_INV, st);
-  const int rc = phi3_dispatch<false>(p, a, nfields, st);
+  const int rc = phi3_dispatch<false, GT>(p, a, nfields, st);
   if (rc != PHI3_UNSUPPORTED) return rc;
   dim3 grid(p->nlat2 / a.NP, p->nz, nfields);
   const size_t smem = (size_t)a.NP * seq_stride(p->nphi) * sizeof(float2);
-  return phi32_dispatch<false>(p, a, grid, smem, st);
+  return phi32_dispatch<false, GT>(p, a, grid, smem, st);
+}
+
+}  // namespace
+
+int launch_cont_phys_g(const sph_plan* p, const void* const* grids, int nfields, cudaStream_t st, bool f32) {
+  if (!p->contg || p->C <= 0 || p->d > 32 || nfields < 1 || nfields > SPH_MAX_FIELDS) return SPH_EINVAL;
+  return f32 ? cont_phys_t<float>(p, grids, nfields, st) : cont_phys_t<double>(p, grids, nfields, st);
+}
+
+int launch_phi_fwd32_g(const sph_plan* p, const void* const* grids, int nfields, cudaStream_t st,
+                       const void* const* grids_hi, bool f32) {
+  return f32 ? phi_fwd32_t<float>(p, grids, nfields, st, grids_hi)
+             : phi_fwd32_t<double>(p, grids, nfields, st, grids_hi);
+}
+
+int launch_phi_inv32_g(const sph_plan* p, void* const* grids, int nfields, cudaStream_t st, bool f32) {
+  return f32 ? phi_inv32_t<float>(p, grids, nfields, st) : phi_inv32_t<double>(p, grids, nfields, st);
+}
+
+int launch_cont_phys(const sph_plan* p, const double* const* grids, int nfields, cudaStream_t st) {
+  const void* g[SPH_MAX_FIELDS] = {};
+  for (int f = 0; f < nfields && f < SPH_MAX_FIELDS; ++f) g[f] = grids[f];
+  return launch_cont_phys_g(p, g, nfields, st, false);
+}
+
+int launch_phi_fwd32(const sph_plan* p, const double* const* grids, int nfields, cudaStream_t st,
+                     const double* const* grids_hi) {
+  const void* g[SPH_MAX_FIELDS] = {};
+  const void* gh[SPH_MAX_FIELDS] = {};
+  for (int f = 0; f < nfields && f < SPH_MAX_FIELDS; ++f) {
+    g[f] = grids[f];
+    if (grids_hi) gh[f] = grids_hi[f];
+  }
+  return launch_phi_fwd32_g(p, g, nfields, st, grids_hi ? gh : nullptr, false);
+}
+
+int launch_phi_inv32(const sph_plan* p, double* const* grids, int nfields, cudaStream_t st) {
+  void* g[SPH_MAX_FIELDS] = {};
+  for (int f = 0; f < nfields && f < SPH_MAX_FIELDS; ++f) g[f] = grids[f];
+  return launch_phi_inv32_g(p, g, nfields, st, false);
 }
 
 int launch_tc_analysis(const sph_plan* p, int vector, double2* out, double2* out2, cudaStream_t st) {

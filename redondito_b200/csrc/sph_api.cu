@@ -196,6 +196,8 @@ static void plan_free(sph_plan* p) {
     if (q) cudaFree(q);
   for (auto& q : p->gr)
     if (q) cudaFree(q);
+  for (auto& q : p->fsp)
+    if (q) cudaFree(q);
   if (!p->tables) {
     mixed_free_tables(p);
     for (void* q : table_ptrs(p))
@@ -443,6 +445,7 @@ extern "C" int sph_plan_clone(const sph_plan* src, sph_plan** out) {
   p->G = nullptr;
   for (auto& q : p->sp) q = nullptr;
   for (auto& q : p->gr) q = nullptr;
+  for (auto& q : p->fsp) q = nullptr;
   p->nsp = p->ngr = 0;
   p->energy = p->spectrum = nullptr;
   p->dflag = nullptr;

@@ -123,6 +123,8 @@ struct sph_plan {
   // grid scratch for the NL step (nz*nphi*nlat doubles each)
   double* gr[9] = {nullptr};
   int ngr = 0;
+  // FP64 spectral scratch of the single-precision entry points (allocated on first use)
+  double2* fsp[3] = {nullptr};
   // boundary: kinds at the inner and outer wall (0 noslip, 1 freeslip); the
   // plan owns binv/d2bor when its kinds differ from the shared tables'
   int bck[2] = {0, 0};
@@ -274,6 +276,11 @@ int launch_phi_fwd32(const sph_plan* p, const double* const* grids, int nfields,
 // FC-Gram continuation of physical fields: planes N..nz-1 of each field into
 // p->contg (field f at f * Cz planes), from its planes 0..oz-1 and N-oz..N-1
 int launch_cont_phys(const sph_plan* p, const double* const* grids, int nfields, cudaStream_t st);
+// the same on grids of float (f32) or FP64 values (the single-precision entry points)
+int launch_cont_phys_g(const sph_plan* p, const void* const* grids, int nfields, cudaStream_t st, bool f32);
+int launch_phi_fwd32_g(const sph_plan* p, const void* const* grids, int nfields, cudaStream_t st,
+                       const void* const* grids_hi, bool f32);
+int launch_phi_inv32_g(const sph_plan* p, void* const* grids, int nfields, cudaStream_t st, bool f32);
 int launch_phi_inv32(const sph_plan* p, double* const* grids, int nfields, cudaStream_t st);
 int launch_tc_analysis(const sph_plan* p, int vector, double2* out, double2* out2, cudaStream_t st);
 int launch_tc_synthesis(const sph_plan* p, int vector, const double2* in, const double2* in2,

@@ -18,9 +18,11 @@ the state (Z, W, phi).  The server keeps the bytes of its slots within
 
 Admission.  Requests are admitted as they arrive.  A waiting request takes a
 free slot of its (size, kind); without one, a new slot is created if it fits
-the budget; otherwise idle slots of other (size, kind) are released, least
-recently used first, until it fits.  A request that still does not fit
-waits until running slots finish.  The work of an
+the budget.  Otherwise a (size, kind) that already has a slot waits for it,
+and one that has none releases idle slots of other (size, kind) until it
+fits: clones first, least recently used first, the last slot of a size
+(which holds its tables) only after them.  A request that still does not
+fit waits until running slots finish.  The work of an
 admitted request is queued at once on its slot's stream, so requests of all
 sizes run side by side on the device; the host loop never blocks on the
 device, it polls completion events.
@@ -211,7 +213,13 @@ class Server:
         if self.max_slots.get(key) is not None and len(self.slots[key]) >= self.max_slots[key]:
             return None
         source = self._source(lmax)
-        if not self._release_idle(self._need(lmax, kind, source is None), key):
+        need = self._need(lmax, kind, source is None)
+        if self.bytes + need > self.budget and self.slots[key]:
+            # a (size, kind) that has a slot waits for it instead of pushing
+            # other sizes out: every release frees device memory (a device-wide
+            # synchronisation) and the next request of that size allocates again
+            return None
+        if not self._release_idle(need, key):
             return None
         if source is not None and self._source(lmax) is None:
             # releasing took the last plan of this size: the new slot builds the tables

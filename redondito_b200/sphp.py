@@ -51,6 +51,12 @@ SYMBOLS = (
     "sph_read_namelist", "sph_write_grids", "sph_energy_spectrum", "sph_run", "sph_plan_clone",
     "sph_fcgram_load_neumann_tables", "sph_plan_set_neumann", "sph_neumann_reconstruct",
     "sph_robin_reconstruct",
+    "sph_fftp2d_real_to_complex_xy_f32", "sph_fftp2d_complex_to_real_xy_f32",
+    "sph_fftp1d_real_to_complex_z_f32", "sph_fftp1d_complex_to_real_z_f32",
+    "sph_fftp3d_real_to_complex_f32", "sph_fftp3d_complex_to_real_f32",
+    "sph_fftp2d_vec_to_qst_f32", "sph_fftp2d_qst_to_vec_f32",
+    "sph_fftp3d_vec_to_qst_f32", "sph_fftp3d_qst_to_vec_f32",
+    "sph_derivr_f32", "sph_dlr_f32", "sph_fc_filter_f32",
 )
 TIMER_CLASSES = ("phi_fwd", "phi_inv", "leg_analysis", "leg_synthesis", "vec_analysis",
                  "vec_synthesis", "zfft", "ops")
@@ -131,6 +137,19 @@ def lib(build_if_missing=True):
             "sph_plan_set_neumann": [P, pD, pD],
             "sph_neumann_reconstruct": [P, Vp, I, I, Vp],
             "sph_robin_reconstruct": [P, Vp, I, Vp, Vp],
+            "sph_fftp2d_real_to_complex_xy_f32": [P, Vp, Vp, Vp],
+            "sph_fftp2d_complex_to_real_xy_f32": [P, Vp, Vp, Vp],
+            "sph_fftp1d_real_to_complex_z_f32": [P, Vp, Vp],
+            "sph_fftp1d_complex_to_real_z_f32": [P, Vp, Vp],
+            "sph_fftp3d_real_to_complex_f32": [P, Vp, Vp, Vp],
+            "sph_fftp3d_complex_to_real_f32": [P, Vp, Vp, Vp],
+            "sph_fftp2d_vec_to_qst_f32": [P] + [Vp] * 6 + [Vp],
+            "sph_fftp2d_qst_to_vec_f32": [P] + [Vp] * 6 + [Vp],
+            "sph_fftp3d_vec_to_qst_f32": [P] + [Vp] * 6 + [Vp],
+            "sph_fftp3d_qst_to_vec_f32": [P] + [Vp] * 6 + [Vp],
+            "sph_derivr_f32": [P, Vp, Vp, I, ctypes.c_char, Vp],
+            "sph_dlr_f32": [P, Vp, Vp, Vp],
+            "sph_fc_filter_f32": [P, Vp, ctypes.c_char, Vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -254,6 +273,14 @@ class Plan:
     def new_spec(self):
         return torch.zeros((self.nz, self.nlmv), dtype=torch.complex128, device=self.device)
 
+    def new_grid32(self):
+        """a float grid for the single-precision entry points (whole field)"""
+        return torch.zeros((self.nz, self.nphi, self.nlat), dtype=torch.float32, device=self.device)
+
+    def new_spec32(self):
+        """float complex spectra for the single-precision entry points (whole field)"""
+        return torch.zeros((self.nz, self.nlm), dtype=torch.complex64, device=self.device)
+
     def new_plane_spec(self):
         """per-plane spectra of the caller's planes, (nplanes, nlm)"""
         return torch.zeros((self.nzv, self.nlm), dtype=torch.complex128, device=self.device)
@@ -284,6 +311,16 @@ def _s(plan, t):
 def _sp(plan, t):
     """per-plane spectra of the caller's planes (the 2D transforms): (nplanes, nlm)"""
     return _ptr(t, (plan.nzv, plan.nlm), torch.complex128)
+
+
+def _g32(plan, t):
+    """float grid of the whole field (single-precision entry points)"""
+    return _ptr(t, (plan.nz, plan.nphi, plan.nlat), torch.float32)
+
+
+def _s32(plan, t):
+    """float complex spectra of the whole field (single-precision entry points)"""
+    return _ptr(t, (plan.nz, plan.nlm), torch.complex64)
 
 
 def set_slab(plan, k0, nplanes, lm0, nlm_local):
@@ -442,6 +479,67 @@ def v_imposebc(plan, tor, phi, pol, stream=None):
 
 def v_imposebc_fast(plan, tor, phi, pol, stream=None):
     _call("sph_v_imposebc_fast", plan.h, _s(plan, tor), _s(plan, phi), _s(plan, pol), _stream(stream))
+
+
+# ---------------------------------------------------------------- single precision
+# The arrays of a GSINGLE_PRECISION build of the reference
+# (src/sphp/fprecision_mod.F90:13-18): float grids and complex64 spectra on
+# an SPH_MIXED plan over whole fields; the inverse transforms preserve their
+# input.
+def fftp2d_real_to_complex_xy_f32(plan, in_, out, stream=None):
+    _call("sph_fftp2d_real_to_complex_xy_f32", plan.h, _g32(plan, in_), _s32(plan, out), _stream(stream))
+
+
+def fftp2d_complex_to_real_xy_f32(plan, in_, out, stream=None):
+    _call("sph_fftp2d_complex_to_real_xy_f32", plan.h, _s32(plan, in_), _g32(plan, out), _stream(stream))
+
+
+def fftp1d_real_to_complex_z_f32(plan, inout, stream=None):
+    _call("sph_fftp1d_real_to_complex_z_f32", plan.h, _s32(plan, inout), _stream(stream))
+
+
+def fftp1d_complex_to_real_z_f32(plan, inout, stream=None):
+    _call("sph_fftp1d_complex_to_real_z_f32", plan.h, _s32(plan, inout), _stream(stream))
+
+
+def fftp3d_real_to_complex_f32(plan, in_, out, stream=None):
+    _call("sph_fftp3d_real_to_complex_f32", plan.h, _g32(plan, in_), _s32(plan, out), _stream(stream))
+
+
+def fftp3d_complex_to_real_f32(plan, in_, out, stream=None):
+    _call("sph_fftp3d_complex_to_real_f32", plan.h, _s32(plan, in_), _g32(plan, out), _stream(stream))
+
+
+def fftp2d_vec_to_qst_f32(plan, vr, vt, vp, q, s, t, stream=None):
+    _call("sph_fftp2d_vec_to_qst_f32", plan.h, _g32(plan, vr), _g32(plan, vt), _g32(plan, vp),
+          _s32(plan, q), _s32(plan, s), _s32(plan, t), _stream(stream))
+
+
+def fftp2d_qst_to_vec_f32(plan, q, s, t, vr, vt, vp, stream=None):
+    _call("sph_fftp2d_qst_to_vec_f32", plan.h, _s32(plan, q), _s32(plan, s), _s32(plan, t),
+          _g32(plan, vr), _g32(plan, vt), _g32(plan, vp), _stream(stream))
+
+
+def fftp3d_vec_to_qst_f32(plan, vr, vt, vp, q, s, t, stream=None):
+    _call("sph_fftp3d_vec_to_qst_f32", plan.h, _g32(plan, vr), _g32(plan, vt), _g32(plan, vp),
+          _s32(plan, q), _s32(plan, s), _s32(plan, t), _stream(stream))
+
+
+def fftp3d_qst_to_vec_f32(plan, q, s, t, vr, vt, vp, stream=None):
+    _call("sph_fftp3d_qst_to_vec_f32", plan.h, _s32(plan, q), _s32(plan, s), _s32(plan, t),
+          _g32(plan, vr), _g32(plan, vt), _g32(plan, vp), _stream(stream))
+
+
+def derivr_f32(plan, a, b, order, esp="r", stream=None):
+    _call("sph_derivr_f32", plan.h, _s32(plan, a), _s32(plan, b), int(order), esp.encode(), _stream(stream))
+
+
+def dlr_f32(plan, a, b, stream=None):
+    _call("sph_dlr_f32", plan.h, _s32(plan, a), _s32(plan, b), _stream(stream))
+
+
+def fc_filter_f32(plan, a, esp="r", stream=None):
+    _call("sph_fc_filter_f32", plan.h, _s32(plan, a), esp.encode(), _stream(stream))
 
 
 # ---------------------------------------------------------------- NL + RK3

@@ -91,4 +91,6 @@ def test_rk3_run_does_not_compound():
                    torch.linalg.vector_norm(out["fp64"][j][i])) for j in range(2)]
         print(f"RK3 mixed vs FP64, {name}: after 10 steps {d[0]:.3e}, after 20 steps {d[1]:.3e}")
         check(d[1], 3e-7, f"20 RK3 steps, mixed vs FP64, {name}")
-        check(d[1] / max(d[0], 1e-30), 2.5, f"growth from 10 to 20 steps, {name}")
+        # at most linear growth (with an absolute allowance for differences
+        # that start near zero, as phi's does after the first imposebc)
+        check(d[1] - 2.5 * d[0], 2e-8, f"growth from 10 to 20 steps, {name}")

@@ -3,7 +3,7 @@ test_gpu_mixed.py do not reach, against the CPU oracle at the mixed form's
 tolerance:
 
 * the two-pass forward transform (nphi 1536) over more plane-fields than
-  one batch of its scratch holds (16), so several batches run;
+  one batch of its scratch holds (64), so a second batch runs;
 * an odd number of ring pairs (nlat/2 odd): tiles of 2, 4 or 8 ring pairs
   do not divide it, so both directions take the one-ring-pair kernels;
 * a grid that is 8-byte but not 16-byte aligned (a view into a larger
