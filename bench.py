@@ -415,12 +415,18 @@ def serving_c5(S, torch, nreq=200, rate=500.0, rank=0, world=1, dist=None, budge
         warm = [serve.Request(i, 0.0, l, k, 1) for i, (l, k) in enumerate((l, k) for l in sizes
                                                                          for k in ("pair", "rk3"))]
         srv.serve(warm)
+        # a slot pool sized for the mix (more slots for the frequent small
+        # sizes), created before the traffic within the budget
+        srv.reserve({(l, k): n for l, n in ((31, 4), (63, 4), (127, 2), (255, 2), (511, 1))
+                     for k in ("pair", "rk3")})
+        created0 = srv.created
         sat = run(srv, serve.poisson_mix(nreq, rate, seed=20261203 + 5))
         half = 0.5 * sat["jobs_per_s"]
         below = run(srv, serve.poisson_mix(nreq, half, seed=20261203 + 6))
         out[name] = {"offered_500_per_s": dict(sat, offered_per_s=rate),
                      "offered_half_capacity": dict(below, offered_per_s=half),
-                     "slots_created": srv.created, "slots_released": srv.released,
+                     "slots_reserved": created0, "slots_created": srv.created - created0,
+                     "slots_released": srv.released,
                      "peak_hbm_gb": srv.peak_bytes / 1e9}
         srv.close()
         torch.cuda.empty_cache()

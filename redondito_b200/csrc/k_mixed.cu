@@ -1029,7 +1029,7 @@ __global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB_INV) phi3_
 // (plane, tile).  Pass 2 bulk-copies an image into shared memory (double
 // buffered) and finishes steps (B), (C), the fold and the tile rows.
 // The passes alternate over batches of PHI2_BATCH plane-fields; pass 1
-// streams the grid (loads marked evict-first: each value is read once).
+// reads whole grid rows.
 // Batches of 16 plane-fields, whose images (77 MB at nphi 1536) stay in L2
 // between the passes, were measured slower on the B200 (6.5 against 5.1 ms
 // per pair): four times the launches, and a pass 2 of 768 tiles on 296 CTAs
@@ -1050,7 +1050,7 @@ __global__ void __launch_bounds__(PHI2_PB* PHI2_NMC, 2) phi2a_fwd32(Phi32Args a,
 #pragma unroll
   for (int n1 = 0; n1 < A; ++n1) {
     const GT* row = pl + (size_t)(nm + M * n1) * nlat;
-    v[n1] = make_float2((float)__ldcs(row + pair), (float)__ldcs(row + (nlat - 1 - pair)));
+    v[n1] = make_float2((float)__ldg(row + pair), (float)__ldg(row + (nlat - 1 - pair)));
   }
   ct::RD<float2, A, -1>::run(v);
 #pragma unroll

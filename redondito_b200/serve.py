@@ -77,7 +77,9 @@ class Slot:
 
     def __init__(self, S, torch, lmax, kind, precision, source=None):
         self.S, self.torch, self.lmax, self.kind = S, torch, lmax, kind
-        torch.cuda.synchronize()
+        # cudaMalloc returns once the memory is reserved, so the free-memory
+        # delta needs no device synchronisation (which would stall the
+        # requests running on the other slots' streams)
         free0 = torch.cuda.mem_get_info()[0]
         if source is not None:
             self.plan = source.clone()
@@ -88,7 +90,6 @@ class Slot:
         P = self.plan
         if kind == "rk3":
             S.setup_bc(P)
-        torch.cuda.synchronize()
         plan_bytes = max(0, free0 - torch.cuda.mem_get_info()[0])  # the plan's own cudaMalloc'd memory
         if kind == "rk3":
             self.Z, self.W, self.F = P.new_spec(), P.new_spec(), P.new_spec()
@@ -240,6 +241,23 @@ class Server:
             s = self._free_slot(lmax, kind, 0.0)
             if s is not None:
                 s.last_used = 0.0
+
+    def reserve(self, counts):
+        """Create slots ahead of the traffic: up to counts[(lmax, kind)] of
+        each, in the order given, while they fit the budget without
+        releasing any (later requests still create and release slots on
+        demand).  Creating a slot allocates device memory, which a serving
+        loop would otherwise do between requests."""
+        for key, n in counts.items():
+            need = lambda: self._need(key[0], key[1], self._source(key[0]) is None)
+            while len(self.slots[key]) < n and self.bytes + need() <= self.budget:
+                source = self._source(key[0])
+                s = Slot(self.S, self.torch, key[0], key[1], self.precision, source)
+                self.measured[(key[0], key[1], s.fresh)] = s.bytes
+                self.bytes += s.bytes
+                self.peak_bytes = max(self.peak_bytes, self.bytes)
+                self.slots[key].append(s)
+                self.created += 1
 
     def close(self):
         for ss in self.slots.values():

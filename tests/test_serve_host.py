@@ -153,3 +153,13 @@ def test_release_keeps_the_last_slot_of_a_size(fake_server):
     srv.budget = 0.5 * clone
     assert not srv._release_idle(clone, keep=(127, "pair"))
     assert sum(len(v) for v in srv.slots.values()) == 0
+
+
+def test_reserve_fills_the_pool_within_the_budget(fake_server):
+    srv = fake_server(3 * _fresh(63, "pair") + _fresh(31, "pair"))
+    srv.reserve({(31, "pair"): 2, (63, "pair"): 9})
+    assert len(srv.slots[(31, "pair")]) == 2
+    assert 1 <= len(srv.slots[(63, "pair")]) < 9
+    assert srv.bytes <= srv.budget and srv.released == 0
+    fresh = [s.fresh for s in srv.slots[(63, "pair")]]
+    assert fresh[0] and not any(fresh[1:])  # one plan with tables, the rest clones
