@@ -448,10 +448,7 @@ int phi3d_dispatch_n(const sph_plan* p, const PhiArgs& a, int nfields, cudaStrea
 // 2 (mod 8) 16-byte slots.
 template <int N, int CL>
 struct P3c {
-  // ring pairs per CTA and per cluster tile (16 for clusters of 4 and 8);
-  // clusters of 8 CTAs of 2 ring pairs each run two CTAs per SM, so that one
-  // CTA's loads and barriers overlap the other's transform
-  static constexpr int NPL = CL == 8 ? 2 : 4, NPC = NPL * CL;
+  static constexpr int NPL = 4, NPC = NPL * CL;  // ring pairs per CTA, per cluster tile
   static constexpr int A = 16, M = N / A, B = ct::pow2_part_cap16(M), C = M / B;
   static constexpr int ROWS = N / CL;                          // phi rows staged by one CTA
   static constexpr int BR = largest_divisor_le(ROWS, 256);     // rows per TMA box
@@ -464,9 +461,7 @@ struct P3c {
   static constexpr size_t XBYTES = (size_t)NPL * SB * sizeof(double2);
   static constexpr size_t TILE_BYTES = (size_t)2 * ROWS * ROWB;  // rings and mirrors
   static constexpr size_t STAGE = round_up(XBYTES > TILE_BYTES ? XBYTES : TILE_BYTES, 1024);
-  static constexpr int MINB = CL == 8 ? 2 : 1;                 // CTAs per SM
-  static constexpr bool TW_SMEM = MINB == 1;  // twiddles in shared memory (else read through L1)
-  static constexpr size_t SMEM = 2 * STAGE + (TW_SMEM ? (size_t)N * sizeof(double2) : 0) + 64;
+  static constexpr size_t SMEM = 2 * STAGE + (size_t)N * sizeof(double2) + 64;
   // byte offset of staged element (row, column) within one half of a stage
   static __device__ __forceinline__ uint32_t off(int row, int col) {
     const uint32_t o = (uint32_t)(row * ROWB + col * 8);
@@ -476,14 +471,13 @@ struct P3c {
 
 template <int N, int CL>
 constexpr bool phi3c_ok() {
-  if constexpr (N % 16 != 0 || N < 48 || (CL != 2 && CL != 4 && CL != 8) || N % CL != 0) {
+  if constexpr (N % 16 != 0 || N < 48 || (CL != 2 && CL != 4)) {
     return false;
   } else {
     using G = P3c<N, CL>;
-    // every TMA box and both halves of a stage start on a 1024-byte boundary
-    // (swizzle atoms); MINB CTAs fit an SM's shared memory
+    // every TMA box and both halves of a stage start on a 1024-byte boundary (swizzle atoms)
     return G::THREADS <= 1024 && ((size_t)G::ROWS * G::ROWB) % 1024 == 0 && (G::BR * G::ROWB) % 1024 == 0 &&
-           G::SMEM * G::MINB <= (size_t)(G::MINB == 1 ? 227 : 226) * 1024;
+           G::SMEM <= 227 * 1024;
   }
 }
 
@@ -492,24 +486,21 @@ struct GridMaps {
 };
 
 template <int N, int CL>
-__global__ void __launch_bounds__(P3c<N, CL>::THREADS, P3c<N, CL>::MINB)
+__global__ void __launch_bounds__(P3c<N, CL>::THREADS, 1)
     phi3c_fwd64(PhiArgs a, int ntiles, const __grid_constant__ GridMaps maps) {
   using G = P3c<N, CL>;
   constexpr int A = G::A, M = G::M, B = G::B, C = G::C, T = G::THREADS, NPL = G::NPL, NPC = G::NPC;
   constexpr int ROWS = G::ROWS, BR = G::BR;
   extern __shared__ __align__(1024) unsigned char sm3c[];
-  constexpr size_t TWB = G::TW_SMEM ? (size_t)N * sizeof(double2) : 0;
   double2* tws = reinterpret_cast<double2*>(sm3c + 2 * G::STAGE);
-  uint64_t* full = reinterpret_cast<uint64_t*>(sm3c + 2 * G::STAGE + TWB);
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm3c + 2 * G::STAGE + (size_t)N * sizeof(double2));
   int* bad = reinterpret_cast<int*>(full + 2);  // this CTA's last wait gave up (read by the cluster)
   const int t = threadIdx.x, warp = t / 32;
   const uint32_t rank = cluster_rank();
   const int cid = blockIdx.x / CL, ncl = gridDim.x / CL;
   const int nlat = a.nlat, ngroups = nlat / 2 / NPC;
-  if constexpr (G::TW_SMEM)
-    for (int i = t; i < N; i += T) tws[i] = __ldg(a.fd.tw + i);
-  // W_N^e, from shared memory or through L1
-  auto tw = [&](int e) { return G::TW_SMEM ? tws[e] : __ldg(a.fd.tw + e); };
+  for (int i = t; i < N; i += T) tws[i] = __ldg(a.fd.tw + i);
+  auto tw = [&](int e) { return tws[e]; };  // W_N^e
   if (t == 0) {
     tc05::mbar_init(&full[0], 1);
     tc05::mbar_init(&full[1], 1);
@@ -701,8 +692,7 @@ template <int N>
 int phi3c_dispatch_n(const sph_plan* p, const PhiArgs& a, int nfields, cudaStream_t st) {
   if (p->tile_np) return PHI3C_UNSUPPORTED;  // tuned ring pairs: the kernels they were tuned on
   if (p->nlat2 % 16 == 0) {
-    int rc = phi3c_run<N, 8>(p, a, nfields, st);
-    if (rc == PHI3C_UNSUPPORTED) rc = phi3c_run<N, 4>(p, a, nfields, st);
+    const int rc = phi3c_run<N, 4>(p, a, nfields, st);
     if (rc != PHI3C_UNSUPPORTED) return rc;
   }
   if (p->nlat2 % 8 == 0) return phi3c_run<N, 2>(p, a, nfields, st);
