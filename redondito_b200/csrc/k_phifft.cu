@@ -441,8 +441,9 @@ int phi3d_dispatch_n(const sph_plan* p, const PhiArgs& a, int nfields, cudaStrea
 // coefficients G[m][parity][k][node] like phi_fwd_ct.  Only warp 0, which
 // stores nothing to global memory, arrives at barrier (1) with release
 // semantics, and every warp arrives at (2) relaxed once its step-(A) loads
-// have returned: the folding warps' stores are not drained at the barriers.  The staged rows are
-// swizzled by the TMA (16-byte chunk index XOR 128-byte row index), so the
+// have returned: the folding warps' stores are not drained at the barriers.
+// The dispatcher uses clusters of 2.  The staged rows are swizzled by the
+// TMA (16-byte chunk index XOR 128-byte row index), so the
 // step-(A) reads of a half warp (4 ring pairs x 4 rows) spread over the
 // banks; the transform area has an odd row pitch and a ring-pair stride of
 // 2 (mod 8) 16-byte slots.
@@ -685,16 +686,13 @@ int phi3c_run(const sph_plan* p, const PhiArgs& a, int nfields, cudaStream_t st)
   }
 }
 
-// cluster size: 4 (128-byte runs) where nlat/2 splits into tiles of 16 ring
-// pairs, else 2; a plan with ring pairs set by sph_plan_set_tiles keeps the
-// single-CTA kernels those settings were tuned on
+// clusters of 2 CTAs (64-byte runs): at nphi 1536 they place on all 148 SMs
+// (clusters of 4 on 132) and their barriers are cheaper, 5.2 against 7.8 ms
+// for the four fields of the benchmark pair; a plan with ring pairs set by
+// sph_plan_set_tiles keeps the single-CTA kernels those settings were tuned on
 template <int N>
 int phi3c_dispatch_n(const sph_plan* p, const PhiArgs& a, int nfields, cudaStream_t st) {
   if (p->tile_np) return PHI3C_UNSUPPORTED;  // tuned ring pairs: the kernels they were tuned on
-  if (p->nlat2 % 16 == 0) {
-    const int rc = phi3c_run<N, 4>(p, a, nfields, st);
-    if (rc != PHI3C_UNSUPPORTED) return rc;
-  }
   if (p->nlat2 % 8 == 0) return phi3c_run<N, 2>(p, a, nfields, st);
   return PHI3C_UNSUPPORTED;
 }
