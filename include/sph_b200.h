@@ -253,10 +253,11 @@ int sph_prodvec(sph_plan* plan, const double* ar, const double* at, const double
  *              W = 0, W'' - 2 W'/r = 0, Z' - 2 Z/r = 0, the last by the
  *              Robin reconstruction (needs sph_plan_set_neumann, else
  *              SPH_ENOTREADY).
- * Builds the FC-Gram derivative matrices, the row-scaled LU per l in FP64
- * on the host (rows 2 and N-1 of B_l by the kind of their wall), and uploads
- * M_l (N x (N-4) per l) and the d2/dr2 border rows; a clone whose source
- * built them for the same kinds shares them. */
+ * Builds the FC-Gram derivative matrices (a direct DFT), the row-scaled LU
+ * per l and the solve on the host in long double (rows 2 and N-1 of B_l by
+ * the kind of their wall), and uploads M_l (N x (N-4) per l, rounded to
+ * FP64) and the d2/dr2 border rows; a clone whose source built them for the
+ * same kinds shares them. */
 int sph_setup_bc(sph_plan* plan, const char* bcint, const char* bcext);
 /* neumann_reconstruct (src/sphp/fcgram_mod.f90:368-520, the z boundaries)
  * on spectral (nlm, nz) f: boun 0 = inner wall (z index 0), 1 = outer wall
@@ -339,7 +340,8 @@ int sph_run(sph_plan* plan, double* Z, double* W, double* phi, double nu, double
  * arrays (grids: float[nz][nphi][nlat]; spectra: float pairs [nz][nlm]), on
  * an SPH_MIXED plan over whole fields (SPH_EINVAL otherwise).  The mixed
  * engine reads and writes the float grids in its phi FFTs and the float
- * spectra in its z transforms directly; results agree with the FP64 path to
+ * spectra in its z transforms directly, and the pointwise operators read and
+ * write float arrays (computing in FP64); results agree with the FP64 path to
  * the mixed form's accuracy and float rounding.  The inverse transforms
  * preserve their input. */
 int sph_fftp2d_real_to_complex_xy_f32(sph_plan* plan, const float* in, float* out, void* stream);
@@ -359,6 +361,23 @@ int sph_fftp3d_qst_to_vec_f32(sph_plan* plan, const float* q, const float* s, co
 int sph_derivr_f32(sph_plan* plan, const float* a, float* b, int p, char esp, void* stream);
 int sph_dlr_f32(sph_plan* plan, const float* a, float* b, void* stream);
 int sph_fc_filter_f32(sph_plan* plan, float* a, char esp, void* stream);
+int sph_laplang_f32(sph_plan* plan, const float* a, float* b, void* stream);
+int sph_multr_f32(sph_plan* plan, const float* a, float* b, int p, void* stream);
+int sph_saxpby_c_f32(sph_plan* plan, float* z, const float* x, double a, const float* y, double b, void* stream);
+int sph_saxpby_r_f32(sph_plan* plan, float* z, const float* x, double a, const float* y, double b, void* stream);
+int sph_copy_f32(sph_plan* plan, const float* a, float* b, void* stream);
+int sph_prodvec_f32(sph_plan* plan, const float* ar, const float* at, const float* ap, const float* br,
+                    const float* bt, const float* bp, float* cr, float* ct, float* cp, void* stream);
+int sph_dirichlet_f32(sph_plan* plan, float* a, void* stream);
+/* the boundary solve and the NL step on FP64 copies of the float spectra in
+ * the plan's scratch (needs sph_setup_bc like their FP64 counterparts) */
+int sph_invDl_f32(sph_plan* plan, const float* phi, float* w, void* stream);
+int sph_v_imposebc_f32(sph_plan* plan, float* tor, float* phi, float* pol, void* stream);
+int sph_v_imposebc_fast_f32(sph_plan* plan, float* tor, float* phi, float* pol, void* stream);
+int sph_nl_rhs_f32(sph_plan* plan, const float* Z, const float* W, const float* phi, double nu, float* rhs_z,
+                   float* rhs_phi, double* energy, void* stream);
+int sph_rk3_step_f32(sph_plan* plan, float* Z, float* W, float* phi, double nu, double dt, double* energy,
+                     void* stream);
 
 /* ---------------------------------------------------------------- timers
  * The reference accumulates wall time per stage in gtimer handles

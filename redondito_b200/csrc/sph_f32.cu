@@ -54,12 +54,68 @@ int narrow(const double* in, float* out, size_t n, cudaStream_t st) {
   return SPH_OK;
 }
 
-// FP64 spectral scratch i (0..2) of the plan, allocated on first use
+// FP64 spectral scratch i (0..4) of the plan, allocated on first use
 int scratch(sph_plan* p, int i, double2** out) {
   if (!p->fsp[i] && cudaMalloc((void**)&p->fsp[i], spec_elems(p) * sizeof(double2)) != cudaSuccess)
     return SPH_ENOMEM;
   *out = p->fsp[i];
   return SPH_OK;
+}
+
+// pointwise operators on float arrays, computed in FP64
+// (pseudospec_hd.f90:138-251,291-366; boundary_mod.f90:62-93)
+__global__ void laplang_f32(const float2* __restrict__ a, float2* __restrict__ b, const int* __restrict__ ell,
+                            int nlm, size_t n) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const int l = ell[q % nlm];
+    const double f = -(double)(l * (l + 1));
+    const float2 v = a[q];
+    b[q] = make_float2((float)(f * v.x), (float)(f * v.y));
+  }
+}
+__global__ void multr_f32(const float2* __restrict__ a, float2* __restrict__ b, const double* __restrict__ z,
+                          int power, int nlm, size_t n) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    double zk = z[q / nlm], zp = 1.0;
+    const int ap = power < 0 ? -power : power;
+    for (int i = 0; i < ap; ++i) zp *= zk;
+    if (power < 0) zp = 1.0 / zp;
+    const float2 v = a[q];
+    b[q] = make_float2((float)(zp * v.x), (float)(zp * v.y));
+  }
+}
+__global__ void saxpby_f32(float* z, const float* x, double a, const float* y, double b, size_t n) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+    z[q] = (float)(a * (double)x[q] + b * (double)y[q]);
+}
+__global__ void prodvec_f32(const float* __restrict__ ar, const float* __restrict__ at, const float* __restrict__ ap,
+                            const float* __restrict__ br, const float* __restrict__ bt, const float* __restrict__ bp,
+                            float* cr, float* ct, float* cp, size_t nphys, size_t ntot) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < ntot; q += (size_t)gridDim.x * blockDim.x) {
+    if (q < nphys) {
+      const double xr = ar[q], xt = at[q], xp = ap[q], yr = br[q], yt = bt[q], yp = bp[q];
+      cr[q] = (float)(xt * yp - xp * yt);
+      ct[q] = (float)(xp * yr - xr * yp);
+      cp[q] = (float)(xr * yt - xt * yr);
+    } else {
+      cr[q] = ct[q] = cp[q] = 0.0f;
+    }
+  }
+}
+__global__ void dirichlet_f32(float2* a, int nlm, int N) {
+  for (int lm = blockIdx.x * blockDim.x + threadIdx.x; lm < nlm; lm += gridDim.x * blockDim.x) {
+    a[lm] = make_float2(0.f, 0.f);
+    a[(size_t)(N - 1) * nlm + lm] = make_float2(0.f, 0.f);
+  }
+}
+
+// float spectra -> FP64 scratch i
+int widen_spec(sph_plan* p, const float* in, int i, double2** out, cudaStream_t st) {
+  RCF(scratch(p, i, out));
+  return widen(in, reinterpret_cast<double*>(*out), 2 * spec_elems(p), st);
+}
+int narrow_spec(const sph_plan* p, const double2* in, float* out, cudaStream_t st) {
+  return narrow(reinterpret_cast<const double*>(in), out, 2 * spec_elems(p), st);
 }
 
 // the analysis of nv fields (1: scalar, 3: vector) from float grids g into
@@ -218,4 +274,129 @@ extern "C" int sph_fc_filter_f32(sph_plan* p, float* a, char esp, void* s) {
   RCF(widen(a, reinterpret_cast<double*>(x), 2 * spec_elems(p), st_of(s)));
   RCF(sph_fc_filter(p, reinterpret_cast<double*>(x), 'k', s));
   return narrow(reinterpret_cast<const double*>(x), a, 2 * spec_elems(p), st_of(s));
+}
+
+// ---------------------------------------------------------------- pointwise operators
+extern "C" int sph_laplang_f32(sph_plan* p, const float* a, float* b, void* s) {
+  if (!f32_ok(p) || !a || !b) return SPH_EINVAL;
+  const size_t n = spec_elems(p);
+  laplang_f32<<<blocks_for(n), 256, 0, st_of(s)>>>(reinterpret_cast<const float2*>(a), reinterpret_cast<float2*>(b),
+                                                    p->d_ell, p->nlm, n);
+  SPH_LAUNCH_OK();
+  return SPH_OK;
+}
+
+extern "C" int sph_multr_f32(sph_plan* p, const float* a, float* b, int pw, void* s) {
+  if (!f32_ok(p) || !a || !b) return SPH_EINVAL;
+  const size_t n = spec_elems(p);
+  multr_f32<<<blocks_for(n), 256, 0, st_of(s)>>>(reinterpret_cast<const float2*>(a), reinterpret_cast<float2*>(b),
+                                                  p->d_z, pw, p->nlm, n);
+  SPH_LAUNCH_OK();
+  return SPH_OK;
+}
+
+extern "C" int sph_saxpby_c_f32(sph_plan* p, float* z, const float* x, double a, const float* y, double b, void* s) {
+  if (!f32_ok(p) || !z || !x || !y) return SPH_EINVAL;
+  const size_t n = 2 * spec_elems(p);
+  saxpby_f32<<<blocks_for(n), 256, 0, st_of(s)>>>(z, x, a, y, b, n);
+  SPH_LAUNCH_OK();
+  return SPH_OK;
+}
+
+extern "C" int sph_saxpby_r_f32(sph_plan* p, float* z, const float* x, double a, const float* y, double b, void* s) {
+  if (!f32_ok(p) || !z || !x || !y) return SPH_EINVAL;
+  const size_t n = grid_elems(p);
+  saxpby_f32<<<blocks_for(n), 256, 0, st_of(s)>>>(z, x, a, y, b, n);
+  SPH_LAUNCH_OK();
+  return SPH_OK;
+}
+
+extern "C" int sph_copy_f32(sph_plan* p, const float* a, float* b, void* s) {
+  if (!f32_ok(p) || !a || !b) return SPH_EINVAL;
+  if (a != b && cudaMemcpyAsync(b, a, spec_elems(p) * 2 * sizeof(float), cudaMemcpyDeviceToDevice, st_of(s)) !=
+                    cudaSuccess)
+    return SPH_ECUDA;
+  return SPH_OK;
+}
+
+extern "C" int sph_prodvec_f32(sph_plan* p, const float* ar, const float* at, const float* ap, const float* br,
+                               const float* bt, const float* bp, float* cr, float* ct, float* cp, void* s) {
+  if (!f32_ok(p) || !ar || !at || !ap || !br || !bt || !bp || !cr || !ct || !cp) return SPH_EINVAL;
+  const size_t plane = (size_t)p->nlat * p->nphi, ntot = plane * p->nz, nphys = plane * p->N;
+  prodvec_f32<<<blocks_for(ntot), 256, 0, st_of(s)>>>(ar, at, ap, br, bt, bp, cr, ct, cp, nphys, ntot);
+  SPH_LAUNCH_OK();
+  return SPH_OK;
+}
+
+extern "C" int sph_dirichlet_f32(sph_plan* p, float* a, void* s) {
+  if (!f32_ok(p) || !a) return SPH_EINVAL;
+  dirichlet_f32<<<blocks_for(p->nlm), 256, 0, st_of(s)>>>(reinterpret_cast<float2*>(a), p->nlm, p->N);
+  SPH_LAUNCH_OK();
+  return SPH_OK;
+}
+
+// ---------------------------------------------------------------- boundary, NL step
+// The boundary solve and the nonlinear step run on FP64 copies of the float
+// spectra in the plan's scratch (the state of a step is FP64 by design; the
+// copies are a small share of a step's traffic).
+extern "C" int sph_invDl_f32(sph_plan* p, const float* phi, float* w, void* s) {
+  if (!f32_ok(p) || !phi || !w) return SPH_EINVAL;
+  double2 *f, *x;
+  RCF(widen_spec(p, phi, 0, &f, st_of(s)));
+  RCF(scratch(p, 1, &x));
+  RCF(sph_invDl(p, reinterpret_cast<const double*>(f), reinterpret_cast<double*>(x), s));
+  return narrow_spec(p, x, w, st_of(s));
+}
+
+namespace {
+int imposebc_f32(sph_plan* p, float* tor, float* phi, float* pol, void* s, bool fast) {
+  if (!f32_ok(p) || !tor || !phi || !pol) return SPH_EINVAL;
+  double2 *t, *f, *w;
+  RCF(widen_spec(p, tor, 0, &t, st_of(s)));
+  RCF(widen_spec(p, phi, 1, &f, st_of(s)));
+  RCF(widen_spec(p, pol, 2, &w, st_of(s)));  // v_imposebc_fast keeps pol's rows it does not set
+  double *td = reinterpret_cast<double*>(t), *fd = reinterpret_cast<double*>(f), *wd = reinterpret_cast<double*>(w);
+  RCF(fast ? sph_v_imposebc_fast(p, td, fd, wd, s) : sph_v_imposebc(p, td, fd, wd, s));
+  RCF(narrow_spec(p, t, tor, st_of(s)));
+  RCF(narrow_spec(p, f, phi, st_of(s)));
+  return narrow_spec(p, w, pol, st_of(s));
+}
+}  // namespace
+
+extern "C" int sph_v_imposebc_f32(sph_plan* p, float* tor, float* phi, float* pol, void* s) {
+  return imposebc_f32(p, tor, phi, pol, s, false);
+}
+
+extern "C" int sph_v_imposebc_fast_f32(sph_plan* p, float* tor, float* phi, float* pol, void* s) {
+  return imposebc_f32(p, tor, phi, pol, s, true);
+}
+
+extern "C" int sph_nl_rhs_f32(sph_plan* p, const float* Z, const float* W, const float* phi, double nu, float* rhs_z,
+                              float* rhs_phi, double* energy, void* s) {
+  if (!f32_ok(p) || !Z || !W || !phi || !rhs_z || !rhs_phi) return SPH_EINVAL;
+  double2 *z, *w, *f, *rz, *rf;
+  RCF(widen_spec(p, Z, 0, &z, st_of(s)));
+  RCF(widen_spec(p, W, 1, &w, st_of(s)));
+  RCF(widen_spec(p, phi, 2, &f, st_of(s)));
+  RCF(scratch(p, 3, &rz));
+  RCF(scratch(p, 4, &rf));
+  RCF(sph_nl_rhs(p, reinterpret_cast<const double*>(z), reinterpret_cast<const double*>(w),
+                 reinterpret_cast<const double*>(f), nu, reinterpret_cast<double*>(rz), reinterpret_cast<double*>(rf),
+                 energy, s));
+  RCF(narrow_spec(p, rz, rhs_z, st_of(s)));
+  return narrow_spec(p, rf, rhs_phi, st_of(s));
+}
+
+extern "C" int sph_rk3_step_f32(sph_plan* p, float* Z, float* W, float* phi, double nu, double dt, double* energy,
+                                void* s) {
+  if (!f32_ok(p) || !Z || !W || !phi) return SPH_EINVAL;
+  double2 *z, *w, *f;
+  RCF(widen_spec(p, Z, 0, &z, st_of(s)));
+  RCF(widen_spec(p, W, 1, &w, st_of(s)));
+  RCF(widen_spec(p, phi, 2, &f, st_of(s)));
+  RCF(sph_rk3_step(p, reinterpret_cast<double*>(z), reinterpret_cast<double*>(w), reinterpret_cast<double*>(f), nu,
+                   dt, energy, s));
+  RCF(narrow_spec(p, z, Z, st_of(s)));
+  RCF(narrow_spec(p, w, W, st_of(s)));
+  return narrow_spec(p, f, phi, st_of(s));
 }

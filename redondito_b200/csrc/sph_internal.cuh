@@ -124,7 +124,7 @@ struct sph_plan {
   double* gr[9] = {nullptr};
   int ngr = 0;
   // FP64 spectral scratch of the single-precision entry points (allocated on first use)
-  double2* fsp[3] = {nullptr};
+  double2* fsp[5] = {nullptr};
   // boundary: kinds at the inner and outer wall (0 noslip, 1 freeslip); the
   // plan owns binv/d2bor when its kinds differ from the shared tables'
   int bck[2] = {0, 0};

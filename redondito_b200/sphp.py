@@ -57,6 +57,9 @@ SYMBOLS = (
     "sph_fftp2d_vec_to_qst_f32", "sph_fftp2d_qst_to_vec_f32",
     "sph_fftp3d_vec_to_qst_f32", "sph_fftp3d_qst_to_vec_f32",
     "sph_derivr_f32", "sph_dlr_f32", "sph_fc_filter_f32",
+    "sph_laplang_f32", "sph_multr_f32", "sph_saxpby_c_f32", "sph_saxpby_r_f32", "sph_copy_f32",
+    "sph_prodvec_f32", "sph_dirichlet_f32", "sph_invDl_f32", "sph_v_imposebc_f32",
+    "sph_v_imposebc_fast_f32", "sph_nl_rhs_f32", "sph_rk3_step_f32",
 )
 TIMER_CLASSES = ("phi_fwd", "phi_inv", "leg_analysis", "leg_synthesis", "vec_analysis",
                  "vec_synthesis", "zfft", "ops")
@@ -150,6 +153,18 @@ def lib(build_if_missing=True):
             "sph_derivr_f32": [P, Vp, Vp, I, ctypes.c_char, Vp],
             "sph_dlr_f32": [P, Vp, Vp, Vp],
             "sph_fc_filter_f32": [P, Vp, ctypes.c_char, Vp],
+            "sph_laplang_f32": [P, Vp, Vp, Vp],
+            "sph_multr_f32": [P, Vp, Vp, I, Vp],
+            "sph_saxpby_c_f32": [P, Vp, Vp, D, Vp, D, Vp],
+            "sph_saxpby_r_f32": [P, Vp, Vp, D, Vp, D, Vp],
+            "sph_copy_f32": [P, Vp, Vp, Vp],
+            "sph_prodvec_f32": [P] + [Vp] * 9 + [Vp],
+            "sph_dirichlet_f32": [P, Vp, Vp],
+            "sph_invDl_f32": [P, Vp, Vp, Vp],
+            "sph_v_imposebc_f32": [P, Vp, Vp, Vp, Vp],
+            "sph_v_imposebc_fast_f32": [P, Vp, Vp, Vp, Vp],
+            "sph_nl_rhs_f32": [P, Vp, Vp, Vp, D, Vp, Vp, pD, Vp],
+            "sph_rk3_step_f32": [P, Vp, Vp, Vp, D, D, pD, Vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -540,6 +555,63 @@ def dlr_f32(plan, a, b, stream=None):
 
 def fc_filter_f32(plan, a, esp="r", stream=None):
     _call("sph_fc_filter_f32", plan.h, _s32(plan, a), esp.encode(), _stream(stream))
+
+
+def laplang_f32(plan, a, b, stream=None):
+    _call("sph_laplang_f32", plan.h, _s32(plan, a), _s32(plan, b), _stream(stream))
+
+
+def multr_f32(plan, a, b, p, stream=None):
+    _call("sph_multr_f32", plan.h, _s32(plan, a), _s32(plan, b), int(p), _stream(stream))
+
+
+def saxpby_c_f32(plan, z, x, a, y, b, stream=None):
+    _call("sph_saxpby_c_f32", plan.h, _s32(plan, z), _s32(plan, x), float(a), _s32(plan, y), float(b),
+          _stream(stream))
+
+
+def saxpby_r_f32(plan, z, x, a, y, b, stream=None):
+    _call("sph_saxpby_r_f32", plan.h, _g32(plan, z), _g32(plan, x), float(a), _g32(plan, y), float(b),
+          _stream(stream))
+
+
+def copy_f32(plan, a, b, stream=None):
+    _call("sph_copy_f32", plan.h, _s32(plan, a), _s32(plan, b), _stream(stream))
+
+
+def prodvec_f32(plan, ar, at, ap, br, bt, bp, cr, ct, cp, stream=None):
+    _call("sph_prodvec_f32", plan.h, *[_g32(plan, x) for x in (ar, at, ap, br, bt, bp, cr, ct, cp)],
+          _stream(stream))
+
+
+def dirichlet_f32(plan, a, stream=None):
+    _call("sph_dirichlet_f32", plan.h, _s32(plan, a), _stream(stream))
+
+
+def invDl_f32(plan, phi, w, stream=None):
+    _call("sph_invDl_f32", plan.h, _s32(plan, phi), _s32(plan, w), _stream(stream))
+
+
+def v_imposebc_f32(plan, tor, phi, pol, stream=None):
+    _call("sph_v_imposebc_f32", plan.h, _s32(plan, tor), _s32(plan, phi), _s32(plan, pol), _stream(stream))
+
+
+def v_imposebc_fast_f32(plan, tor, phi, pol, stream=None):
+    _call("sph_v_imposebc_fast_f32", plan.h, _s32(plan, tor), _s32(plan, phi), _s32(plan, pol), _stream(stream))
+
+
+def nl_rhs_f32(plan, Z, W, phi, nu, rhs_z, rhs_phi, stream=None):
+    e = ctypes.c_double(0.0)
+    _call("sph_nl_rhs_f32", plan.h, _s32(plan, Z), _s32(plan, W), _s32(plan, phi), float(nu),
+          _s32(plan, rhs_z), _s32(plan, rhs_phi), ctypes.byref(e), _stream(stream))
+    return e.value
+
+
+def rk3_step_f32(plan, Z, W, phi, nu, dt, stream=None, energy=True):
+    e = ctypes.c_double(0.0)
+    _call("sph_rk3_step_f32", plan.h, _s32(plan, Z), _s32(plan, W), _s32(plan, phi), float(nu), float(dt),
+          ctypes.byref(e) if energy else None, _stream(stream))
+    return e.value
 
 
 # ---------------------------------------------------------------- NL + RK3

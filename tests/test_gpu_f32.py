@@ -127,3 +127,75 @@ def test_fp64_plans_are_refused():
     with pytest.raises(S.SphError):
         S.fftp3d_real_to_complex_f32(G, G.new_grid32(), G.new_spec32())
     G.close()
+
+
+def test_pointwise_operators():
+    """Computed in FP64 from the float inputs: within float rounding of the
+    oracle on the widened inputs."""
+    S, P, G = _pair(15, 64, 24, 48)
+    rng = np.random.default_rng(8)
+    a, y = widened(random_spec(P, rng)), widened(random_spec(P, rng))
+    b = G.new_spec32()
+    S.laplang_f32(G, f32(a), b)
+    check(rel_l2(host64(b), P.laplang(a)), 1e-7, "laplang")
+    S.multr_f32(G, f32(a), b, -2)
+    check(rel_l2(host64(b), P.multr(a, -2)), 1e-7, "multr")
+    z = G.new_spec32()
+    S.saxpby_c_f32(G, z, f32(a), 2.0, f32(y), -3.0)
+    check(rel_l2(host64(z), P.saxpby_c(a, 2.0, y, -3.0)), 1e-7, "saxpby_c")
+    S.copy_f32(G, f32(a), b)
+    assert rel_l2(host64(b), a) == 0.0
+    x = f32(a)
+    S.dirichlet_f32(G, x)
+    check(rel_l2(host64(x), P.dirichlet(a)), 1e-7, "dirichlet")
+    g = [widened(P.sh_synthesis(random_spec(P, rng))) for _ in range(6)]
+    c = [G.new_grid32() for _ in range(3)]
+    S.prodvec_f32(G, *(f32(v) for v in g), *c)
+    for u, v, name in zip(c, P.prodvec(g[:3], g[3:]), ("r", "t", "p")):
+        check(rel_l2(host64(u), v), 1e-7, f"prodvec {name}")
+    zr = G.new_grid32()
+    S.saxpby_r_f32(G, zr, f32(g[0]), 0.5, f32(g[1]), 2.0)
+    check(rel_l2(host64(zr), P.saxpby_r(g[0], 0.5, g[1], 2.0)), 1e-7, "saxpby_r")
+    G.close()
+
+
+def test_boundary_and_nl_step_match_the_fp64_arrays():
+    """The boundary solve, the NL step and RK3 on float arrays run the FP64
+    routines on widened copies: their outputs equal the FP64-array calls on
+    the same (widened) inputs to float rounding."""
+    S, P, G = _pair(15, 64, 24, 48)
+    S.setup_bc(G)
+    rng = np.random.default_rng(9)
+    Z = widened(random_spec(P, rng, power=3.0))
+    W = widened(random_spec(P, rng, power=3.0))
+    phi = widened(P.dlr(W))
+
+    def d64(x):
+        return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+    w32, w64 = G.new_spec32(), G.new_spec()
+    S.invDl_f32(G, f32(phi), w32)
+    S.invDl(G, d64(phi), w64)
+    check(rel_l2(host64(w32), host64(w64)), 1e-7, "invDl")
+    for fast in (False, True):
+        t32, f32_, p32 = f32(Z), f32(phi), G.new_spec32()
+        t64, f64_, p64 = d64(Z), d64(phi), G.new_spec()
+        (S.v_imposebc_fast_f32 if fast else S.v_imposebc_f32)(G, t32, f32_, p32)
+        (S.v_imposebc_fast if fast else S.v_imposebc)(G, t64, f64_, p64)
+        for a, b, name in ((t32, t64, "tor"), (f32_, f64_, "phi"), (p32, p64, "pol")):
+            check(rel_l2(host64(a), host64(b)), 1e-7, f"imposebc fast={fast} {name}")
+    Zs, Ws, Fs = (widened(host64(x)) for x in (t64, p64, f64_))
+    rz32, rf32, rz64, rf64 = G.new_spec32(), G.new_spec32(), G.new_spec(), G.new_spec()
+    e32 = S.nl_rhs_f32(G, f32(Zs), f32(Ws), f32(Fs), 1e-3, rz32, rf32)
+    e64 = S.nl_rhs(G, d64(Zs), d64(Ws), d64(Fs), 1e-3, rz64, rf64)
+    assert e32 == e64
+    check(rel_l2(host64(rz32), host64(rz64)), 1e-7, "rhs_z")
+    check(rel_l2(host64(rf32), host64(rf64)), 1e-7, "rhs_phi")
+    a32 = [f32(x) for x in (Zs, Ws, Fs)]
+    a64 = [d64(x) for x in (Zs, Ws, Fs)]
+    S.rk3_step_f32(G, *a32, 1e-3, 1e-4)
+    S.rk3_step(G, *a64, 1e-3, 1e-4)
+    for a, b, name in zip(a32, a64, ("Z", "W", "phi")):
+        check(rel_l2(host64(a), host64(b)), 1e-7, f"RK3 {name}")
+    S.plan_status(G)
+    G.close()
