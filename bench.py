@@ -66,6 +66,7 @@ def parse():
                     help="mixed (the headline, with the FP64 form timed beside it) or fp64")
     ap.add_argument("--no-fp64", action="store_true", help="mixed only: skip the FP64 comparison")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-f32", action="store_true", help="skip the single-precision-array pair")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-c4", action="store_true", help="skip the 64-problem batched ensemble")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop measurement")
@@ -262,6 +263,17 @@ def pair(S, P, st, grids):
     S.fftp3d_vec_to_qst(P, g1, g2, g3, q, s, t)
 
 
+def pair32(S, P, st, grids):
+    """The same pair with float grids and complex64 spectra (the
+    single-precision entry points, a GSINGLE_PRECISION build's arrays)."""
+    a, q, s, t = st
+    g0, g1, g2, g3 = grids
+    S.fftp3d_complex_to_real_f32(P, a, g0)
+    S.fftp3d_qst_to_vec_f32(P, q, s, t, g1, g2, g3)
+    S.fftp3d_real_to_complex_f32(P, g0, a)
+    S.fftp3d_vec_to_qst_f32(P, g1, g2, g3, q, s, t)
+
+
 def fp64_peak():
     from redondito_b200 import build as B
     try:
@@ -433,7 +445,7 @@ def serving_c5(S, torch, nreq=200, rate=500.0, rank=0, world=1, dist=None, budge
     return out
 
 
-def time_pairs(S, P, st, grids, steps, stream, torch, dist, world):
+def time_pairs(S, P, st, grids, steps, stream, torch, dist, world, fn=pair):
     """Device time of `steps` pairs (barrier + sync on both sides, max over ranks)."""
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if world > 1:
@@ -441,7 +453,7 @@ def time_pairs(S, P, st, grids, steps, stream, torch, dist, world):
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(steps):
-        pair(S, P, st, grids)
+        fn(S, P, st, grids)
     e1.record(stream)
     torch.cuda.synchronize()
     if world > 1:
@@ -487,7 +499,7 @@ def per_output_errors(S, Pm, Pd, st0, torch):
     return rel, mx
 
 
-def e2e_pairs(S, P, st, grids, steps, stream, torch, dist, world):
+def e2e_pairs(S, P, st, grids, steps, stream, torch, dist, world, fn=pair):
     """The pair through the C ABI with host buffers: every step copies its four
     spectral fields from pinned host memory, runs the pair and copies the
     results back.  Steps are pipelined the way a streaming caller would run
@@ -521,7 +533,7 @@ def e2e_pairs(S, P, st, grids, steps, stream, torch, dist, world):
         in_done[b].record(s_in)
         stream.wait_event(in_done[b])
         with torch.cuda.stream(stream):
-            pair(S, P, d, grids)
+            fn(S, P, d, grids)
         comp_done[b].record(stream)
         s_out.wait_event(comp_done[b])
         with torch.cuda.stream(s_out):
@@ -728,6 +740,21 @@ def main():
     if not args.no_e2e:
         e2e = e2e_pairs(S, P, st, grids, args.steps, stream, torch, dist, world)
 
+    # the same pair with the single-precision arrays on the mixed plan: device
+    # time and e2e (float host buffers: half the bytes each way)
+    single = None
+    if prec == S.SPH_MIXED and not args.no_f32:
+        st32 = [x.to(torch.complex64) for x in st0]
+        g32 = [P.new_grid32() for _ in range(4)]
+        for _ in range(max(1, args.warmup)):
+            pair32(S, P, st32, g32)
+        ms32 = time_pairs(S, P, st32, g32, args.steps, stream, torch, dist, world, fn=pair32)
+        single = {"value": world * args.steps / (ms32 * 1e-3), "unit": "pairs/s", "ms_per_step": ms32 / args.steps,
+                  "arrays": "float grids, complex64 spectra (sph_*_f32 on the mixed plan)"}
+        if not args.no_e2e:
+            single["e2e"] = e2e_pairs(S, P, st32, g32, args.steps, stream, torch, dist, world, fn=pair32)
+        del st32, g32
+
     # the FP64 form on the same state: its time, per-kernel rooflines and e2e,
     # and the mixed form's error per output against it
     fp64 = None
@@ -830,6 +857,7 @@ def main():
         "kernels": per_class,
         "stage_share": shares,
         "fp64": fp64,
+        "single": single,
         "speedup_vs_fp64": (value / fp64["value"]) if fp64 else None,
         "accuracy": errors,
         "c1": c1,
