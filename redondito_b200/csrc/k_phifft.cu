@@ -553,7 +553,13 @@ __global__ void __launch_bounds__(P3c<N, CL>::THREADS, 1)
     const int g = tile % ngroups, rr = tile / ngroups, k = rr % a.nz, f = rr / a.nz;
     // (A) the samples x[nm + M n1] of local ring pair b (ring: real part, mirror: imaginary part)
     const bool act = t < G::ITEMS_A;
-    const int b = t % NPL, nm = t / NPL;
+    // ring pair b of the CTA, row nm: with clusters of 2 a staged row is 64
+    // bytes and this CTA reads 32 of them; a half warp takes rows
+    // {q, q+1, q+4, q+5} (bits 1 and 2 of the row index swapped within blocks
+    // of 8 rows), which the 64-byte swizzle puts in four distinct 32-byte bank
+    // groups (rows q and q+2 would share one)
+    const int b = t % NPL, g8 = t / NPL;
+    const int nm = (CL == 2 && (g8 | 7) < M) ? ((g8 & ~7) | (g8 & 1) | ((g8 & 2) << 1) | ((g8 & 4) >> 1)) : g8;
     double2 v[A];
     if (act) {
       const int col = (int)rank * NPL + b;
