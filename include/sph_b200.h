@@ -167,8 +167,10 @@ int sph_fftp1d_complex_to_real_z(sph_plan* plan, double* inout, void* stream);
 int sph_fftp3d_real_to_complex(sph_plan* plan, const double* in, double* out, void* stream);
 
 /* fftp3d_complex_to_real (src/sphp-gpu/sphp_sca.F90:948-981): z inverse +
- * 2D synthesis.  in is destroyed (the z transform is in place), as in the
- * reference. */
+ * 2D synthesis.  in may be destroyed, as in the reference: FP64 plans
+ * transform it in place in z; SPH_MIXED plans (nz of 16, 32, 48, 64, 96,
+ * 128, 192, 256 or 512) write the z inverse straight into the synthesis
+ * tiles and leave it unchanged. */
 int sph_fftp3d_complex_to_real(sph_plan* plan, double* in, double* out, void* stream);
 
 /* fftp2d_vec_to_qst (src/sphp-gpu/sphp_vec.F90:128-218): (v_r,v_th,v_ph) ->
@@ -184,8 +186,8 @@ int sph_fftp2d_qst_to_vec(sph_plan* plan, const double* q, const double* s, cons
  * them in its nonlinear-term code as fftp2d_vec_to_qst followed by
  * fftp1d_real_to_complex_z on q, s and t, and fftp1d_complex_to_real_z on
  * q, s, t followed by fftp2d_qst_to_vec; these entry points compute exactly
- * those compositions).  sph_fftp3d_qst_to_vec transforms q, s, t in place
- * in z, like sph_fftp3d_complex_to_real.  On SPH_MIXED plans with FC-Gram
+ * those compositions).  sph_fftp3d_qst_to_vec may destroy q, s, t the way
+ * sph_fftp3d_complex_to_real may destroy its input.  On SPH_MIXED plans with FC-Gram
  * continuation the forward one continues the physical planes in FP64 before
  * the angular analysis, which keeps the continuation from amplifying the
  * angular round-off (the same holds for sph_fftp3d_real_to_complex). */

@@ -1273,6 +1273,68 @@ __global__ void spec_to_tiles(const double2* __restrict__ in, const double2* __r
   }
 }
 
+// z inverse (fftp1d_complex_to_real_z, src/sphp/sphp_sca.F90:495-530, sign
+// +1) of the 16 columns l = m + 16c .. m + 16c + 15 of one m, written
+// straight into the synthesis tiles the way spec_to_tiles writes them: one
+// CTA per (m, c) item loads the columns in digit-reversed row order (zero
+// past lmax), transforms them in shared memory by the passes of
+// zfft_kernel<Z_INV> (the same operations per column, so the same bits), and
+// each plane's 8 values of a parity go out as one 16-byte row chunk per piece.
+// The column stride of 17 slots keeps the read-out conflict-free.  It saves
+// the z inverse's write of the spectra and spec_to_tiles' read of them.
+constexpr int ZT_COLS = 16, ZT_PITCH = 17, ZT_THREADS = 256;
+
+struct ZtArgs {
+  const double2* in;
+  __nv_bfloat16* tiles;
+  const long long* toff;
+  const int* mbase;
+  const int2* items;
+  int lmax, nlm, nz;
+  const int* rev;
+  const double2* twp;
+};
+
+__device__ __forceinline__ void cp_async16zf(void* dst, const void* src, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+
+template <int NZ>
+__global__ void __launch_bounds__(ZT_THREADS) zinv_tiles(ZtArgs a) {
+  extern __shared__ double2 zs[];  // element e of column j at j + ZT_PITCH e
+  const int2 it = a.items[blockIdx.x];
+  const int m = it.x, c = it.y, t = threadIdx.x;
+  const double2* base = a.in + (a.mbase[m] - m);  // column l of row r at base[r nlm + l]
+  for (int idx = t; idx < NZ * ZT_COLS; idx += ZT_THREADS) {
+    const int r = idx / ZT_COLS, j = idx % ZT_COLS, l = m + ZT_COLS * c + j;
+    const bool in = l <= a.lmax;
+    cp_async16zf(zs + j + ZT_PITCH * __ldg(a.rev + r), in ? base + (size_t)r * a.nlm + l : a.in, in ? 16 : 0);
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncthreads();
+  const ct::Geo<NZ, 0, false> g{ZT_COLS, 1, ZT_PITCH};
+  ct::dit<double2, NZ, NZ>(zs, g, a.twp, +1);
+  const int kt = c / (TK / 8), kk0 = (c % (TK / 8)) * 8;
+  for (int w = t; w < NZ * 2; w += ZT_THREADS) {
+    const int k = w >> 1, par = w & 1;
+    if (kt >= ntiles_of(a.lmax, m, par)) continue;
+    float re[8], im[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const double2 v = zs[2 * i + par + ZT_PITCH * k];
+      re[i] = (float)v.x;
+      im[i] = (float)v.y;
+    }
+    __nv_bfloat16* tt = a.tiles + syn_tile(a.toff, a.lmax, m, par, k / PLANES, kt) * TILE_HALVES;
+    store_tile_row<8>(tt, 2 * (k % PLANES), kk0, re);
+    store_tile_row<8>(tt, 2 * (k % PLANES) + 1, kk0, im);
+  }
+}
+
+#define ZT_SIZES(X) X(16) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(512)
+
 // ---------------------------------------------------------------- host tables
 __host__ inline uint16_t bf16_bits(double x) {
   // x already rounded to 8 significant bits: exact in fp32 and bf16
@@ -1528,6 +1590,16 @@ int mixed_alloc_scratch(sph_plan* p) {
   }
   if (rc == SPH_OK && cudaMalloc((void**)&p->dflag, sizeof(int)) != cudaSuccess) rc = SPH_ENOMEM;
   if (rc == SPH_OK && cudaMemset(p->dflag, 0, sizeof(int)) != cudaSuccess) rc = SPH_ECUDA;
+  if (rc == SPH_OK) {  // (m, 16-degree chunk) items of the fused z inverse
+    std::vector<int2> items;
+    for (int m = 0; m <= lmax; ++m)
+      for (int c = 0; c * ZT_COLS <= lmax - m; ++c) items.push_back(make_int2(m, c));
+    p->nztitems = (int)items.size();
+    if (cudaMalloc((void**)&p->d_ztitems, items.size() * sizeof(int2)) != cudaSuccess) rc = SPH_ENOMEM;
+    else if (cudaMemcpy(p->d_ztitems, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice) !=
+             cudaSuccess)
+      rc = SPH_ECUDA;
+  }
   return rc;
 }
 
@@ -1559,9 +1631,11 @@ void mixed_free_tables(sph_plan* p) {
 }
 
 void mixed_free_scratch(sph_plan* p) {
-  void* ptrs[] = {p->dflag, p->Tana, p->Tsyn, p->contg, p->phi2};
+  void* ptrs[] = {p->dflag, p->Tana, p->Tsyn, p->contg, p->phi2, p->d_ztitems};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  p->d_ztitems = nullptr;
+  p->nztitems = 0;
   p->phi2 = nullptr;
   p->phi2_planes = 0;
   p->contg = nullptr;
@@ -2070,6 +2144,66 @@ int tc_group_launch(const GroupLaunch& g, int* flag, cudaStream_t st) {
   }
   SPH_LAUNCH_OK();
   return SPH_OK;
+}
+
+bool zinv_tiles_ok(const sph_plan* p) {
+  if (p->precision != SPH_MIXED || !p->d_ztitems || p->nztitems < 1) return false;
+  switch (p->nz) {
+#define CASE(n) \
+  case n:       \
+    return true;
+    ZT_SIZES(CASE)
+#undef CASE
+  }
+  return false;
+}
+
+namespace {
+template <int NZ>
+int zinv_tiles_run(const sph_plan* p, const ZtArgs& a, cudaStream_t st) {
+  const size_t smem = (size_t)ZT_PITCH * NZ * sizeof(double2);
+  static DeviceOnce once;
+  if (!once.run([] {
+        return cudaFuncSetAttribute(zinv_tiles<NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)((size_t)ZT_PITCH * NZ * sizeof(double2))) == cudaSuccess &&
+               cudaFuncSetAttribute(zinv_tiles<NZ>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) ==
+                   cudaSuccess;
+      }))
+    return SPH_ECUDA;
+  zinv_tiles<NZ><<<p->nztitems, ZT_THREADS, smem, st>>>(a);
+  SPH_LAUNCH_OK();
+  return SPH_OK;
+}
+}  // namespace
+
+int launch_zinv_tiles(const sph_plan* p, const double2* in, int field, cudaStream_t st) {
+  if (!zinv_tiles_ok(p) || !in || field < 0 || field >= SPH_MAX_FIELDS) return SPH_EINVAL;
+  ZtArgs a;
+  a.in = in;
+  a.tiles = reinterpret_cast<__nv_bfloat16*>(p->Tsyn) + (size_t)field * p->Tsynfield;
+  a.toff = p->d_toff;
+  a.mbase = p->d_mbase;
+  a.items = p->d_ztitems;
+  a.lmax = p->lmax;
+  a.nlm = p->nlm;
+  a.nz = p->nz;
+  a.rev = p->fz.rev;
+  a.twp = p->fz.twp;
+  TimedLaunch tl(p, T_ZFFT, st);
+  switch (p->nz) {
+#define CASE(n) \
+  case n: return zinv_tiles_run<n>(p, a, st);
+    ZT_SIZES(CASE)
+#undef CASE
+  }
+  return SPH_EINVAL;
+}
+
+int launch_tc_synthesis_tiles(const sph_plan* p, int vector, cudaStream_t st) {
+  TcArgs a = tc_args(p);
+  a.tiles = reinterpret_cast<const __nv_bfloat16*>(p->Tsyn);
+  TimedLaunch tl(p, vector ? T_VEC_SYN : T_LEG_SYN, st);
+  return vector ? run_tc<SYN_V>(p, p->tcSV, a, st) : run_tc<SYN_S>(p, p->tcSS, a, st);
 }
 
 int launch_spec_to_tiles_field(const sph_plan* p, const double2* in, int field, cudaStream_t st) {

@@ -450,6 +450,8 @@ extern "C" int sph_plan_clone(const sph_plan* src, sph_plan** out) {
   p->energy = p->spectrum = nullptr;
   p->dflag = nullptr;
   p->Tana = p->Tsyn = nullptr;
+  p->d_ztitems = nullptr;
+  p->nztitems = 0;
   p->contg = nullptr;
   p->phi2 = nullptr;
   p->phi2_planes = 0;
@@ -797,6 +799,12 @@ extern "C" int sph_fftp3d_real_to_complex(sph_plan* p, const double* in, double*
 
 extern "C" int sph_fftp3d_complex_to_real(sph_plan* p, double* in, double* out, void* s) {
   if (!p || !slab_whole(p)) return SPH_EINVAL;
+  if (in && out && zinv_tiles_ok(p)) {  // mixed: the z inverse writes the synthesis tiles (input preserved)
+    RC(launch_zinv_tiles(p, CD2(in), 0, ST(s)));
+    RC(launch_tc_synthesis_tiles(p, 0, ST(s)));
+    double* g[1] = {out};
+    return launch_phi_inv32(p, g, 1, ST(s));
+  }
   RC(sph_fftp1d_complex_to_real_z(p, in, s));
   return sph_fftp2d_complex_to_real_xy(p, in, out, s);
 }
@@ -863,6 +871,15 @@ extern "C" int sph_fftp3d_vec_to_qst(sph_plan* p, const double* vr, const double
 extern "C" int sph_fftp3d_qst_to_vec(sph_plan* p, double* q, double* sI, double* t, double* vr, double* vt,
                                      double* vp, void* s) {
   if (!p || !vr || !vt || !vp || !q || !sI || !t || !slab_whole(p)) return SPH_EINVAL;
+  if (zinv_tiles_ok(p)) {  // mixed: the z inverses write the synthesis tiles (inputs preserved)
+    RC(launch_zinv_tiles(p, CD2(q), 0, ST(s)));
+    RC(launch_tc_synthesis_tiles(p, 0, ST(s)));
+    RC(launch_zinv_tiles(p, CD2(sI), 0, ST(s)));
+    RC(launch_zinv_tiles(p, CD2(t), 1, ST(s)));
+    RC(launch_tc_synthesis_tiles(p, 1, ST(s)));
+    double* g[3] = {vr, vt, vp};
+    return launch_phi_inv32(p, g, 3, ST(s));
+  }
   for (double* x : {q, sI, t}) RC(sph_fftp1d_complex_to_real_z(p, x, s));
   return sph_fftp2d_qst_to_vec(p, q, sI, t, vr, vt, vp, s);
 }

@@ -123,6 +123,9 @@ struct sph_plan {
   // grid scratch for the NL step (nz*nphi*nlat doubles each)
   double* gr[9] = {nullptr};
   int ngr = 0;
+  // (m, 16-degree chunk) items of the fused z inverse into synthesis tiles (mixed)
+  int2* d_ztitems = nullptr;
+  int nztitems = 0;
   // FP64 spectral scratch of the single-precision entry points (allocated on first use)
   double2* fsp[5] = {nullptr};
   // boundary: kinds at the inner and outer wall (0 noslip, 1 freeslip); the
@@ -309,6 +312,13 @@ int tc_group_launch(const GroupLaunch& g, int* flag, cudaStream_t st);
 void group_free(GroupLaunch* g);
 // spectra -> synthesis data tiles of field slot `field` (mixed plans)
 int launch_spec_to_tiles_field(const sph_plan* p, const double2* in, int field, cudaStream_t st);
+// the z inverse of FP64 spectra (fftp1d_complex_to_real_z) written straight
+// into synthesis tiles of field `field` (the input is preserved); SPH_EINVAL
+// where it does not apply (nz without a compile-time transform length)
+bool zinv_tiles_ok(const sph_plan* p);
+int launch_zinv_tiles(const sph_plan* p, const double2* in, int field, cudaStream_t st);
+// the tensor-core synthesis from tiles already in place
+int launch_tc_synthesis_tiles(const sph_plan* p, int vector, cudaStream_t st);
 
 // Runs a set-up step (typically cudaFuncSetAttribute: a kernel's dynamic
 // shared-memory limit) once per device.  Function attributes belong to the

@@ -381,7 +381,8 @@ def fftp3d_real_to_complex(plan, in_, out, stream=None):
 
 
 def fftp3d_complex_to_real(plan, in_, out, stream=None):
-    """The input is destroyed (the z transform is in place), as in the reference."""
+    """The input may be destroyed, as in the reference (FP64 plans transform it
+    in place in z; mixed plans write the z inverse into the synthesis tiles)."""
     _call("sph_fftp3d_complex_to_real", plan.h, _s(plan, in_), _g(plan, out), _stream(stream))
 
 

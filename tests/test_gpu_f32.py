@@ -188,7 +188,7 @@ def test_boundary_and_nl_step_match_the_fp64_arrays():
     rz32, rf32, rz64, rf64 = G.new_spec32(), G.new_spec32(), G.new_spec(), G.new_spec()
     e32 = S.nl_rhs_f32(G, f32(Zs), f32(Ws), f32(Fs), 1e-3, rz32, rf32)
     e64 = S.nl_rhs(G, d64(Zs), d64(Ws), d64(Fs), 1e-3, rz64, rf64)
-    assert e32 == e64
+    assert abs(e32 - e64) <= 1e-12 * abs(e64)  # the energy sum is reduced with atomics
     check(rel_l2(host64(rz32), host64(rz64)), 1e-7, "rhs_z")
     check(rel_l2(host64(rf32), host64(rf64)), 1e-7, "rhs_phi")
     a32 = [f32(x) for x in (Zs, Ws, Fs)]
