@@ -1285,7 +1285,7 @@ __global__ void spec_to_tiles(const double2* __restrict__ in, const double2* __r
 constexpr int ZT_COLS = 16, ZT_PITCH = 17, ZT_THREADS = 256;
 
 struct ZtArgs {
-  const double2* in;
+  const void* in;  // double2, or float2 for the single-precision entry points
   __nv_bfloat16* tiles;
   const long long* toff;
   const int* mbase;
@@ -1300,16 +1300,22 @@ __device__ __forceinline__ void cp_async16zf(void* dst, const void* src, int src
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
 }
 
-template <int NZ>
+template <int NZ, typename TI>
 __global__ void __launch_bounds__(ZT_THREADS) zinv_tiles(ZtArgs a) {
   extern __shared__ double2 zs[];  // element e of column j at j + ZT_PITCH e
   const int2 it = a.items[blockIdx.x];
   const int m = it.x, c = it.y, t = threadIdx.x;
-  const double2* base = a.in + (a.mbase[m] - m);  // column l of row r at base[r nlm + l]
+  const TI* base = static_cast<const TI*>(a.in) + (a.mbase[m] - m);  // column l of row r at base[r nlm + l]
   for (int idx = t; idx < NZ * ZT_COLS; idx += ZT_THREADS) {
     const int r = idx / ZT_COLS, j = idx % ZT_COLS, l = m + ZT_COLS * c + j;
     const bool in = l <= a.lmax;
-    cp_async16zf(zs + j + ZT_PITCH * __ldg(a.rev + r), in ? base + (size_t)r * a.nlm + l : a.in, in ? 16 : 0);
+    double2* dst = zs + j + ZT_PITCH * __ldg(a.rev + r);
+    if constexpr (sizeof(TI) == sizeof(double2)) {
+      cp_async16zf(dst, in ? base + (size_t)r * a.nlm + l : a.in, in ? 16 : 0);
+    } else {  // float input, widened
+      const TI v = in ? __ldg(base + (size_t)r * a.nlm + l) : TI{0.f, 0.f};
+      *dst = make_double2((double)v.x, (double)v.y);
+    }
   }
   asm volatile("cp.async.commit_group;\n" ::: "memory");
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -2159,24 +2165,28 @@ bool zinv_tiles_ok(const sph_plan* p) {
 }
 
 namespace {
-template <int NZ>
+template <int NZ, typename TI>
 int zinv_tiles_run(const sph_plan* p, const ZtArgs& a, cudaStream_t st) {
   const size_t smem = (size_t)ZT_PITCH * NZ * sizeof(double2);
   static DeviceOnce once;
   if (!once.run([] {
-        return cudaFuncSetAttribute(zinv_tiles<NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        return cudaFuncSetAttribute(zinv_tiles<NZ, TI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)((size_t)ZT_PITCH * NZ * sizeof(double2))) == cudaSuccess &&
-               cudaFuncSetAttribute(zinv_tiles<NZ>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) ==
+               cudaFuncSetAttribute(zinv_tiles<NZ, TI>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) ==
                    cudaSuccess;
       }))
     return SPH_ECUDA;
-  zinv_tiles<NZ><<<p->nztitems, ZT_THREADS, smem, st>>>(a);
+  zinv_tiles<NZ, TI><<<p->nztitems, ZT_THREADS, smem, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
 }  // namespace
 
 int launch_zinv_tiles(const sph_plan* p, const double2* in, int field, cudaStream_t st) {
+  return launch_zinv_tiles_g(p, in, field, st, false);
+}
+
+int launch_zinv_tiles_g(const sph_plan* p, const void* in, int field, cudaStream_t st, bool f32) {
   if (!zinv_tiles_ok(p) || !in || field < 0 || field >= SPH_MAX_FIELDS) return SPH_EINVAL;
   ZtArgs a;
   a.in = in;
@@ -2192,7 +2202,7 @@ int launch_zinv_tiles(const sph_plan* p, const double2* in, int field, cudaStrea
   TimedLaunch tl(p, T_ZFFT, st);
   switch (p->nz) {
 #define CASE(n) \
-  case n: return zinv_tiles_run<n>(p, a, st);
+  case n: return f32 ? zinv_tiles_run<n, float2>(p, a, st) : zinv_tiles_run<n, double2>(p, a, st);
     ZT_SIZES(CASE)
 #undef CASE
   }

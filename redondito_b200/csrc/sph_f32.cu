@@ -189,6 +189,12 @@ extern "C" int sph_fftp3d_real_to_complex_f32(sph_plan* p, const float* in, floa
 // scratch for the synthesis; the input is preserved
 extern "C" int sph_fftp3d_complex_to_real_f32(sph_plan* p, const float* in, float* out, void* s) {
   if (!f32_ok(p) || !in || !out) return SPH_EINVAL;
+  if (zinv_tiles_ok(p)) {  // the z inverse writes the synthesis tiles directly
+    RCF(launch_zinv_tiles_g(p, in, 0, st_of(s), true));
+    RCF(launch_tc_synthesis_tiles(p, 0, st_of(s)));
+    void* g[1] = {out};
+    return launch_phi_inv32_g(p, g, 1, st_of(s), true);
+  }
   double2* i;
   RCF(scratch(p, 0, &i));
   RCF(launch_zfft_io(p, Z_INV, in, i, ZIO_FD, 0, st_of(s)));
@@ -236,6 +242,15 @@ extern "C" int sph_fftp3d_vec_to_qst_f32(sph_plan* p, const float* vr, const flo
 extern "C" int sph_fftp3d_qst_to_vec_f32(sph_plan* p, const float* q, const float* sI, const float* t, float* vr,
                                          float* vt, float* vp, void* s) {
   if (!f32_ok(p) || !q || !sI || !t || !vr || !vt || !vp) return SPH_EINVAL;
+  if (zinv_tiles_ok(p)) {
+    RCF(launch_zinv_tiles_g(p, q, 0, st_of(s), true));
+    RCF(launch_tc_synthesis_tiles(p, 0, st_of(s)));
+    RCF(launch_zinv_tiles_g(p, sI, 0, st_of(s), true));
+    RCF(launch_zinv_tiles_g(p, t, 1, st_of(s), true));
+    RCF(launch_tc_synthesis_tiles(p, 1, st_of(s)));
+    void* g[3] = {vr, vt, vp};
+    return launch_phi_inv32_g(p, g, 3, st_of(s), true);
+  }
   double2* i[3];
   const float* in[3] = {q, sI, t};
   for (int f = 0; f < 3; ++f) {
