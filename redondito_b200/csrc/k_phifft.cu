@@ -303,21 +303,22 @@ __global__ void __launch_bounds__(P3d<N, NP>::THREADS, P3d<N, NP>::MINB) phi3_in
   const int t = threadIdx.x;
   for (int i = t; i < N; i += T) tw[i] = __ldg(a.fd.tw + i);
   const size_t pstride = (size_t)a.nz * a.ldn;  // parity stride of the folded coefficients
+  // the coefficients of a tile into the stage, by cp.async (every thread its share)
+  auto issue = [&](int tile) {
+    const int g = tile % ngroups, r = tile / ngroups, k = r % a.nz, f = r / a.nz;
+    const double2* gs = a.Gc + (size_t)f * a.Gfield + (size_t)k * a.ldn + g * NP;
+    const int total = (lmax + 1) * 2 * NP;
+    for (int q = t; q < total; q += T) {
+      const int b = q % NP, rr = q / NP, par = rr & 1, mm = rr >> 1;
+      cp_async16(st + mm * 2 * NP + (par ^ stage_swz64<NP>(mm)) * NP + b, gs + (size_t)rr * pstride + b);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  if ((int)blockIdx.x < ntiles) issue(blockIdx.x);
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int g = tile % ngroups, r = tile / ngroups, k = r % a.nz, f = r / a.nz, p0 = g * NP;
-    // the staged tile of the previous iteration was last read before the
-    // barrier that follows step (C'), so it can be refilled here
-    {
-      const double2* gs = a.Gc + (size_t)f * a.Gfield + (size_t)k * a.ldn + p0;
-      const int total = (lmax + 1) * 2 * NP;
-      for (int q = t; q < total; q += T) {
-        const int b = q % NP, rr = q / NP, par = rr & 1, mm = rr >> 1;
-        cp_async16(st + mm * 2 * NP + (par ^ stage_swz64<NP>(mm)) * NP + b, gs + (size_t)rr * pstride + b);
-      }
-      asm volatile("cp.async.commit_group;\n" ::: "memory");
-      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    }
-    __syncthreads();
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();  // the tile's coefficients have landed; the last tile's step (A') is done with X
     auto zin = [&](int m, int b) {
       const bool lo = m <= lmax, hi = N - m <= lmax;
       if (!lo && !hi) return make_double2(0.0, 0.0);
@@ -343,6 +344,9 @@ __global__ void __launch_bounds__(P3d<N, NP>::THREADS, P3d<N, NP>::MINB) phi3_in
       for (int c = 0; c < C; ++c) row[c] = (c && kb) ? ct::mul(u[c], conj(tw[A * c * kb])) : u[c];
     }
     __syncthreads();
+    // step (C') was the last reader of the stage: the next tile's
+    // coefficients load while steps (B') and (A') run
+    if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
     if constexpr (B > 1) {  // (B'): stored at column c + C nb
       for (int it = t; it < G::ITEMS_B; it += T) {
         const int ka = it % A, rr = it / A, c = rr % C, b = rr / C;
