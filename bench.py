@@ -51,7 +51,9 @@ W = dict(lmax=511, nlat=768, nphi=1536, nz=256, Cz=25, oz=5, rint=0.35, rext=1.0
 # a smaller case of the same kernels for ncu captures (each grid 150 MB, still > L2)
 CASES = {"c3": W, "small": dict(lmax=255, nlat=384, nphi=768, nz=64, Cz=25, oz=5, rint=0.35, rext=1.0),
          # the benchmark's angular size on 32 planes (each grid 302 MB)
-         "angular": dict(lmax=511, nlat=768, nphi=1536, nz=32, Cz=25, oz=5, rint=0.35, rext=1.0)}
+         "angular": dict(lmax=511, nlat=768, nphi=1536, nz=32, Cz=25, oz=5, rint=0.35, rext=1.0),
+         # the benchmark's radial size on a quarter of its lm columns (each spectral field 135 MB)
+         "radial": dict(lmax=255, nlat=384, nphi=768, nz=256, Cz=25, oz=5, rint=0.35, rext=1.0)}
 METRIC = "3D transform pairs/s at lmax=511 nr=256"
 SEED = 20261203 + 3
 
@@ -72,7 +74,7 @@ def parse():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop measurement")
     ap.add_argument("--no-configs", action="store_true", help="skip the config 1 and config 2 blocks")
     ap.add_argument("--case", default="c3", choices=sorted(CASES),
-                    help="c3: the benchmark workload; small, angular: profiling cases for ncu")
+                    help="c3: the benchmark workload; small, angular, radial: profiling cases for ncu")
     a = ap.parse_args()
     W.update(CASES[a.case]) if a.case != "c3" else None
     return a

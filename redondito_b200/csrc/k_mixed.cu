@@ -952,12 +952,10 @@ __global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB_INV) phi3_
     }
     cp_async_commit();
   };
+  if ((int)blockIdx.x < ntiles) issue(blockIdx.x, stg);
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    // the staged tile of the previous iteration was last read before the
-    // barrier that follows step (C'), so it can be refilled here
-    issue(tile, stg);
     cp_async_wait_all();
-    __syncthreads();
+    __syncthreads();  // the tile's coefficients have landed; the last tile's step (A') is done with X
     const int g = tile % ngroups, r = tile / ngroups, k = r % a.nz, f = r / a.nz, p0 = g * NP;
     const float2* st = stg;
     // Z(m) of ring pair b (x = ring + i mirror) from the folded coefficients of both parities
@@ -984,6 +982,9 @@ __global__ void __launch_bounds__(P3<N, NP>::THREADS, P3<N, NP>::MINB_INV) phi3_
       for (int c = 0; c < C; ++c) row[c] = (c && kb) ? ct::mul(u[c], conj2(tw[A * c * kb])) : u[c];
     }
     __syncthreads();
+    // step (C') was the last reader of the stage: the next tile's
+    // coefficients load while steps (B') and (A') run
+    if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x, stg);
     if constexpr (B > 1) {  // (B') B-point inverse DFTs over kb, stored at column c + C nb
       for (int it = t; it < G::ITEMS_B; it += T) {
         const int ka = it % A, rr = it / A, c = rr % C, b = rr / C;
@@ -1797,9 +1798,30 @@ constexpr bool phi3_ok() {
          (size_t)2 * N * 2 * NP * sizeof(double) + (size_t)N * sizeof(float2) <= PHI3_SMEM_MAX;
 }
 
+// the inverse holds one staged coefficient tile (for the largest lmax,
+// N/2 - 1) instead of two forward tiles, so it takes 8 ring pairs at
+// lengths whose forward does not: 32-byte runs of float grid rows, 64-byte
+// runs of FP64 ones
+template <int N, int NP>
+constexpr bool phi3_inv_ok() {
+  if constexpr (N % 16 != 0 || N < 48 || NP * (N / 16) > 1024) {
+    return false;
+  } else {
+    return P3<N, NP>::XBYTES + (size_t)N * sizeof(float2) + (size_t)N * NP * sizeof(float2) <= PHI3_SMEM_MAX;
+  }
+}
+template <int N, int NP, bool FWD>
+constexpr bool phi3_fits() {
+  if constexpr (FWD) {
+    return phi3_ok<N, NP>();
+  } else {
+    return phi3_inv_ok<N, NP>();
+  }
+}
+
 template <int N, int NP, bool FWD, typename GT>
 int phi3_run(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream_t st) {
-  if constexpr (!phi3_ok<N, NP>()) {
+  if constexpr (!phi3_fits<N, NP, FWD>()) {
     return PHI3_UNSUPPORTED;
   } else {
     using G = P3<N, NP>;
@@ -1914,12 +1936,12 @@ size_t phi2_plane_floats(int nphi, int nlat2) {
 }
 
 // ring pairs per tile: the most that fit, at most the tuned ring_pairs
-template <int N>
+template <int N, bool FWD>
 int phi3_pairs(const sph_plan* p) {
   const int cap = p->tile_np ? p->tile_np : 8;
-  if (phi3_ok<N, 8>() && cap >= 8 && p->nlat2 % 8 == 0) return 8;
-  if (phi3_ok<N, 4>() && cap >= 4 && p->nlat2 % 4 == 0) return 4;
-  if (phi3_ok<N, 2>() && cap >= 2 && p->nlat2 % 2 == 0) return 2;
+  if (phi3_fits<N, 8, FWD>() && cap >= 8 && p->nlat2 % 8 == 0) return 8;
+  if (phi3_fits<N, 4, FWD>() && cap >= 4 && p->nlat2 % 4 == 0) return 4;
+  if (phi3_fits<N, 2, FWD>() && cap >= 2 && p->nlat2 % 2 == 0) return 2;
   return 0;
 }
 
@@ -1928,7 +1950,7 @@ int phi3_dispatch(const sph_plan* p, const Phi32Args& a, int nfields, cudaStream
   switch (p->nphi) {
 #define CASE(n)                                                  \
   case n:                                                        \
-    switch (phi3_pairs<n>(p)) {                                  \
+    switch (phi3_pairs<n, FWD>(p)) {                             \
       case 8: return phi3_run<n, 8, FWD, GT>(p, a, nfields, st); \
       case 4: return phi3_run<n, 4, FWD, GT>(p, a, nfields, st); \
       case 2: return phi3_run<n, 2, FWD, GT>(p, a, nfields, st); \
