@@ -151,6 +151,35 @@ struct RD<T2, 24, SG> {
   static __device__ __forceinline__ void run(T2 (&v)[24]) { comp_dft<T2, 8, 3, SG>(v); }
 };
 
+// Length 256 as 16 x 16 on one column of a shared-memory slab (element n
+// at col[n * stride]), n = n2 + 16 n1, k = k1 + 16 k2, 16 threads per
+// column.  Step 1, thread h = n2: the 16-point DFT over n1 of x[h + 16 n1],
+// times W_256^(SG h k1) (tw[e] = exp(-2 pi i e / 256)), written back over
+// the same 16 slots, at h + 16 k1.  Step 2 (after a barrier), thread h = k1:
+// the 16-point DFT over n2 of the slots 16 h .. 16 h + 15, which is X[h + 16
+// k2] in v[k2].  Two shared-memory passes instead of three radix passes, and
+// the results leave from registers.
+template <int SG>
+__device__ __forceinline__ void dft256_step1(double2* col, int stride, int h, const double2* __restrict__ tw) {
+  double2 v[16];
+#pragma unroll
+  for (int n1 = 0; n1 < 16; ++n1) v[n1] = col[(h + 16 * n1) * stride];
+  RD<double2, 16, SG>::run(v);
+  col[h * stride] = v[0];
+#pragma unroll
+  for (int k1 = 1; k1 < 16; ++k1) {
+    double2 w = __ldg(tw + h * k1);
+    if (SG > 0) w.y = -w.y;
+    col[(h + 16 * k1) * stride] = mul(v[k1], w);
+  }
+}
+template <int SG>
+__device__ __forceinline__ void dft256_step2(const double2* col, int stride, int h, double2 (&v)[16]) {
+#pragma unroll
+  for (int n2 = 0; n2 < 16; ++n2) v[n2] = col[(n2 + 16 * h) * stride];
+  RD<double2, 16, SG>::run(v);
+}
+
 // Three-step split of a phi length N = A M, M = B C: A = 16, B the
 // power-of-two part of M capped at 16, C the rest.
 __host__ __device__ constexpr int pow2_part_cap16(int m) {

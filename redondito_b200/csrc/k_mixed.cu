@@ -1294,6 +1294,7 @@ struct ZtArgs {
   int lmax, nlm, nz;
   const int* rev;
   const double2* twp;
+  const double2* tw;  // W_nz^e, e < nz (the 16 x 16 split at nz 256)
 };
 
 __device__ __forceinline__ void cp_async16zf(void* dst, const void* src, int src_bytes) {
@@ -1302,7 +1303,7 @@ __device__ __forceinline__ void cp_async16zf(void* dst, const void* src, int src
 }
 
 template <int NZ, typename TI>
-__global__ void __launch_bounds__(ZT_THREADS) zinv_tiles(ZtArgs a) {
+__global__ void __launch_bounds__(ZT_THREADS, 3) zinv_tiles(ZtArgs a) {
   extern __shared__ double2 zs[];  // element e of column j at j + ZT_PITCH e
   const int2 it = a.items[blockIdx.x];
   const int m = it.x, c = it.y, t = threadIdx.x;
@@ -1310,7 +1311,8 @@ __global__ void __launch_bounds__(ZT_THREADS) zinv_tiles(ZtArgs a) {
   for (int idx = t; idx < NZ * ZT_COLS; idx += ZT_THREADS) {
     const int r = idx / ZT_COLS, j = idx % ZT_COLS, l = m + ZT_COLS * c + j;
     const bool in = l <= a.lmax;
-    double2* dst = zs + j + ZT_PITCH * __ldg(a.rev + r);
+    // the radix passes take the input digit-reversed; the 16 x 16 split in natural order
+    double2* dst = zs + j + ZT_PITCH * (NZ == 256 ? r : __ldg(a.rev + r));
     if constexpr (sizeof(TI) == sizeof(double2)) {
       cp_async16zf(dst, in ? base + (size_t)r * a.nlm + l : a.in, in ? 16 : 0);
     } else {  // float input, widened
@@ -1322,7 +1324,21 @@ __global__ void __launch_bounds__(ZT_THREADS) zinv_tiles(ZtArgs a) {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncthreads();
   const ct::Geo<NZ, 0, false> g{ZT_COLS, 1, ZT_PITCH};
-  ct::dit<double2, NZ, NZ>(zs, g, a.twp, +1);
+  if constexpr (NZ == 256 && ZT_THREADS == ZT_COLS * 16) {
+    // the arithmetic of the plain z inverse at nz 256 (zfft256_kernel), so
+    // that both inverse paths agree bit for bit
+    const int j = t % ZT_COLS, h = t / ZT_COLS;
+    ct::dft256_step1<1>(zs + j, ZT_PITCH, h, a.tw);
+    __syncthreads();
+    double2 v[16];
+    ct::dft256_step2<1>(zs + j, ZT_PITCH, h, v);
+    __syncthreads();
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) zs[j + ZT_PITCH * (h + 16 * k2)] = v[k2];
+    __syncthreads();
+  } else {
+    ct::dit<double2, NZ, NZ>(zs, g, a.twp, +1);
+  }
   const int kt = c / (TK / 8), kk0 = (c % (TK / 8)) * 8;
   for (int w = t; w < NZ * 2; w += ZT_THREADS) {
     const int k = w >> 1, par = w & 1;
@@ -2221,6 +2237,7 @@ int launch_zinv_tiles_g(const sph_plan* p, const void* in, int field, cudaStream
   a.nz = p->nz;
   a.rev = p->fz.rev;
   a.twp = p->fz.twp;
+  a.tw = p->fz.tw;
   TimedLaunch tl(p, T_ZFFT, st);
   switch (p->nz) {
 #define CASE(n) \

@@ -14,6 +14,7 @@
 //     likewise.
 #include <mutex>
 
+#include "fft3.cuh"
 #include "fft_ct.cuh"
 
 namespace {
@@ -204,6 +205,59 @@ __global__ void __launch_bounds__(ZTHREADS) zfft_kernel(ZArgs a) {
   }
 }
 
+// nz = 256, the plain forward and inverse transforms: blocks of 8 columns,
+// 16 threads per column, the 16 x 16 split of fft3.cuh (two shared-memory
+// passes; results stored from registers).  Same loads, continuation and
+// output layout as zfft_kernel; the input of the inverse in natural order.
+constexpr int Z256_LB = 8, Z256_THREADS = Z256_LB * 16;
+
+template <int MODE, int IO>
+__global__ void __launch_bounds__(Z256_THREADS) zfft256_kernel(ZArgs a) {
+  static_assert(MODE == Z_FWD || MODE == Z_INV, "plain transforms");
+  constexpr int NZ = 256, LB = Z256_LB, SG = MODE == Z_INV ? 1 : -1;
+  extern __shared__ double2 sm[];
+  const int nlm = a.nlm, tid = threadIdx.x, lm0 = blockIdx.x * LB;
+  const bool cont = MODE == Z_FWD && a.C > 0;
+  const int nload = cont ? a.N : NZ;
+  for (int idx = tid; idx < nload * LB; idx += Z256_THREADS) {
+    const int r = idx / LB, c = idx - r * LB, lm = lm0 + c;
+    zload<IO>(a, sm + idx, (size_t)r * nlm + lm, lm < nlm);
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncthreads();
+  if (cont) {  // as in zfft_kernel
+    const int C = a.C, d = a.d, N = a.N;
+    for (int idx = tid; idx < C * LB; idx += Z256_THREADS) {
+      int ii = idx / LB, c = idx - ii * LB;
+      double2 acc;
+      {
+        double wr = __ldg(a.dir + ii), wl = __ldg(a.dir + (C - 1 - ii));
+        double2 xr = sm[(N - d) * LB + c], xl = sm[(d - 1) * LB + c];
+        acc = make_double2(wr * xr.x + wl * xl.x, wr * xr.y + wl * xl.y);
+      }
+      for (int jj = 1; jj < d; ++jj) {
+        double wr = __ldg(a.dir + ii + C * jj), wl = __ldg(a.dir + (C - 1 - ii) + C * jj);
+        double2 xr = sm[(N - d + jj) * LB + c], xl = sm[(d - 1 - jj) * LB + c];
+        acc.x = (acc.x + wr * xr.x) + wl * xl.x;
+        acc.y = (acc.y + wr * xr.y) + wl * xl.y;
+      }
+      sm[(N + ii) * LB + c] = acc;
+    }
+    __syncthreads();
+  }
+  const int c = tid % LB, h = tid / LB, lm = lm0 + c;
+  ct::dft256_step1<SG>(sm + c, LB, h, a.fd.tw);
+  __syncthreads();
+  double2 v[16];
+  ct::dft256_step2<SG>(sm + c, LB, h, v);
+  if (lm < nlm) {
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2)
+      zstore<IO>(a, (size_t)(h + 16 * k2) * nlm + lm, MODE == Z_FWD ? div_nz(v[k2], NZ) : v[k2]);
+  }
+}
+
 template <int MODE, int CTN, int IO>
 int launch_ct(const ZArgs& a, int nblocks, size_t smem, cudaStream_t st) {
   static DeviceOnce once;
@@ -214,6 +268,19 @@ int launch_ct(const ZArgs& a, int nblocks, size_t smem, cudaStream_t st) {
                                     100) == cudaSuccess;
       }))
     return SPH_ECUDA;
+  if constexpr (CTN == 256 && (MODE == Z_FWD || MODE == Z_INV)) {
+    if (a.LB == Z256_LB) {
+      static DeviceOnce once256;
+      if (!once256.run([] {
+            return cudaFuncSetAttribute(zfft256_kernel<MODE, IO>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        100) == cudaSuccess;
+          }))
+        return SPH_ECUDA;
+      zfft256_kernel<MODE, IO><<<nblocks, Z256_THREADS, smem, st>>>(a);
+      SPH_LAUNCH_OK();
+      return SPH_OK;
+    }
+  }
   zfft_kernel<MODE, CTN, IO><<<nblocks, ZTHREADS, smem, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;

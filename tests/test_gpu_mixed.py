@@ -177,12 +177,14 @@ def test_mixed_zero_and_spike_inputs():
     check(rel_l2(host(g), grid_ref), TOL_MIXED)
 
 
-@pytest.mark.parametrize("lmax,nz,nlat,nphi", [(63, 64, 96, 192), (127, 96, 192, 384), (31, 33, 48, 96)])
+@pytest.mark.parametrize("lmax,nz,nlat,nphi", [(63, 64, 96, 192), (127, 96, 192, 384), (31, 33, 48, 96),
+                                             (31, 256, 48, 96)])
 def test_3d_inverse_through_tiles_equals_the_composition(lmax, nz, nlat, nphi):
     """The mixed 3D inverses write the z inverse straight into the synthesis
     tiles (nz with a compile-time transform length; nz 33 takes the
-    composition itself): bit for bit the z inverse in place followed by the
-    2D synthesis, and the input is left unchanged."""
+    composition itself; nz 256 the 16 x 16 split in both paths): bit for bit
+    the z inverse in place followed by the 2D synthesis, and the input is
+    left unchanged."""
     from redondito_b200 import sphp as S
     P, G = _pair(lmax, nz, nlat, nphi, C=25, d=5)
     rng = np.random.default_rng(lmax + nz)
