@@ -151,33 +151,44 @@ struct RD<T2, 24, SG> {
   static __device__ __forceinline__ void run(T2 (&v)[24]) { comp_dft<T2, 8, 3, SG>(v); }
 };
 
-// Length 256 as 16 x 16 on one column of a shared-memory slab (element n
-// at col[n * stride]), n = n2 + 16 n1, k = k1 + 16 k2, 16 threads per
-// column.  Step 1, thread h = n2: the 16-point DFT over n1 of x[h + 16 n1],
-// times W_256^(SG h k1) (tw[e] = exp(-2 pi i e / 256)), written back over
-// the same 16 slots, at h + 16 k1.  Step 2 (after a barrier), thread h = k1:
-// the 16-point DFT over n2 of the slots 16 h .. 16 h + 15, which is X[h + 16
-// k2] in v[k2].  Two shared-memory passes instead of three radix passes, and
-// the results leave from registers.
-template <int SG>
-__device__ __forceinline__ void dft256_step1(double2* col, int stride, int h, const double2* __restrict__ tw) {
-  double2 v[16];
+// Two-step split of a length N = R1 R2 on one column of a shared-memory
+// slab (element n at col[n * stride]): n = n2 + R2 n1, k = k1 + R1 k2, and
+// max(R1, R2) threads per column.  Step 1, thread h = n2 < R2: the R1-point
+// DFT over n1 of x[h + R2 n1], times W_N^(SG h k1) (tw[e] = exp(-2 pi i e /
+// N)), written back over the same R1 slots, at h + R2 k1.  Step 2 (after a
+// barrier), thread h = k1 < R1: the R2-point DFT over n2 of the slots R2 h ..
+// R2 h + R2 - 1, which is X[h + R1 k2] in v[k2].  Two shared-memory passes
+// instead of one per radix pass, and the results leave from registers.
+template <int R1, int R2, int SG>
+__device__ __forceinline__ void dft2_step1(double2* col, int stride, int h, const double2* __restrict__ tw) {
+  if (h >= R2) return;
+  double2 v[R1];
 #pragma unroll
-  for (int n1 = 0; n1 < 16; ++n1) v[n1] = col[(h + 16 * n1) * stride];
-  RD<double2, 16, SG>::run(v);
+  for (int n1 = 0; n1 < R1; ++n1) v[n1] = col[(h + R2 * n1) * stride];
+  RD<double2, R1, SG>::run(v);
   col[h * stride] = v[0];
 #pragma unroll
-  for (int k1 = 1; k1 < 16; ++k1) {
+  for (int k1 = 1; k1 < R1; ++k1) {
     double2 w = __ldg(tw + h * k1);
     if (SG > 0) w.y = -w.y;
-    col[(h + 16 * k1) * stride] = mul(v[k1], w);
+    col[(h + R2 * k1) * stride] = mul(v[k1], w);
   }
 }
-template <int SG>
-__device__ __forceinline__ void dft256_step2(const double2* col, int stride, int h, double2 (&v)[16]) {
+template <int R1, int R2, int SG>
+__device__ __forceinline__ void dft2_step2(const double2* col, int stride, int h, double2 (&v)[R2]) {
+  if (h >= R1) return;
 #pragma unroll
-  for (int n2 = 0; n2 < 16; ++n2) v[n2] = col[(n2 + 16 * h) * stride];
-  RD<double2, 16, SG>::run(v);
+  for (int n2 = 0; n2 < R2; ++n2) v[n2] = col[(n2 + R2 * h) * stride];
+  RD<double2, R2, SG>::run(v);
+}
+// the first factor of the two-step split of the radial lengths with a
+// compile-time transform (0: radix passes)
+__host__ __device__ constexpr int split2_r1(int n) {
+  return n == 16 ? 4 : n == 32 ? 8 : n == 48 ? 12 : n == 64 ? 8 : n == 96 ? 12 : n == 128 ? 16 : n == 192 ? 16
+       : n == 256 ? 16 : 0;
+}
+__host__ __device__ constexpr int split2_tpc(int n) {  // threads per column
+  return split2_r1(n) == 0 ? 0 : (split2_r1(n) > n / split2_r1(n) ? split2_r1(n) : n / split2_r1(n));
 }
 
 // Three-step split of a phi length N = A M, M = B C: A = 16, B the

@@ -1294,7 +1294,7 @@ struct ZtArgs {
   int lmax, nlm, nz;
   const int* rev;
   const double2* twp;
-  const double2* tw;  // W_nz^e, e < nz (the 16 x 16 split at nz 256)
+  const double2* tw;  // W_nz^e, e < nz (the two-step split)
 };
 
 __device__ __forceinline__ void cp_async16zf(void* dst, const void* src, int src_bytes) {
@@ -1311,8 +1311,8 @@ __global__ void __launch_bounds__(ZT_THREADS, 3) zinv_tiles(ZtArgs a) {
   for (int idx = t; idx < NZ * ZT_COLS; idx += ZT_THREADS) {
     const int r = idx / ZT_COLS, j = idx % ZT_COLS, l = m + ZT_COLS * c + j;
     const bool in = l <= a.lmax;
-    // the radix passes take the input digit-reversed; the 16 x 16 split in natural order
-    double2* dst = zs + j + ZT_PITCH * (NZ == 256 ? r : __ldg(a.rev + r));
+    // the radix passes take the input digit-reversed; the two-step split in natural order
+    double2* dst = zs + j + ZT_PITCH * (ct::split2_r1(NZ) > 0 ? r : __ldg(a.rev + r));
     if constexpr (sizeof(TI) == sizeof(double2)) {
       cp_async16zf(dst, in ? base + (size_t)r * a.nlm + l : a.in, in ? 16 : 0);
     } else {  // float input, widened
@@ -1324,17 +1324,20 @@ __global__ void __launch_bounds__(ZT_THREADS, 3) zinv_tiles(ZtArgs a) {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncthreads();
   const ct::Geo<NZ, 0, false> g{ZT_COLS, 1, ZT_PITCH};
-  if constexpr (NZ == 256 && ZT_THREADS == ZT_COLS * 16) {
-    // the arithmetic of the plain z inverse at nz 256 (zfft256_kernel), so
-    // that both inverse paths agree bit for bit
+  if constexpr (ct::split2_r1(NZ) > 0 && ct::split2_tpc(NZ) * ZT_COLS <= ZT_THREADS) {
+    // the arithmetic of the plain z inverse (zfft2_kernel), so that both
+    // inverse paths agree bit for bit
+    constexpr int R1 = ct::split2_r1(NZ), R2 = NZ / R1, TPC = ct::split2_tpc(NZ);
     const int j = t % ZT_COLS, h = t / ZT_COLS;
-    ct::dft256_step1<1>(zs + j, ZT_PITCH, h, a.tw);
+    if (h < TPC) ct::dft2_step1<R1, R2, 1>(zs + j, ZT_PITCH, h, a.tw);
     __syncthreads();
-    double2 v[16];
-    ct::dft256_step2<1>(zs + j, ZT_PITCH, h, v);
+    double2 v[R2];
+    if (h < TPC) ct::dft2_step2<R1, R2, 1>(zs + j, ZT_PITCH, h, v);
     __syncthreads();
+    if (h < R1) {
 #pragma unroll
-    for (int k2 = 0; k2 < 16; ++k2) zs[j + ZT_PITCH * (h + 16 * k2)] = v[k2];
+      for (int k2 = 0; k2 < R2; ++k2) zs[j + ZT_PITCH * (h + R1 * k2)] = v[k2];
+    }
     __syncthreads();
   } else {
     ct::dit<double2, NZ, NZ>(zs, g, a.twp, +1);

@@ -205,30 +205,60 @@ __global__ void __launch_bounds__(ZTHREADS) zfft_kernel(ZArgs a) {
   }
 }
 
-// nz = 256, the plain forward and inverse transforms: blocks of 8 columns,
-// 16 threads per column, the 16 x 16 split of fft3.cuh (two shared-memory
-// passes; results stored from registers).  Same loads, continuation and
-// output layout as zfft_kernel; the input of the inverse in natural order.
-constexpr int Z256_LB = 8, Z256_THREADS = Z256_LB * 16;
+// Lengths with a two-step split N = R1 R2 (ct::split2_r1, fft3.cuh): every
+// mode, max(R1, R2) threads per column, the column slab in shared memory as
+// in zfft_kernel (same loads and continuation, the inverse's input in
+// natural order).  A plain transform is the two register steps, its results
+// stored from registers; the spectral modes run the forward steps, multiply
+// in registers, put the spectrum back in natural order and run the inverse
+// steps.
+// The columns per CTA are those launch_zfft_io picks by default for the
+// length (32 KB slabs), fixed at compile time; other choices take the radix
+// kernel.  Registers are held to about 100 per thread for the plain
+// transforms (five CTAs of 128 threads per SM at nz 256) and 128 for the
+// spectral modes (four).
+__host__ __device__ constexpr int z2_lb(int nz) {
+  int lb = 64;
+  while (lb > 1 && lb * nz > ZMAXCOL / 2) lb >>= 1;
+  return lb;
+}
+template <int MODE, int NZ, int TPC>
+struct Z2Geo {
+  static constexpr int LB = z2_lb(NZ), THREADS = LB * TPC;
+  static constexpr bool PLAIN = MODE == Z_FWD || MODE == Z_INV;
+  static constexpr int RPT = PLAIN ? 96 : 128;
+  static constexpr int MINB = 65536 / (THREADS * RPT) > 1 ? 65536 / (THREADS * RPT) : 1;
+};
 
-template <int MODE, int IO>
-__global__ void __launch_bounds__(Z256_THREADS) zfft256_kernel(ZArgs a) {
-  static_assert(MODE == Z_FWD || MODE == Z_INV, "plain transforms");
-  constexpr int NZ = 256, LB = Z256_LB, SG = MODE == Z_INV ? 1 : -1;
+template <int MODE, int R1, int R2, int IO>
+__global__ void __launch_bounds__(Z2Geo<MODE, R1 * R2, (R1 > R2 ? R1 : R2)>::THREADS,
+                                  Z2Geo<MODE, R1 * R2, (R1 > R2 ? R1 : R2)>::MINB) zfft2_kernel(ZArgs a) {
+  constexpr int NZ = R1 * R2, TPC = R1 > R2 ? R1 : R2;
+  using GZ = Z2Geo<MODE, NZ, TPC>;
+  constexpr bool PLAIN = GZ::PLAIN;
+  constexpr int SG = MODE == Z_INV ? 1 : -1;  // first transform's sign
+  constexpr int LB = GZ::LB, nthreads = GZ::THREADS;
   extern __shared__ double2 sm[];
   const int nlm = a.nlm, tid = threadIdx.x, lm0 = blockIdx.x * LB;
-  const bool cont = MODE == Z_FWD && a.C > 0;
+  const bool cont = MODE != Z_INV && a.C > 0;
   const int nload = cont ? a.N : NZ;
-  for (int idx = tid; idx < nload * LB; idx += Z256_THREADS) {
+  double2* orig = sm + (size_t)LB * NZ;  // D_l keeps the input column for the l(l+1)/r^2 term
+  for (int idx = tid; idx < nload * LB; idx += nthreads) {
     const int r = idx / LB, c = idx - r * LB, lm = lm0 + c;
     zload<IO>(a, sm + idx, (size_t)r * nlm + lm, lm < nlm);
+  }
+  if (MODE == Z_DLR) {
+    for (int idx = tid; idx < NZ * LB; idx += nthreads) {
+      const int r = idx / LB, c = idx - r * LB, lm = lm0 + c;
+      zload<IO>(a, orig + idx, (size_t)r * nlm + lm, lm < nlm);
+    }
   }
   asm volatile("cp.async.commit_group;\n" ::: "memory");
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncthreads();
   if (cont) {  // as in zfft_kernel
     const int C = a.C, d = a.d, N = a.N;
-    for (int idx = tid; idx < C * LB; idx += Z256_THREADS) {
+    for (int idx = tid; idx < C * LB; idx += nthreads) {
       int ii = idx / LB, c = idx - ii * LB;
       double2 acc;
       {
@@ -247,14 +277,45 @@ __global__ void __launch_bounds__(Z256_THREADS) zfft256_kernel(ZArgs a) {
     __syncthreads();
   }
   const int c = tid % LB, h = tid / LB, lm = lm0 + c;
-  ct::dft256_step1<SG>(sm + c, LB, h, a.fd.tw);
+  double2* col = sm + c;
+  ct::dft2_step1<R1, R2, SG>(col, LB, h, a.fd.tw);
   __syncthreads();
-  double2 v[16];
-  ct::dft256_step2<SG>(sm + c, LB, h, v);
-  if (lm < nlm) {
+  double2 v[R2];
+  ct::dft2_step2<R1, R2, SG>(col, LB, h, v);
+  if constexpr (!PLAIN) {
+    // X[k] / nz times (i kz)^p or the filter, k = h + R1 k2; back in natural
+    // order once every thread has read its step-2 slots; then the inverse
+    __syncthreads();
+    if (h < R1) {
 #pragma unroll
-    for (int k2 = 0; k2 < 16; ++k2)
-      zstore<IO>(a, (size_t)(h + 16 * k2) * nlm + lm, MODE == Z_FWD ? div_nz(v[k2], NZ) : v[k2]);
+      for (int k2 = 0; k2 < R2; ++k2) {
+        const int k = h + R1 * k2;
+        double2 x = div_nz(v[k2], NZ);
+        if (MODE == Z_FILTER) x = cscale(x, a.filt[k]);
+        else x = cmul(a.kfac[k], x);
+        col[k * LB] = x;
+      }
+    }
+    __syncthreads();
+    ct::dft2_step1<R1, R2, 1>(col, LB, h, a.fd.tw);
+    __syncthreads();
+    ct::dft2_step2<R1, R2, 1>(col, LB, h, v);
+  }
+  if (h < R1 && lm < nlm) {
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) {
+      const int r = h + R1 * k2;
+      double2 x = MODE == Z_FWD ? div_nz(v[k2], NZ) : v[k2];
+      if (MODE == Z_DLR) {
+        // b = b + z^-2 * (-l(l+1) a)   (laplang, multr(-2), saxpby_c)
+        const double lf = -(double)(a.ell[lm] * (a.ell[lm] + 1));
+        const double2 o = orig[r * LB + c];
+        const double zi = a.zinv2[r];
+        x.x = x.x + zi * (lf * o.x);
+        x.y = x.y + zi * (lf * o.y);
+      }
+      zstore<IO>(a, (size_t)r * nlm + lm, x);
+    }
   }
 }
 
@@ -268,15 +329,19 @@ int launch_ct(const ZArgs& a, int nblocks, size_t smem, cudaStream_t st) {
                                     100) == cudaSuccess;
       }))
     return SPH_ECUDA;
-  if constexpr (CTN == 256 && (MODE == Z_FWD || MODE == Z_INV)) {
-    if (a.LB == Z256_LB) {
-      static DeviceOnce once256;
-      if (!once256.run([] {
-            return cudaFuncSetAttribute(zfft256_kernel<MODE, IO>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                        100) == cudaSuccess;
+  if constexpr (CTN > 0 && ct::split2_r1(CTN) > 0) {
+    constexpr int R1 = ct::split2_r1(CTN), R2 = CTN / R1;
+    using GZ = Z2Geo<MODE, CTN, ct::split2_tpc(CTN)>;
+    if (a.LB == GZ::LB) {
+      static DeviceOnce once2;
+      if (!once2.run([] {
+            return cudaFuncSetAttribute(zfft2_kernel<MODE, R1, R2, IO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        200 * 1024) == cudaSuccess &&
+                   cudaFuncSetAttribute(zfft2_kernel<MODE, R1, R2, IO>,
+                                        cudaFuncAttributePreferredSharedMemoryCarveout, 100) == cudaSuccess;
           }))
         return SPH_ECUDA;
-      zfft256_kernel<MODE, IO><<<nblocks, Z256_THREADS, smem, st>>>(a);
+      zfft2_kernel<MODE, R1, R2, IO><<<nblocks, GZ::THREADS, smem, st>>>(a);
       SPH_LAUNCH_OK();
       return SPH_OK;
     }
@@ -428,7 +493,8 @@ extern "C" int sph_derivr_noalloc(const double* a, double* b, int nlm, int nz, i
       }
   }
   int LB = 64;
-  while (LB > 1 && LB * nz > ZMAXCOL) LB >>= 1;
+  // the column blocks of the plan path (so that both run the same kernel)
+  while (LB > 1 && LB * nz > ZMAXCOL / 2) LB >>= 1;
   if (LB * nz > ZMAXCOL) return SPH_EINVAL;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return SPH_ECUDA;
