@@ -214,9 +214,9 @@ __global__ void __launch_bounds__(ZTHREADS) zfft_kernel(ZArgs a) {
 // steps.
 // The columns per CTA are those launch_zfft_io picks by default for the
 // length (32 KB slabs), fixed at compile time; other choices take the radix
-// kernel.  Registers are held to about 100 per thread for the plain
-// transforms (five CTAs of 128 threads per SM at nz 256) and 128 for the
-// spectral modes (four).
+// kernel.  Registers are held to 80 per thread for the plain transforms
+// (six CTAs of 128 threads per SM at nz 256; 1.66 against 1.68 ms for eight
+// transforms with five) and 128 for the spectral modes (four).
 __host__ __device__ constexpr int z2_lb(int nz) {
   int lb = 64;
   while (lb > 1 && lb * nz > ZMAXCOL / 2) lb >>= 1;
@@ -226,7 +226,7 @@ template <int MODE, int NZ, int TPC>
 struct Z2Geo {
   static constexpr int LB = z2_lb(NZ), THREADS = LB * TPC;
   static constexpr bool PLAIN = MODE == Z_FWD || MODE == Z_INV;
-  static constexpr int RPT = PLAIN ? 96 : 128;
+  static constexpr int RPT = PLAIN ? 84 : 128;
   static constexpr int MINB = 65536 / (THREADS * RPT) > 1 ? 65536 / (THREADS * RPT) : 1;
 };
 
