@@ -402,7 +402,9 @@ int sph_timer_read(sph_plan* plan, double* ms, int* launches);
  * ignored by FP64 plans); ring_pairs: Gauss ring pairs per CTA of the phi
  * transforms (1, 2, 4, 8, dividing nlat/2, ring_pairs*nphi <= 8192);
  * z_cols: lm columns per CTA of the z transforms (a power of two <= 64,
- * z_cols*nz <= 4096).  0 selects the built-in choice.  Results do not
+ * z_cols*nz <= 4096; nz 16, 32, 48, 64, 96, 128, 192 and 256 keep their
+ * fixed width, the one their two-step kernel is compiled for).  0 selects
+ * the built-in choice.  Results do not
  * depend on the tile shapes beyond round-off.  Synchronises the device. */
 int sph_plan_set_tiles(sph_plan* plan, int rows, int ring_pairs, int z_cols);
 

@@ -25,6 +25,7 @@ DEFAULT_TABLE = os.path.join(HERE, "tiles_b200.json")
 ROWS = (64, 128)
 RING_PAIRS = (2, 4, 8)
 Z_COLS = (8, 16, 32, 64)
+Z_SPLIT = (16, 32, 48, 64, 96, 128, 192, 256)  # z lengths whose width is fixed
 CONCURRENT = 8  # problems per timed batch
 
 # the C4 ensemble: lmax in {63, 127, 255}, nz in {32, 64, 96, 128}, nlat = 3(lmax+1)/2, nphi = 2 nlat
@@ -57,7 +58,8 @@ def candidates(lmax, nz, nlat, nphi, precision):
     # 0: the built-in choice (FP64: the cluster forward phi kernel where its
     # tiles divide nlat/2; mixed: the kernels chosen by the transform length)
     pairs = [0] + [r for r in RING_PAIRS if (nlat // 2) % r == 0 and r * nphi <= 8192]
-    cols = [c for c in Z_COLS if c * nz <= 4096]
+    # the z lengths with a two-step kernel run at its compiled width
+    cols = [0] if nz in Z_SPLIT else [c for c in Z_COLS if c * nz <= 4096]
     return [dict(rows=r, ring_pairs=p, z_cols=c) for r, p, c in itertools.product(rows, pairs, cols)]
 
 

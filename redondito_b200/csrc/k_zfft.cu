@@ -353,6 +353,17 @@ int launch_ct(const ZArgs& a, int nblocks, size_t smem, cudaStream_t st) {
 
 #define Z_SIZES(X) X(16) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(512)
 
+// the lengths that take the two-step split
+bool zsplit_length(int nz) {
+  switch (nz) {
+#define CASE(n) \
+  case n: return ct::split2_r1(n) > 0;
+    Z_SIZES(CASE)
+#undef CASE
+  }
+  return false;
+}
+
 template <int MODE, int IO>
 int launch_mode(const ZArgs& a, int nblocks, size_t smem, cudaStream_t st) {
   switch (a.nz) {
@@ -411,7 +422,9 @@ int launch_zfft_io(const sph_plan* p, int mode, const void* in, void* out, int i
   // (32 KB slabs: 4 CTAs per SM, still full 128-byte lines per row at nz = 256)
   int LB = 64;
   while (LB > 1 && LB * p->nz > ZMAXCOL / 2) LB >>= 1;
-  if (p->tile_lb) LB = p->tile_lb;
+  // a tuned width, except for the lengths with the two-step split, whose
+  // kernel is compiled for the default width
+  if (p->tile_lb && !zsplit_length(p->nz)) LB = p->tile_lb;
   if (LB * p->nz > ZMAXCOL) return SPH_EINVAL;
   a.LB = LB;
   int nblocks = (p->nlmv + LB - 1) / LB;
