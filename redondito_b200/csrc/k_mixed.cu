@@ -1295,6 +1295,7 @@ struct ZtArgs {
   const int* rev;
   const double2* twp;
   const double2* tw;  // W_nz^e, e < nz (the two-step split)
+  double2* out;       // also the radial-space spectra, same layout as in (may be in); nullable
 };
 
 __device__ __forceinline__ void cp_async16zf(void* dst, const void* src, int src_bytes) {
@@ -1341,6 +1342,12 @@ __global__ void __launch_bounds__(ZT_THREADS, 3) zinv_tiles(ZtArgs a) {
     __syncthreads();
   } else {
     ct::dit<double2, NZ, NZ>(zs, g, a.twp, +1);
+  }
+  if (a.out) {  // the z inverse itself, in the spectra's layout (rows of 16 consecutive lm)
+    for (int idx = t; idx < NZ * ZT_COLS; idx += ZT_THREADS) {
+      const int r = idx / ZT_COLS, j = idx % ZT_COLS, l = m + ZT_COLS * c + j;
+      if (l <= a.lmax) a.out[(size_t)(a.mbase[m] - m) + (size_t)r * a.nlm + l] = zs[j + ZT_PITCH * r];
+    }
   }
   const int kt = c / (TK / 8), kk0 = (c % (TK / 8)) * 8;
   for (int w = t; w < NZ * 2; w += ZT_THREADS) {
@@ -2223,14 +2230,15 @@ int zinv_tiles_run(const sph_plan* p, const ZtArgs& a, cudaStream_t st) {
 }
 }  // namespace
 
-int launch_zinv_tiles(const sph_plan* p, const double2* in, int field, cudaStream_t st) {
-  return launch_zinv_tiles_g(p, in, field, st, false);
+int launch_zinv_tiles(const sph_plan* p, const double2* in, int field, cudaStream_t st, double2* out) {
+  return launch_zinv_tiles_g(p, in, field, st, false, out);
 }
 
-int launch_zinv_tiles_g(const sph_plan* p, const void* in, int field, cudaStream_t st, bool f32) {
-  if (!zinv_tiles_ok(p) || !in || field < 0 || field >= SPH_MAX_FIELDS) return SPH_EINVAL;
+int launch_zinv_tiles_g(const sph_plan* p, const void* in, int field, cudaStream_t st, bool f32, double2* out) {
+  if (!zinv_tiles_ok(p) || !in || field < 0 || field >= SPH_MAX_FIELDS || (f32 && out)) return SPH_EINVAL;
   ZtArgs a;
   a.in = in;
+  a.out = out;
   a.tiles = reinterpret_cast<__nv_bfloat16*>(p->Tsyn) + (size_t)field * p->Tsynfield;
   a.toff = p->d_toff;
   a.mbase = p->d_mbase;

@@ -316,8 +316,11 @@ int launch_spec_to_tiles_field(const sph_plan* p, const double2* in, int field, 
 // into synthesis tiles of field `field` (the input is preserved); SPH_EINVAL
 // where it does not apply (nz without a compile-time transform length)
 bool zinv_tiles_ok(const sph_plan* p);
-int launch_zinv_tiles(const sph_plan* p, const double2* in, int field, cudaStream_t st);
-int launch_zinv_tiles_g(const sph_plan* p, const void* in, int field, cudaStream_t st, bool f32);
+// the z inverse of field `field`'s spectra straight into its synthesis
+// tiles; with out, also the radial-space spectra (out may be in: in place)
+int launch_zinv_tiles(const sph_plan* p, const double2* in, int field, cudaStream_t st, double2* out = nullptr);
+int launch_zinv_tiles_g(const sph_plan* p, const void* in, int field, cudaStream_t st, bool f32,
+                        double2* out = nullptr);
 // the tensor-core synthesis from tiles already in place
 int launch_tc_synthesis_tiles(const sph_plan* p, int vector, cudaStream_t st);
 
