@@ -1296,6 +1296,12 @@ struct ZtArgs {
   const double2* twp;
   const double2* tw;  // W_nz^e, e < nz (the two-step split)
   double2* out;       // also the radial-space spectra, same layout as in (may be in); nullable
+  // the radial derivative of those (derivr(., 1, 'r')), when the kernel is
+  // instantiated for it: output, FC-Gram operator, i kz
+  double2* dout;
+  const double* dir;
+  int C, d, N;
+  const double2* kfac;
 };
 
 __device__ __forceinline__ void cp_async16zf(void* dst, const void* src, int src_bytes) {
@@ -1303,8 +1309,10 @@ __device__ __forceinline__ void cp_async16zf(void* dst, const void* src, int src
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
 }
 
-template <int NZ, typename TI>
-__global__ void __launch_bounds__(ZT_THREADS, 3) zinv_tiles(ZtArgs a) {
+// three CTAs per SM (80 registers); the derivative at nz 256 takes two
+// (its 16-point steps spill heavily at 80)
+template <int NZ, typename TI, bool DER = false>
+__global__ void __launch_bounds__(ZT_THREADS, (DER && NZ >= 256) ? 2 : 3) zinv_tiles(ZtArgs a) {
   extern __shared__ double2 zs[];  // element e of column j at j + ZT_PITCH e
   const int2 it = a.items[blockIdx.x];
   const int m = it.x, c = it.y, t = threadIdx.x;
@@ -1363,6 +1371,44 @@ __global__ void __launch_bounds__(ZT_THREADS, 3) zinv_tiles(ZtArgs a) {
     __nv_bfloat16* tt = a.tiles + syn_tile(a.toff, a.lmax, m, par, k / PLANES, kt) * TILE_HALVES;
     store_tile_row<8>(tt, 2 * (k % PLANES), kk0, re);
     store_tile_row<8>(tt, 2 * (k % PLANES) + 1, kk0, im);
+  }
+  if constexpr (DER && ct::split2_r1(NZ) > 0 && ct::split2_tpc(NZ) * ZT_COLS <= ZT_THREADS) {
+    // derivr(., 1, 'r') of the radial-space columns, the arithmetic of
+    // zfft2_kernel<Z_DERIV>: continuation of the last C rows, the forward
+    // split, / nz times i kz, the inverse split
+    constexpr int R1 = ct::split2_r1(NZ), R2 = NZ / R1, TPC = ct::split2_tpc(NZ);
+    const int j = t % ZT_COLS, h = t / ZT_COLS;
+    double2* col = zs + j;
+    __syncthreads();  // every read of the radial values above is done
+    if (a.C > 0) {
+      for (int idx = t; idx < a.C * ZT_COLS; idx += ZT_THREADS) {
+        const int ii = idx / ZT_COLS, jj = idx % ZT_COLS;
+        zs[jj + ZT_PITCH * (a.N + ii)] = fc_cont_elem(a.dir, a.C, a.d, a.N, ii, zs + jj, ZT_PITCH);
+      }
+      __syncthreads();
+    }
+    if (h < TPC) ct::dft2_step1<R1, R2, -1>(col, ZT_PITCH, h, a.tw);
+    __syncthreads();
+    double2 v[R2];
+    if (h < TPC) ct::dft2_step2<R1, R2, -1>(col, ZT_PITCH, h, v);
+    __syncthreads();
+    if (h < R1) {
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) {
+        const int k = h + R1 * k2;
+        col[k * ZT_PITCH] = cmul(a.kfac[k], div_nz(v[k2], NZ));
+      }
+    }
+    __syncthreads();
+    if (h < TPC) ct::dft2_step1<R1, R2, 1>(col, ZT_PITCH, h, a.tw);
+    __syncthreads();
+    if (h < TPC) ct::dft2_step2<R1, R2, 1>(col, ZT_PITCH, h, v);
+    const int l = m + ZT_COLS * c + j;
+    if (h < R1 && l <= a.lmax) {
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2)
+        a.dout[(size_t)(a.mbase[m] - m) + (size_t)(h + R1 * k2) * a.nlm + l] = v[k2];
+    }
   }
 }
 
@@ -2213,32 +2259,42 @@ bool zinv_tiles_ok(const sph_plan* p) {
 }
 
 namespace {
-template <int NZ, typename TI>
+template <int NZ, typename TI, bool DER = false>
 int zinv_tiles_run(const sph_plan* p, const ZtArgs& a, cudaStream_t st) {
   const size_t smem = (size_t)ZT_PITCH * NZ * sizeof(double2);
   static DeviceOnce once;
   if (!once.run([] {
-        return cudaFuncSetAttribute(zinv_tiles<NZ, TI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        return cudaFuncSetAttribute(zinv_tiles<NZ, TI, DER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)((size_t)ZT_PITCH * NZ * sizeof(double2))) == cudaSuccess &&
-               cudaFuncSetAttribute(zinv_tiles<NZ, TI>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) ==
-                   cudaSuccess;
+               cudaFuncSetAttribute(zinv_tiles<NZ, TI, DER>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    100) == cudaSuccess;
       }))
     return SPH_ECUDA;
-  zinv_tiles<NZ, TI><<<p->nztitems, ZT_THREADS, smem, st>>>(a);
+  zinv_tiles<NZ, TI, DER><<<p->nztitems, ZT_THREADS, smem, st>>>(a);
   SPH_LAUNCH_OK();
   return SPH_OK;
 }
 }  // namespace
 
-int launch_zinv_tiles(const sph_plan* p, const double2* in, int field, cudaStream_t st, double2* out) {
-  return launch_zinv_tiles_g(p, in, field, st, false, out);
+int launch_zinv_tiles(const sph_plan* p, const double2* in, int field, cudaStream_t st, double2* out,
+                      double2* dout) {
+  return launch_zinv_tiles_g(p, in, field, st, false, out, dout);
 }
 
-int launch_zinv_tiles_g(const sph_plan* p, const void* in, int field, cudaStream_t st, bool f32, double2* out) {
-  if (!zinv_tiles_ok(p) || !in || field < 0 || field >= SPH_MAX_FIELDS || (f32 && out)) return SPH_EINVAL;
+int launch_zinv_tiles_g(const sph_plan* p, const void* in, int field, cudaStream_t st, bool f32, double2* out,
+                        double2* dout) {
+  if (!zinv_tiles_ok(p) || !in || field < 0 || field >= SPH_MAX_FIELDS || (f32 && (out || dout)) ||
+      (dout && (!zinv_der_ok(p) || !p->kfac)))
+    return SPH_EINVAL;
   ZtArgs a;
   a.in = in;
   a.out = out;
+  a.dout = dout;
+  a.dir = p->d_dir;
+  a.C = p->C;
+  a.d = p->d;
+  a.N = p->N;
+  a.kfac = p->kfac;  // (i kz)^1
   a.tiles = reinterpret_cast<__nv_bfloat16*>(p->Tsyn) + (size_t)field * p->Tsynfield;
   a.toff = p->d_toff;
   a.mbase = p->d_mbase;
@@ -2251,12 +2307,27 @@ int launch_zinv_tiles_g(const sph_plan* p, const void* in, int field, cudaStream
   a.tw = p->fz.tw;
   TimedLaunch tl(p, T_ZFFT, st);
   switch (p->nz) {
-#define CASE(n) \
-  case n: return f32 ? zinv_tiles_run<n, float2>(p, a, st) : zinv_tiles_run<n, double2>(p, a, st);
+#define CASE(n)                                                                  \
+  case n:                                                                        \
+    if constexpr (ct::split2_r1(n) > 0) {                                        \
+      if (dout) return zinv_tiles_run<n, double2, true>(p, a, st);               \
+    }                                                                            \
+    return f32 ? zinv_tiles_run<n, float2>(p, a, st) : zinv_tiles_run<n, double2>(p, a, st);
     ZT_SIZES(CASE)
 #undef CASE
   }
   return SPH_EINVAL;
+}
+
+bool zinv_der_ok(const sph_plan* p) {
+  if (!zinv_tiles_ok(p)) return false;
+  switch (p->nz) {
+#define CASE(n) \
+  case n: return ct::split2_r1(n) > 0 && ct::split2_tpc(n) * ZT_COLS <= ZT_THREADS;
+    ZT_SIZES(CASE)
+#undef CASE
+  }
+  return false;
 }
 
 int launch_tc_synthesis_tiles(const sph_plan* p, int vector, cudaStream_t st) {

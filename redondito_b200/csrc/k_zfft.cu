@@ -66,16 +66,6 @@ __device__ __forceinline__ void cp_async16z(void* dst, const void* src, int src_
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
 }
 
-// v / nz: a multiplication by the exact reciprocal when nz is a power of
-// two (the same result bit for bit, without the cost of a double division)
-__device__ __forceinline__ double2 div_nz(double2 v, int nz) {
-  if ((nz & (nz - 1)) == 0) {
-    const double r = 1.0 / (double)nz;
-    return make_double2(v.x * r, v.y * r);
-  }
-  return make_double2(v.x / (double)nz, v.y / (double)nz);
-}
-
 // column element (row r, column lm) of the input, widened to FP64
 template <int IO>
 __device__ __forceinline__ double2 zin(const ZArgs& a, size_t idx) {
@@ -259,20 +249,8 @@ __global__ void __launch_bounds__(Z2Geo<MODE, R1 * R2, (R1 > R2 ? R1 : R2)>::THR
   if (cont) {  // as in zfft_kernel
     const int C = a.C, d = a.d, N = a.N;
     for (int idx = tid; idx < C * LB; idx += nthreads) {
-      int ii = idx / LB, c = idx - ii * LB;
-      double2 acc;
-      {
-        double wr = __ldg(a.dir + ii), wl = __ldg(a.dir + (C - 1 - ii));
-        double2 xr = sm[(N - d) * LB + c], xl = sm[(d - 1) * LB + c];
-        acc = make_double2(wr * xr.x + wl * xl.x, wr * xr.y + wl * xl.y);
-      }
-      for (int jj = 1; jj < d; ++jj) {
-        double wr = __ldg(a.dir + ii + C * jj), wl = __ldg(a.dir + (C - 1 - ii) + C * jj);
-        double2 xr = sm[(N - d + jj) * LB + c], xl = sm[(d - 1 - jj) * LB + c];
-        acc.x = (acc.x + wr * xr.x) + wl * xl.x;
-        acc.y = (acc.y + wr * xr.y) + wl * xl.y;
-      }
-      sm[(N + ii) * LB + c] = acc;
+      const int ii = idx / LB, c = idx - ii * LB;
+      sm[(N + ii) * LB + c] = fc_cont_elem(a.dir, C, d, N, ii, sm + c, LB);
     }
     __syncthreads();
   }

@@ -3,7 +3,8 @@
 // Each problem is a plan with 1..3 scalar fields.  One run computes, for
 // every (problem, field): the inverse 3D transform of its (lm, kz) spectra
 // (z transform in place, like fftp3d_complex_to_real; on mixed plans one
-// kernel writes both the in-place result and the synthesis tiles), the radial
+// kernel writes the in-place result, the synthesis tiles and the radial
+// derivative below), the radial
 // derivative of the radial-space spectra (derivr(., 1, 'r')), and the
 // forward 3D transform of the synthesised grid back into the spectra.
 //
@@ -83,14 +84,18 @@ int record(sph_batch* b) {
     const sph_plan* P = b->plans[p];
     cudaStream_t s = b->br[p % b->br.size()];
     for (int f = 0; f < b->nf[p]; ++f) {
-      if (mixed && zinv_tiles_ok(P)) {
-        // one kernel: the z inverse in place and the synthesis tiles from it
+      if (mixed && zinv_der_ok(P)) {
+        // one kernel: the z inverse in place, the synthesis tiles and the
+        // radial derivative from it
+        RCB(launch_zinv_tiles(P, CD2(b->spec[p][f]), f, s, D2(b->spec[p][f]), D2(b->dspec[p][f])));
+      } else if (mixed && zinv_tiles_ok(P)) {
         RCB(launch_zinv_tiles(P, CD2(b->spec[p][f]), f, s, D2(b->spec[p][f])));
+        RCB(launch_zfft(P, Z_DERIV, CD2(b->spec[p][f]), D2(b->dspec[p][f]), 1, s));
       } else {
         RCB(launch_zfft(P, Z_INV, CD2(b->spec[p][f]), D2(b->spec[p][f]), 0, s));
+        RCB(launch_zfft(P, Z_DERIV, CD2(b->spec[p][f]), D2(b->dspec[p][f]), 1, s));
         if (mixed) RCB(launch_spec_to_tiles_field(P, CD2(b->spec[p][f]), f, s));
       }
-      RCB(launch_zfft(P, Z_DERIV, CD2(b->spec[p][f]), D2(b->dspec[p][f]), 1, s));
     }
   }
   RCB(join(b, evi));

@@ -216,6 +216,35 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+// v / nz: a multiplication by the exact reciprocal when nz is a power of
+// two (the same result bit for bit, without the cost of a double division)
+__device__ __forceinline__ double2 div_nz(double2 v, int nz) {
+  if ((nz & (nz - 1)) == 0) {
+    const double r = 1.0 / (double)nz;
+    return make_double2(v.x * r, v.y * r);
+  }
+  return make_double2(v.x / (double)nz, v.y / (double)nz);
+}
+// continued element ii (0-based) of a column (element r at col[r * stride])
+// from its first and last d physical ones: sum_jj dir(ii,jj) x(N-d+jj) +
+// dir(C-1-ii,jj) x(d-1-jj), dir C x d column-major, the summation order of
+// the reference's continuation (sphp_sca.F90:369-381)
+__device__ __forceinline__ double2 fc_cont_elem(const double* __restrict__ dir, int C, int d, int N, int ii,
+                                                const double2* col, int stride) {
+  double2 acc;
+  {
+    const double wr = __ldg(dir + ii), wl = __ldg(dir + (C - 1 - ii));
+    const double2 xr = col[(N - d) * stride], xl = col[(d - 1) * stride];
+    acc = make_double2(wr * xr.x + wl * xl.x, wr * xr.y + wl * xl.y);
+  }
+  for (int jj = 1; jj < d; ++jj) {
+    const double wr = __ldg(dir + ii + C * jj), wl = __ldg(dir + (C - 1 - ii) + C * jj);
+    const double2 xr = col[(N - d + jj) * stride], xl = col[(d - 1 - jj) * stride];
+    acc.x = (acc.x + wr * xr.x) + wl * xl.x;
+    acc.y = (acc.y + wr * xr.y) + wl * xl.y;
+  }
+  return acc;
+}
 // multiply by (sign * i)
 __device__ __forceinline__ double2 cmul_si(double2 a, int sign) {
   return sign > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
@@ -317,10 +346,13 @@ int launch_spec_to_tiles_field(const sph_plan* p, const double2* in, int field, 
 // where it does not apply (nz without a compile-time transform length)
 bool zinv_tiles_ok(const sph_plan* p);
 // the z inverse of field `field`'s spectra straight into its synthesis
-// tiles; with out, also the radial-space spectra (out may be in: in place)
-int launch_zinv_tiles(const sph_plan* p, const double2* in, int field, cudaStream_t st, double2* out = nullptr);
+// tiles; with out, also the radial-space spectra (out may be in: in place);
+// with dout (zinv_der_ok), also their radial derivative derivr(., 1, 'r')
+int launch_zinv_tiles(const sph_plan* p, const double2* in, int field, cudaStream_t st, double2* out = nullptr,
+                      double2* dout = nullptr);
+bool zinv_der_ok(const sph_plan* p);
 int launch_zinv_tiles_g(const sph_plan* p, const void* in, int field, cudaStream_t st, bool f32,
-                        double2* out = nullptr);
+                        double2* out = nullptr, double2* dout = nullptr);
 // the tensor-core synthesis from tiles already in place
 int launch_tc_synthesis_tiles(const sph_plan* p, int vector, cudaStream_t st);
 
