@@ -12,6 +12,11 @@
 //     inverse, without the reference's temporary copy;
 //   fc_filter_r (pseudospec_hd.f90:443-467) and dlr (pseudospec_hd.f90:254-288)
 //     likewise.
+// Two kernels do the transform in shared memory: zfft2_kernel for the
+// lengths N = R1 R2 with a two-step register split (every compile-time
+// length up to 256: two shared-memory passes, results stored from
+// registers), zfft_kernel with radix passes for the others (nz 512, lengths
+// without a compile-time transform, tuned column widths).
 #include <mutex>
 
 #include "fft3.cuh"
