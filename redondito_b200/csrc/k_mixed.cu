@@ -412,7 +412,85 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm(TcLaunch L) {
       const uint32_t ta = tbase + (uint32_t)buf * 256 + ((uint32_t)(32 * q) << 16);
       const bool have0 = vector ? it.nk1 > 0 : it.nk > 0;
       const bool have1 = vector && it.nk > it.nk1;
-      for (int c = 16 * ((warp - 2) / 4); c < it.nr; c += 32) {  // the quarter's two warps alternate chunks
+      const int cfirst = 16 * ((warp - 2) / 4);  // the quarter's two warps alternate 16-column chunks
+      // global stores of one chunk whose 16 values per lane are staged in stg:
+      // 16 planes x 16 rows, lanes 0-15 rows of plane 2i, lanes 16-31 of plane 2i+1
+      auto store_chunk = [&](int c) {
+        __syncwarp();
+#pragma unroll 4
+        for (int i = 0; i < 8; ++i) {
+          const int pl = 2 * i + ph, k = kbase + pl;
+          const double re = stg[(2 * pl) * 17 + j_out], im = stg[(2 * pl + 1) * 17 + j_out];
+          const int rr = c + j_out;
+          if (k >= a.nz) continue;
+          if (analysis) {
+            if (rr >= it.nvalid) continue;
+            const int l = it.m + it.par + 2 * (it.r0 + rr);
+            double f = 1.0;
+            if (MODE == ANA_V) f = l ? 1.0 / ((double)l * (double)(l + 1)) : 0.0;
+            double2* out = (MODE == ANA_V && it.out) ? a.out2 : a.out;
+            out[(size_t)k * a.nlm + base_lm + l] = make_double2(re * f, it.m == 0 ? 0.0 : im * f);
+          } else {
+            const int field = (MODE == SYN_V) ? 1 + it.out : 0;
+            const int node = it.r0 + rr;
+            if (node < a.ldn8)
+              a.G32w[(size_t)field * a.G32field + (((size_t)it.m * 2 + it.par) * a.nz + k) * a.ldn8 + node] =
+                  make_float2((float)re, (float)im);
+          }
+        }
+        __syncwarp();
+      };
+      if constexpr (MODE == SYN_V) {
+        // Vector synthesis fills all 512 TMEM columns with one unit, so the
+        // next unit's MMAs wait until the accumulators are drained.  They are
+        // drained first: every chunk of this warp is read and combined into
+        // registers (the same float operations as below), the columns are
+        // released, and the global stores run while the next unit's MMAs do.
+        constexpr int NCH = NR_V / 32;
+        float res[NCH][16];
+        const float s0 = it.out ? -1.f : 1.f;
+        const float sg = odd ? 1.f : -1.f;  // part 1 times +i: re' = -im, im' = re
+#pragma unroll
+        for (int h = 0; h < NCH; ++h) {
+          const int c = cfirst + 32 * h;
+          if (c < it.nr) {
+            uint32_t v0[16], x0[16], v1[16], x1[16];
+            if (have0) {
+              tc05::tmem_ld16_nw(ta + c, v0);
+              tc05::tmem_ld16_nw(ta + CROSS + c, x0);
+            }
+            if (have1) {
+              tc05::tmem_ld16_nw(ta + PART + c, v1);
+              tc05::tmem_ld16_nw(ta + PART + CROSS + c, x1);
+            }
+            tc05::tmem_wait_ld();
+            tc05::tmem_regs(v0);
+            tc05::tmem_regs(x0);
+            tc05::tmem_regs(v1);
+            tc05::tmem_regs(x1);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              float rf = have0 ? s0 * (__uint_as_float(v0[j]) + __uint_as_float(x0[j])) : 0.f;
+              const float y = have1 ? __uint_as_float(v1[j]) + __uint_as_float(x1[j]) : 0.f;
+              rf += sg * __shfl_xor_sync(0xffffffffu, y, 1);
+              res[h][j] = rf;
+            }
+          }
+        }
+        tc05::fence_before();
+        tc05::mbar_arrive(&accEmpty[buf]);
+#pragma unroll
+        for (int h = 0; h < NCH; ++h) {
+          const int c = cfirst + 32 * h;
+          if (c < it.nr) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) stg[lane * 17 + j] = (double)res[h][j];
+            store_chunk(c);
+          }
+        }
+        continue;
+      }
+      for (int c = cfirst; c < it.nr; c += 32) {
         uint32_t v0[16], x0[16], v1[16], x1[16];
         if (have0) {
           tc05::tmem_ld16_nw(ta + c, v0);
@@ -450,30 +528,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm(TcLaunch L) {
           }
           stg[lane * 17 + j] = r;
         }
-        __syncwarp();
-        // 16 planes x 16 rows: lanes 0-15 rows of plane 2i, lanes 16-31 of plane 2i+1
-#pragma unroll 4
-        for (int i = 0; i < 8; ++i) {
-          const int pl = 2 * i + ph, k = kbase + pl;
-          const double re = stg[(2 * pl) * 17 + j_out], im = stg[(2 * pl + 1) * 17 + j_out];
-          const int rr = c + j_out;
-          if (k >= a.nz) continue;
-          if (analysis) {
-            if (rr >= it.nvalid) continue;
-            const int l = it.m + it.par + 2 * (it.r0 + rr);
-            double f = 1.0;
-            if (MODE == ANA_V) f = l ? 1.0 / ((double)l * (double)(l + 1)) : 0.0;
-            double2* out = (MODE == ANA_V && it.out) ? a.out2 : a.out;
-            out[(size_t)k * a.nlm + base_lm + l] = make_double2(re * f, it.m == 0 ? 0.0 : im * f);
-          } else {
-            const int field = (MODE == SYN_V) ? 1 + it.out : 0;
-            const int node = it.r0 + rr;
-            if (node < a.ldn8)
-              a.G32w[(size_t)field * a.G32field + (((size_t)it.m * 2 + it.par) * a.nz + k) * a.ldn8 + node] =
-                  make_float2((float)re, (float)im);
-          }
-        }
-        __syncwarp();
+        store_chunk(c);
       }
       tc05::fence_before();
       tc05::mbar_arrive(&accEmpty[buf]);
