@@ -8,7 +8,7 @@ pair's inverse (fftp3d_complex_to_real, and z inverse + fftp2d_qst_to_vec for
 the vector field) runs from that state and its forward
 (fftp3d_real_to_complex, and fftp2d_vec_to_qst + z forward) from the
 oracle's grids, so each direction is compared on identical inputs.  The
-FP64 form is held to north_star's relative L2 of 1e-12 per output, the
+FP64 form is held to the required relative L2 of 1e-12 per output, the
 mixed form to 1e-6 per output.
 
 C2: the vector nonlinear step at lmax 255, 384 x 768, nz 128, with the
