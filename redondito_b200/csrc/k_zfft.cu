@@ -16,7 +16,10 @@
 // lengths N = R1 R2 with a two-step register split (every compile-time
 // length up to 256: two shared-memory passes, results stored from
 // registers), zfft_kernel with radix passes for the others (nz 512, lengths
-// without a compile-time transform, tuned column widths).
+// without a compile-time transform, tuned column widths).  Batches run the
+// forward transforms of all their problems with one z length as one launch
+// of zfft2_group_kernel (the same body, one column block per CTA).
+#include <algorithm>
 #include <mutex>
 
 #include "fft3.cuh"
@@ -225,16 +228,16 @@ struct Z2Geo {
   static constexpr int MINB = 65536 / (THREADS * RPT) > 1 ? 65536 / (THREADS * RPT) : 1;
 };
 
+// column block blk of the spectra a describes
 template <int MODE, int R1, int R2, int IO>
-__global__ void __launch_bounds__(Z2Geo<MODE, R1 * R2, (R1 > R2 ? R1 : R2)>::THREADS,
-                                  Z2Geo<MODE, R1 * R2, (R1 > R2 ? R1 : R2)>::MINB) zfft2_kernel(ZArgs a) {
+__device__ __forceinline__ void zfft2_body(const ZArgs& a, int blk) {
   constexpr int NZ = R1 * R2, TPC = R1 > R2 ? R1 : R2;
   using GZ = Z2Geo<MODE, NZ, TPC>;
   constexpr bool PLAIN = GZ::PLAIN;
   constexpr int SG = MODE == Z_INV ? 1 : -1;  // first transform's sign
   constexpr int LB = GZ::LB, nthreads = GZ::THREADS;
   extern __shared__ double2 sm[];
-  const int nlm = a.nlm, tid = threadIdx.x, lm0 = blockIdx.x * LB;
+  const int nlm = a.nlm, tid = threadIdx.x, lm0 = blk * LB;
   const bool cont = MODE != Z_INV && a.C > 0;
   const int nload = cont ? a.N : NZ;
   double2* orig = sm + (size_t)LB * NZ;  // D_l keeps the input column for the l(l+1)/r^2 term
@@ -300,6 +303,27 @@ __global__ void __launch_bounds__(Z2Geo<MODE, R1 * R2, (R1 > R2 ? R1 : R2)>::THR
       zstore<IO>(a, (size_t)r * nlm + lm, x);
     }
   }
+}
+
+template <int MODE, int R1, int R2, int IO>
+__global__ void __launch_bounds__(Z2Geo<MODE, R1 * R2, (R1 > R2 ? R1 : R2)>::THREADS,
+                                  Z2Geo<MODE, R1 * R2, (R1 > R2 ? R1 : R2)>::MINB) zfft2_kernel(ZArgs a) {
+  zfft2_body<MODE, R1, R2, IO>(a, blockIdx.x);
+}
+
+// The same over the spectra of several plans with one z length (batches):
+// job j owns the CTAs prefix[j] .. prefix[j+1]-1, one column block each.
+template <int MODE, int R1, int R2, int IO>
+__global__ void __launch_bounds__(Z2Geo<MODE, R1 * R2, (R1 > R2 ? R1 : R2)>::THREADS,
+                                  Z2Geo<MODE, R1 * R2, (R1 > R2 ? R1 : R2)>::MINB)
+    zfft2_group_kernel(const ZArgs* __restrict__ jobs, const int* __restrict__ prefix, int njobs) {
+  int lo = 0, hi = njobs - 1;  // last job whose first CTA is <= blockIdx.x
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(prefix + mid) <= (int)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  zfft2_body<MODE, R1, R2, IO>(jobs[lo], (int)blockIdx.x - __ldg(prefix + lo));
 }
 
 template <int MODE, int CTN, int IO>
@@ -384,9 +408,12 @@ int launch_zfft(const sph_plan* p, int mode, const double2* in, double2* out, in
   return launch_zfft_io(p, mode, in, out, ZIO_DD, order, st, cont);
 }
 
-int launch_zfft_io(const sph_plan* p, int mode, const void* in, void* out, int io, int order, cudaStream_t st,
-                   bool cont) {
-  ZArgs a;
+namespace {
+
+// The arguments of one z transform of plan p's spectra and its CTA count.
+int make_zargs(const sph_plan* p, int mode, const void* in, void* out, int order, bool cont, ZArgs* ap,
+               int* nblocks) {
+  ZArgs& a = *ap;
   a.in = in;
   a.out = out;
   a.nlm = p->nlmv;  // the caller's lm columns [lm0, lm0 + nlmv)
@@ -410,8 +437,20 @@ int launch_zfft_io(const sph_plan* p, int mode, const void* in, void* out, int i
   if (p->tile_lb && !zsplit_length(p->nz)) LB = p->tile_lb;
   if (LB * p->nz > ZMAXCOL) return SPH_EINVAL;
   a.LB = LB;
-  int nblocks = (p->nlmv + LB - 1) / LB;
-  size_t smem = (size_t)LB * p->nz * sizeof(double2) * (mode == Z_DLR ? 2 : 1);
+  *nblocks = (p->nlmv + LB - 1) / LB;
+  if (mode == Z_DLR) a.kfac = p->kfac + (size_t)1 * p->nz;  // (i kz)^2
+  return SPH_OK;
+}
+
+}  // namespace
+
+int launch_zfft_io(const sph_plan* p, int mode, const void* in, void* out, int io, int order, cudaStream_t st,
+                   bool cont) {
+  ZArgs a;
+  int nblocks = 0;
+  const int rc = make_zargs(p, mode, in, out, order, cont, &a, &nblocks);
+  if (rc != SPH_OK) return rc;
+  size_t smem = (size_t)a.LB * p->nz * sizeof(double2) * (mode == Z_DLR ? 2 : 1);
   TimedLaunch tl(p, T_ZFFT, st);
   switch (mode) {
     case Z_FWD: return launch_mode_io<Z_FWD>(a, io, nblocks, smem, st);
@@ -420,11 +459,111 @@ int launch_zfft_io(const sph_plan* p, int mode, const void* in, void* out, int i
       if (!a.kfac) return SPH_EINVAL;
       return launch_mode_io<Z_DERIV>(a, io, nblocks, smem, st);
     case Z_FILTER: return launch_mode_io<Z_FILTER>(a, io, nblocks, smem, st);
-    case Z_DLR:
-      a.kfac = p->kfac + (size_t)1 * p->nz;  // (i kz)^2
-      return launch_mode_io<Z_DLR>(a, io, nblocks, smem, st);
+    case Z_DLR: return launch_mode_io<Z_DLR>(a, io, nblocks, smem, st);
   }
   return SPH_EINVAL;
+}
+
+// ---------------------------------------------------------------- grouped forward z (batches)
+namespace {
+
+template <int R1, int R2>
+int zgroup_launch_len(const ZGroupLen& L, cudaStream_t st) {
+  constexpr int NZ = R1 * R2;
+  using GZ = Z2Geo<Z_FWD, NZ, ct::split2_tpc(NZ)>;
+  static DeviceOnce once;
+  if (!once.run([] {
+        return cudaFuncSetAttribute(zfft2_group_kernel<Z_FWD, R1, R2, ZIO_DD>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) == cudaSuccess &&
+               cudaFuncSetAttribute(zfft2_group_kernel<Z_FWD, R1, R2, ZIO_DD>,
+                                    cudaFuncAttributePreferredSharedMemoryCarveout, 100) == cudaSuccess;
+      }))
+    return SPH_ECUDA;
+  const size_t smem = (size_t)GZ::LB * NZ * sizeof(double2);
+  zfft2_group_kernel<Z_FWD, R1, R2, ZIO_DD>
+      <<<L.total, GZ::THREADS, smem, st>>>(static_cast<const ZArgs*>(L.jobs), L.prefix, L.njobs);
+  SPH_LAUNCH_OK();
+  return SPH_OK;
+}
+
+// the two-step lengths only (the others never reach a grouped launch)
+template <int NZ>
+int zgroup_launch_nz(const ZGroupLen& L, cudaStream_t st) {
+  if constexpr (ct::split2_r1(NZ) > 0) {
+    return zgroup_launch_len<ct::split2_r1(NZ), NZ / ct::split2_r1(NZ)>(L, st);
+  } else {
+    return SPH_EINVAL;
+  }
+}
+
+}  // namespace
+
+int zfwd_group_prepare(const std::vector<ZJob>& jobs, ZGroupLaunch* g, std::vector<int>* rest) {
+  if (!g || !rest) return SPH_EINVAL;
+  rest->clear();
+  std::vector<int> lens;  // z lengths, in order of first appearance
+  std::vector<std::vector<ZArgs>> args;
+  std::vector<std::vector<int>> prefix;
+  for (int k = 0; k < (int)jobs.size(); ++k) {
+    const sph_plan* p = jobs[k].p;
+    ZArgs a;
+    int nb = 0;
+    if (!p || !jobs[k].spec || !zsplit_length(p->nz) ||
+        make_zargs(p, Z_FWD, jobs[k].spec, jobs[k].spec, 0, jobs[k].cont, &a, &nb) != SPH_OK || nb < 1 ||
+        a.LB != z2_lb(p->nz)) {
+      rest->push_back(k);
+      continue;
+    }
+    int li = (int)(std::find(lens.begin(), lens.end(), p->nz) - lens.begin());
+    if (li == (int)lens.size()) {
+      lens.push_back(p->nz);
+      args.emplace_back();
+      prefix.emplace_back(1, 0);
+    }
+    args[li].push_back(a);
+    prefix[li].push_back(prefix[li].back() + nb);
+  }
+  for (size_t li = 0; li < lens.size(); ++li) {
+    ZGroupLen L;
+    L.nz = lens[li];
+    L.njobs = (int)args[li].size();
+    L.total = prefix[li].back();
+    g->lens.push_back(L);
+    ZGroupLen& G = g->lens.back();
+    if (cudaMalloc(&G.jobs, args[li].size() * sizeof(ZArgs)) != cudaSuccess ||
+        cudaMalloc((void**)&G.prefix, prefix[li].size() * sizeof(int)) != cudaSuccess)
+      return SPH_ENOMEM;
+    if (cudaMemcpy(G.jobs, args[li].data(), args[li].size() * sizeof(ZArgs), cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        cudaMemcpy(G.prefix, prefix[li].data(), prefix[li].size() * sizeof(int), cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+      return SPH_ECUDA;
+  }
+  return SPH_OK;
+}
+
+int zfwd_group_launch(const ZGroupLaunch& g, cudaStream_t st) {
+  for (const ZGroupLen& L : g.lens) {
+    int rc = SPH_EINVAL;
+    switch (L.nz) {
+#define CASE(n)                    \
+  case n:                          \
+    rc = zgroup_launch_nz<n>(L, st); \
+    break;
+      Z_SIZES(CASE)
+#undef CASE
+    }
+    if (rc != SPH_OK) return rc;
+  }
+  return SPH_OK;
+}
+
+void zgroup_free(ZGroupLaunch* g) {
+  for (ZGroupLen& L : g->lens) {
+    if (L.jobs) cudaFree(L.jobs);
+    if (L.prefix) cudaFree(L.prefix);
+  }
+  g->lens.clear();
 }
 
 // ---------------------------------------------------------------- no-alloc derivative

@@ -11,8 +11,9 @@
 // The Legendre contractions of all problems run as ONE grouped launch per
 // direction: the persistent tensor-core kernel (mixed plans) or the FP64
 // tile kernel (FP64 plans) walks the triangular m-blocks of every
-// (problem, field) work set.  The FFT and elementwise stages run per problem
-// on parallel graph branches, so that small problems overlap.  The whole
+// (problem, field) work set.  The forward z transforms run as one grouped
+// launch per z length.  The other FFT and elementwise stages run per
+// problem on parallel graph branches, so that small problems overlap.  The whole
 // sequence is captured once into a CUDA graph and replayed by each run.
 #include <algorithm>
 #include <vector>
@@ -25,6 +26,8 @@ struct sph_batch {
   int precision = SPH_FP64;
   std::vector<std::vector<double*>> spec, grid, dspec;
   GroupLaunch syn, ana;
+  ZGroupLaunch zf;                         // grouped forward z transforms
+  std::vector<std::pair<int, int>> zrest;  // (problem, field) pairs zf does not take
   cudaStream_t main = nullptr;
   std::vector<cudaStream_t> br;
   std::vector<cudaEvent_t> ev;
@@ -45,6 +48,7 @@ void batch_free(sph_batch* b) {
   if (b->main) cudaStreamDestroy(b->main);
   group_free(&b->syn);
   group_free(&b->ana);
+  zgroup_free(&b->zf);
   if (b->dflag) cudaFree(b->dflag);
   delete b;
 }
@@ -130,16 +134,19 @@ int record(sph_batch* b) {
   RCB(join(b, evi));
   // 4: every analysis contraction in one grouped launch
   RCB(mixed ? tc_group_launch(b->ana, b->dflag, b->main) : leg_group_launch(b->ana, b->main));
-  // 5: z forward (mixed: the planes past N were continued physically)
-  RCB(fork(b, evi));
-  for (int p = 0; p < np; ++p) {
-    const sph_plan* P = b->plans[p];
-    cudaStream_t s = b->br[p % b->br.size()];
-    const bool cont = !(mixed && P->C > 0 && P->contg);
-    for (int f = 0; f < b->nf[p]; ++f)
-      RCB(launch_zfft(P, Z_FWD, CD2(b->spec[p][f]), D2(b->spec[p][f]), 0, s, cont));
+  // 5: z forward (mixed: the planes past N were continued physically), one
+  // grouped launch per z length; the rest per problem on the branches
+  RCB(zfwd_group_launch(b->zf, b->main));
+  if (!b->zrest.empty()) {
+    RCB(fork(b, evi));
+    for (size_t k = 0; k < b->zrest.size(); ++k) {
+      const int p = b->zrest[k].first, f = b->zrest[k].second;
+      const sph_plan* P = b->plans[p];
+      const bool cont = !(mixed && P->C > 0 && P->contg);
+      RCB(launch_zfft(P, Z_FWD, CD2(b->spec[p][f]), D2(b->spec[p][f]), 0, b->br[k % b->br.size()], cont));
+    }
+    RCB(join(b, evi));
   }
-  RCB(join(b, evi));
   return SPH_OK;
 }
 
@@ -188,6 +195,19 @@ extern "C" int sph_batch_create(sph_batch** out, int nprob, sph_plan* const* pla
   int rc = mixed ? tc_group_prepare(false, jobs, plans[0]->nsm, &b->syn) : leg_group_prepare(false, jobs, &b->syn);
   if (rc == SPH_OK)
     rc = mixed ? tc_group_prepare(true, jobs, plans[0]->nsm, &b->ana) : leg_group_prepare(true, jobs, &b->ana);
+  if (rc == SPH_OK) {
+    std::vector<ZJob> zj;
+    std::vector<std::pair<int, int>> pf;
+    for (int p = 0; p < nprob; ++p)
+      for (int f = 0; f < b->nf[p]; ++f) {
+        const sph_plan* P = b->plans[p];
+        zj.push_back({P, D2(b->spec[p][f]), !(mixed && P->C > 0 && P->contg)});
+        pf.push_back({p, f});
+      }
+    std::vector<int> rest;
+    rc = zfwd_group_prepare(zj, &b->zf, &rest);
+    for (int k : rest) b->zrest.push_back(pf[k]);
+  }
   if (rc == SPH_OK && cudaMalloc((void**)&b->dflag, sizeof(int)) != cudaSuccess) rc = SPH_ENOMEM;
   if (rc == SPH_OK && cudaMemset(b->dflag, 0, sizeof(int)) != cudaSuccess) rc = SPH_ECUDA;
   if (rc == SPH_OK && cudaStreamCreateWithFlags(&b->main, cudaStreamNonBlocking) != cudaSuccess) rc = SPH_ECUDA;

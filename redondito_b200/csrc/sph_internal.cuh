@@ -339,6 +339,27 @@ int leg_group_launch(const GroupLaunch& g, cudaStream_t st);
 int tc_group_prepare(bool analysis, const std::vector<GroupJob>& jobs, int nsm, GroupLaunch* g);
 int tc_group_launch(const GroupLaunch& g, int* flag, cudaStream_t st);
 void group_free(GroupLaunch* g);
+// the in-place forward z transforms of several plans' spectra (batches):
+// one grouped launch per z length whose two-step kernel runs at the plan's
+// column width, each CTA one column block of one job; cont as in
+// launch_zfft.  The indices of the jobs it does not take go to `rest`.
+struct ZJob {
+  const sph_plan* p;
+  double2* spec;
+  bool cont;
+};
+struct ZGroupLen {
+  int nz = 0;
+  void* jobs = nullptr;   // device array of the jobs' kernel arguments
+  int* prefix = nullptr;  // device [njobs + 1]: first CTA of each job
+  int njobs = 0, total = 0;
+};
+struct ZGroupLaunch {
+  std::vector<ZGroupLen> lens;
+};
+int zfwd_group_prepare(const std::vector<ZJob>& jobs, ZGroupLaunch* g, std::vector<int>* rest);
+int zfwd_group_launch(const ZGroupLaunch& g, cudaStream_t st);
+void zgroup_free(ZGroupLaunch* g);
 // spectra -> synthesis data tiles of field slot `field` (mixed plans)
 int launch_spec_to_tiles_field(const sph_plan* p, const double2* in, int field, cudaStream_t st);
 // the z inverse of FP64 spectra (fftp1d_complex_to_real_z) written straight
