@@ -1122,7 +1122,11 @@ __global__ void __launch_bounds__(PHI2_PB* PHI2_NMC, 2) phi2a_fwd32(Phi32Args a,
   }
 }
 
-constexpr int PHI2_T = 384;  // pass-2 threads: two CTAs per SM, one tile image each
+// pass-2 threads: two CTAs per SM, one tile image each.  Measured per pair
+// at 768 x 1536 x 256 x 4 fields: 5.57 ms at 512 threads, 5.08 at 384,
+// 4.99 at 256, 4.84 at 192, 4.91 at 128: fewer threads with more work each
+// (the B-step items four per thread) keep more of each thread's loads in flight.
+constexpr int PHI2_T = 192;
 template <int N>
 __host__ __device__ constexpr size_t phi2_smem() {
   return P3<N, PHI2_NP>::XBYTES + (size_t)P3<N, PHI2_NP>::M * sizeof(float2) + sizeof(uint64_t);
